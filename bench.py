@@ -1,0 +1,494 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Game of Life engine (one JSON line on rank 0).
+
+Workload (the dense bit-packed configuration): a 16384 x 16384 grid of
+i.i.d. Bernoulli(0.5) cells from the reference's RandomOnesZerosDataLoader
+(seed 42), packed into 64-bit rows, advanced 4096 generations per step,
+cells outside the grid dead. The temporal depth k is swept over 1..16
+first and the fastest k runs the headline.
+
+  value  cell-updates/s with the grid resident in HBM (CUDA events on the
+         engine's stream, L2 flushed between steps by a 256 MiB write);
+  e2e    the same metric through the public C ABI with host buffers: per
+         step set_input_u8 (host pack) -> init (H2D) -> run -> finalize
+         (D2H) -> fetch_u8 (host unpack), wall clock;
+  roofline  the pass kernel against measured HBM bandwidth (algorithmic
+         bytes: the grid read once and written once per launch), plus the
+         integer-pipe view against a live LOP3 peak probe;
+  cpu_baseline  the reference's own CPU path (oracle/_ref, GoLCpuBitwise
+         <char,64,AdderOps>) on a bounded sample on this host.
+
+`--impl reference` times the reference's CPU implementation instead, on all
+host threads. Multi-GPU (torchrun): every rank advances its own replica
+(the path has no exchange step); value = all ranks' cell-updates / the
+slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "stencil-optimalizations_b200")
+for _p in (PKG, os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "Gcell-updates/s at 16384^2 bit-exact; batched vs plain on same GPU; p50/p99 lat"
+UNIT = "Gcell-updates/s"
+SIZE = 16384
+GENS = 4096
+SEED = 42
+SWEEP_K = (1, 2, 3, 4, 5, 6, 8, 12, 16)
+FLUSH_BYTES = 256 << 20
+# sec. 8(d): the reference's full-adder formulation costs 33 word ops per
+# 64-cell word (warp-exchange-full-adder-rows.cuh:50)
+ALG_INT_OPS_PER_CELL = 33.0 / 64.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", type=int, default=SIZE)
+    ap.add_argument("--gens", type=int, default=GENS)
+    ap.add_argument("--k", type=int, default=0, help="temporal depth (0 = sweep)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-check", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (one process per GPU, replicas)
+# ---------------------------------------------------------------------------
+
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+
+    def init(self, backend: str):
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        dev = "cuda" if self.pg.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [v.strip() for v in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# reference CPU path (oracle/_ref when built here, else the oracle port)
+# ---------------------------------------------------------------------------
+
+def reference_runner():
+    import oracle
+    if oracle.ref_available():
+        def run(cells, gens):
+            return oracle.ref_cpu_bitwise_adder(cells, gens, 64)
+        return run, "reference", "GoLCpuBitwise<char,64,AdderOps> built from the reference sources"
+
+    def run(cells, gens):
+        return oracle.life_cells(cells, gens, threads=1)
+    return run, "port", "oracle C restatement of GoLCpuBitwise<AdderOps> (reference build absent)"
+
+
+def cpu_baseline(grid: np.ndarray, target_s: float = 10.0) -> dict:
+    """The reference's CPU path, one core, on a bounded sample of the grid."""
+    run, kind, what = reference_runner()
+    y, x = grid.shape
+    t0 = time.perf_counter()
+    run(grid, 2)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    gens = int(max(2, min(GENS, 2 * target_s / dt)))
+    t0 = time.perf_counter()
+    run(grid, gens)
+    dt = time.perf_counter() - t0
+    return {"value": x * y * gens / dt / 1e9, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"{x}x{y} seed {SEED}, {gens} generations, single thread ({what}); "
+                      "the reference CPU path is single-threaded"}
+
+
+def run_reference_arm(args, d: Dist) -> None:
+    if d.rank != 0:
+        return
+    import oracle
+    run, kind, what = reference_runner()
+    cores = os.cpu_count() or 1
+    size = args.size
+    grid = oracle.random_ones_zeros(size, size, SEED)
+    bands = np.array_split(np.arange(size), cores)
+    pieces = [np.ascontiguousarray(grid[b[0]:b[-1] + 1]) for b in bands if len(b)]
+
+    def step(gens):
+        out = [None] * len(pieces)
+
+        def work(i):
+            out[i] = run(pieces[i], gens)
+        ts = [threading.Thread(target=work, args=(i,)) for i in range(len(pieces))]
+        t0 = time.perf_counter()
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        return time.perf_counter() - t0
+
+    dt = max(step(2), 1e-3)
+    gens = int(max(2, min(args.gens, 2 * 2.0 / dt)))   # ~2 s per step
+    for _ in range(max(args.warmup, 0)):
+        step(gens)
+    times = [step(gens) for _ in range(args.steps)]
+    total = sum(times)
+    value = size * size * gens * args.steps / total / 1e9
+    sample = (f"{size}x{size} Bernoulli(0.5) seed {SEED} cut into {len(pieces)} row bands, one "
+              f"{what} instance per host thread, {gens} generations per step")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic",
+        "config": {"workload": f"dense {size}x{size} Bernoulli(0.5) seed {SEED}, 64-bit rows, "
+                               f"{gens} generations per step (bounded CPU sample)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": len(pieces), "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def measured_peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def ncu_traffic(k: int, wpl: int) -> float | None:
+    """DRAM bytes per launch of the pass kernel from a committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            d = json.load(f)
+    except (OSError, ValueError):
+        return None
+    ent = d.get(f"rows_temporal_kernel<{wpl},{k}>@{SIZE}")
+    return None if ent is None else float(ent["dram_bytes_per_launch"])
+
+
+def run_ours(args, d: Dist) -> None:
+    import torch
+
+    import golb200
+    torch.cuda.set_device(d.local_rank)
+    dev = torch.device("cuda", d.local_rank)
+    stream = torch.cuda.Stream(device=dev)
+    size, gens = args.size, args.gens
+    cells = golb200.load_random_ones_zeros(size, size, SEED)
+    cell_updates = size * size * gens
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+
+    def make_engine(k):
+        e = golb200.GolB200(grid_dimensions=(size, size), state_bits_count=64, temporal_steps=k,
+                            device=d.local_rank, stream=stream.cuda_stream)
+        e.set_and_format_input_data(cells)
+        e.initialize_data_structures()
+        return e
+
+    def timed_run(e, n):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        e.run(n)
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    # -- depth sweep (short runs) -------------------------------------------
+    sweep = {}
+    ks = [args.k] if args.k else list(SWEEP_K)
+    sweep_gens = min(gens, 1024)
+    for k in ks:
+        e = make_engine(k)
+        timed_run(e, min(sweep_gens, 256))
+        ms = timed_run(e, sweep_gens)
+        sweep[k] = size * size * sweep_gens / (ms * 1e-3) / 1e9
+        e.close()
+    best_k = max(sweep, key=sweep.get)
+    if d.world > 1:   # every rank uses rank 0's choice so all run the same work
+        import torch.distributed as dist
+        t = torch.tensor([best_k], device=dev)
+        dist.broadcast(t, 0)
+        best_k = int(t.item())
+
+    # -- bit-exactness of the benchmark configuration ------------------------
+    bit_exact = None
+    if not args.no_check and d.rank == 0:
+        import oracle
+        chk = 256
+        e = make_engine(best_k)
+        e.run(chk)
+        e.finalize_data_structures()
+        got = e.fetch_words(64)
+        e.close()
+        want = oracle.life_rows(oracle.pack_rows(cells, 64), size, chk, 64)
+        bit_exact = bool(np.array_equal(got, want))
+
+    # -- headline: device-resident timed steps -------------------------------
+    e = make_engine(best_k)
+    plan = e.plan()
+    for _ in range(args.warmup):
+        e.run(gens)
+        flush.zero_()
+    torch.cuda.synchronize()
+    d.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(d.local_rank)
+    clocks.start()
+    step_ms = []
+    for _ in range(args.steps):
+        step_ms.append(timed_run(e, gens))
+        with torch.cuda.stream(stream):
+            flush.zero_()          # outside the events: between timed steps
+    torch.cuda.synchronize()
+    d.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    total_ms = d.max(sum(step_ms))
+    value = d.world * cell_updates * args.steps / (total_ms * 1e-3) / 1e9
+    passes = gens // best_k + (1 if gens % best_k else 0)
+
+    # -- dominant kernel: per-launch duration (one pass of k generations) ----
+    src = e.device_grid_ptr()
+    scratch = torch.empty(size * size // 32, dtype=torch.int32, device=dev)
+    evs = []
+    for i in range(24):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        golb200.rows_pass(src, scratch.data_ptr(), size, size, best_k, plan["band_rows"],
+                          stream.cuda_stream)
+        b.record(stream)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    launch_ms = statistics.mean(a.elapsed_time(b) for a, b in evs[4:])
+    grid_bytes = size * size // 8
+    alg_bytes = 2 * grid_bytes                       # read once + write once per pass
+    achieved_gbs = alg_bytes / (launch_ms * 1e-3) / 1e9
+    peaks = measured_peaks()
+    hbm_peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if hbm_peak else "fallback"
+    hbm_peak = hbm_peak or 6650.0
+    int_peak = golb200.probe_int_peak(stream.cuda_stream)
+    pass_cell_updates = size * size * best_k
+    int_achieved = pass_cell_updates * ALG_INT_OPS_PER_CELL / (launch_ms * 1e-3)
+    e.close()
+
+    # -- 32-bit variant at 8192^2 (reported beside the headline) -------------
+    var = None
+    if d.rank == 0:
+        vsize = 8192
+        vcells = golb200.load_random_ones_zeros(vsize, vsize, SEED)
+        best = None
+        for k in (1, 2, 4, 8, 16):
+            ve = golb200.GolB200(grid_dimensions=(vsize, vsize), state_bits_count=32,
+                                 temporal_steps=k, device=d.local_rank, stream=stream.cuda_stream)
+            ve.set_and_format_input_data(vcells)
+            ve.initialize_data_structures()
+            timed_run(ve, 256)
+            ms = timed_run(ve, gens)
+            ve.close()
+            r = vsize * vsize * gens / (ms * 1e-3) / 1e9
+            if best is None or r > best[1]:
+                best = (k, r)
+        var = {"workload": f"dense {vsize}x{vsize} Bernoulli(0.5) seed {SEED}, 32-bit rows, "
+                           f"{gens} generations", "value": best[1], "unit": UNIT,
+               "temporal_steps": best[0]}
+
+    # -- e2e through the public API with host buffers -------------------------
+    e2e_times, phases = [], {"set_input": [], "init": [], "run": [], "finalize": [], "fetch": []}
+    out = np.empty_like(cells)
+    eng = golb200.GolB200(grid_dimensions=(size, size), state_bits_count=64,
+                          temporal_steps=best_k, device=d.local_rank, stream=stream.cuda_stream)
+    for it in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.set_and_format_input_data(cells)
+        t1 = time.perf_counter()
+        eng.initialize_data_structures()
+        t2 = time.perf_counter()
+        eng.run(gens)
+        t3 = time.perf_counter()
+        eng.finalize_data_structures()
+        t4 = time.perf_counter()
+        eng.fetch_result(out)
+        t5 = time.perf_counter()
+        if it >= args.warmup:
+            e2e_times.append(t5 - t0)
+            for kname, v in zip(phases, (t1 - t0, t2 - t1, t3 - t2, t4 - t3, t5 - t4)):
+                phases[kname].append(v * 1e3)
+        with torch.cuda.stream(stream):
+            flush.zero_()
+    eng.close()
+    e2e_total = d.max(sum(e2e_times))
+    e2e_value = d.world * cell_updates * args.steps / e2e_total / 1e9
+
+    cpu = None
+    if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(cells)
+
+    if d.rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic",
+            "config": {
+                "workload": f"dense {size}x{size} Bernoulli(0.5) seed {SEED}, 64-bit rows, "
+                            f"{gens} generations per step, cells outside dead",
+                "x": size, "y": size, "generations": gens, "word_bits": 64,
+                "temporal_steps": best_k, "band_rows": plan["band_rows"],
+                "words_per_lane": plan["words_per_lane"],
+                "l2": "flushed between timed steps (256 MiB write, outside the events)",
+                "parallelism": f"replicas x{d.world}" if d.world > 1 else "single GPU",
+            },
+            "bit_exact_vs_oracle_256_gens": bit_exact,
+            "k_sweep": {str(k): round(v, 1) for k, v in sweep.items()},
+            "roofline": {
+                "bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved_gbs / hbm_peak, "traffic": ncu_traffic(best_k, plan["words_per_lane"]),
+                "peak_source": peak_src,
+                "kernel": f"rows_temporal_kernel<{plan['words_per_lane']},{best_k}>",
+                "launch_ms": launch_ms,
+                "algorithmic_bytes_per_launch": alg_bytes,
+                "note": "bytes = grid read once + written once per k-generation pass "
+                        "(0.25/k B per cell-update)",
+            },
+            "int_roofline": {
+                "achieved": int_achieved, "peak": int_peak, "unit": "lane-ops/s",
+                "frac": int_achieved / int_peak,
+                "ops_per_cell_update": ALG_INT_OPS_PER_CELL,
+                "note": "algorithmic ops = the reference full-adder's 33 word-ops per 64 cells; "
+                        "peak = live LOP3 probe (gol_probe_int_peak)",
+            },
+            "variant_8192_32bit": var,
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": grid_bytes, "d2h_bytes_per_step": grid_bytes,
+                    "phases_ms_median": {k: statistics.median(v) for k, v in phases.items()},
+                    "path": "gol_set_input_u8 -> gol_init -> gol_run -> gol_finalize -> "
+                            "gol_fetch_u8 (C ABI, host uint8 grid in and out)"},
+            "gpu_launches": passes * args.steps,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    d = Dist()
+    if args.impl == "reference":
+        run_reference_arm(args, d)      # rank 0 only; no process group needed
+        return
+    import torch
+    if d.world > 1:
+        torch.cuda.set_device(d.local_rank)
+    d.init("nccl")
+    try:
+        run_ours(args, d)
+    finally:
+        d.close()
+
+
+if __name__ == "__main__":
+    main()

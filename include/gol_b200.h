@@ -1,0 +1,172 @@
+/*
+ * gol_b200.h — C ABI of the B200 Game of Life engine (libgolb200.so).
+ *
+ * A drop-in for the reference's algorithm contract
+ *   infrastructure::Algorithm<2, cell_t>   (src/infrastructure/algorithm.hpp:17-87)
+ * as driven by ExperimentManager::perform_alg
+ *   (src/infrastructure/experiment_manager.hpp:365-394):
+ *
+ *   reference virtual                              entry point here
+ *   --------------------------------------------   ------------------------------
+ *   set_params(const ExperimentParams&)  :76-78    gol_create (gol_config)
+ *   set_and_format_input_data(grid)      :37       gol_set_input_u8 / _i32 / _words
+ *   initialize_data_structures()         :42       gol_init
+ *   run(iterations)                      :49       gol_run
+ *   finalize_data_structures()           :54       gol_finalize
+ *   fetch_result()                       :61       gol_fetch_u8 / _i32 / _words
+ *   actually_performed_iterations()      :69       gol_performed
+ *   (destructor)                                   gol_destroy
+ *
+ * Semantics follow the reference: Conway B3/S23, cells outside the grid are
+ * dead, `iterations` generations are advanced (0 leaves the grid as it
+ * is, like GoLCpuNaive, gol_cpu_naive.hpp:26-78), a nonzero cell is alive
+ * when packing (general_bit_grid.hpp:217-246), results unpack to 0/1, and
+ * run() stops early once `max_runtime_seconds` of wall time have passed,
+ * reporting the generations actually done (timer.hpp:29-52).
+ *
+ * The grid lives on one GPU in the reference's fully-packed rows layout
+ * (bit_modes.hpp:127-148): bit i of row word xw is cell (xw*W + i, y), words
+ * row-major. On a little-endian device 32- and 64-bit words give the same
+ * bytes, so `word_bits` only fixes the width granularity (X % word_bits == 0).
+ *
+ * Errors: every int-returning call returns GOL_OK (0) or a negative
+ * GOL_E_* code and never throws; gol_last_error() describes the last
+ * failure of that engine. (The reference throws std::runtime_error /
+ * CudaError instead, cuch.hpp:42-52; the C++ adapter in
+ * stencil-optimalizations_b200/host/gol_b200_algorithm.hpp maps codes back
+ * to exceptions.) There is no CPU fallback: without a usable CUDA device
+ * gol_init fails with GOL_E_CUDA.
+ */
+#ifndef GOL_B200_H
+#define GOL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GOL_B200_ABI_VERSION 1
+
+enum gol_status {
+    GOL_OK = 0,
+    GOL_E_INVALID = -1,      /* bad argument or shape                           */
+    GOL_E_STATE = -2,        /* call out of the contract's phase order          */
+    GOL_E_CUDA = -3,         /* CUDA runtime error (message in gol_last_error)  */
+    GOL_E_NOMEM = -4,        /* host or device allocation failed                */
+    GOL_E_UNSUPPORTED = -5   /* shape/parameters outside what the kernels cover */
+};
+
+/* Which kernel family gol_run uses. */
+enum gol_algorithm {
+    GOL_ALG_AUTO = 0,        /* temporal rows, depth picked by the engine       */
+    GOL_ALG_ROWS = 1,        /* temporal rows with temporal_steps = k           */
+    GOL_ALG_LOCAL = 2        /* change-tracking tiles (skips stable tiles)      */
+};
+
+/* Mirrors the ExperimentParams fields the hot path reads
+ * (src/infrastructure/experiment_params.hpp:21-116). Zero = engine default. */
+typedef struct gol_config {
+    uint32_t struct_size;           /* sizeof(gol_config), for ABI checks        */
+    uint32_t algorithm;             /* enum gol_algorithm                        */
+    uint64_t x, y;                  /* grid_dimensions (cells)                   */
+    uint32_t word_bits;             /* 32 or 64 (state width of the layout)      */
+    uint32_t temporal_steps;        /* k generations per pass (0 = auto)         */
+    uint32_t thread_block_size;     /* rows per CTA band (0 = auto)              */
+    uint32_t tile_rows;             /* change-tracking tile height (0 = auto)    */
+    uint64_t max_runtime_seconds;   /* 0 = unlimited                             */
+    int32_t device;                 /* CUDA device ordinal                       */
+    uint32_t reserved;
+    void* stream;                   /* cudaStream_t to use; NULL = own stream    */
+} gol_config;
+
+typedef struct gol_engine gol_engine;
+
+/* Fills *cfg with defaults for an x-by-y grid. */
+void gol_config_init(gol_config* cfg, uint64_t x, uint64_t y);
+
+/* Creates an engine (no device work yet). */
+int gol_create(gol_engine** out, const gol_config* cfg);
+
+/* set_and_format_input_data: copies and packs a host cell grid (row-major,
+ * x fastest: cell (cx, cy) at cells[cy*x + cx]). x, y must match the config. */
+int gol_set_input_u8(gol_engine* e, const uint8_t* cells, uint64_t x, uint64_t y);
+int gol_set_input_i32(gol_engine* e, const int32_t* cells, uint64_t x, uint64_t y);
+/* Already packed rows (word_bits 32 or 64, x/word_bits words per row). */
+int gol_set_input_words(gol_engine* e, const void* words, uint64_t x, uint64_t y,
+                        uint32_t word_bits);
+
+/* initialize_data_structures: allocates the device grids, copies input in. */
+int gol_init(gol_engine* e);
+
+/* run: advances n generations on the device (asynchronous on the engine's
+ * stream; gol_finalize or gol_sync waits). */
+int gol_run(gol_engine* e, uint64_t n);
+
+/* Waits for the engine's queued device work. */
+int gol_sync(gol_engine* e);
+
+/* finalize_data_structures: waits, copies the grid back, frees device memory. */
+int gol_finalize(gol_engine* e);
+
+/* fetch_result: unpacks the finalized grid into the caller's buffer. */
+int gol_fetch_u8(gol_engine* e, uint8_t* cells);
+int gol_fetch_i32(gol_engine* e, int32_t* cells);
+int gol_fetch_words(gol_engine* e, void* words, uint32_t word_bits);
+
+/* actually_performed_iterations of the last gol_run. */
+uint64_t gol_performed(const gol_engine* e);
+
+void gol_destroy(gol_engine* e);
+
+/* Last failure of this engine (or of gol_create when e is NULL). */
+const char* gol_last_error(const gol_engine* e);
+
+/* --- Input generation ----------------------------------------------------- */
+
+/* The reference's RandomOnesZerosDataLoader
+ * (src/infrastructure/data_loader.hpp:57-75): one
+ * std::uniform_int_distribution<int>(0, 1) draw from std::mt19937(seed) per
+ * cell, raster order (cells[cy*x + cx]). Host only. */
+int gol_load_random_ones_zeros(uint8_t* cells, uint64_t x, uint64_t y, uint64_t seed);
+
+/* --- Device-resident access (between gol_init and gol_finalize) ---------- */
+
+/* Device pointer to the current grid (x/32 uint32 words per row). */
+void* gol_device_grid(gol_engine* e);
+/* The engine's cudaStream_t. */
+void* gol_stream(gol_engine* e);
+/* Temporal depth and band height gol_run uses (after gol_init). */
+int gol_plan(const gol_engine* e, uint32_t* temporal_steps, uint32_t* band_rows,
+             uint32_t* words_per_lane);
+
+/* --- Stateless device entry points -------------------------------------- */
+
+/* One pass of k generations, d_src -> d_dst (device row grids, x/32 words
+ * per row, must not overlap). k in 1..16. band_rows = 0 picks a default.
+ * Asynchronous on `stream`. */
+int gol_rows_pass(const void* d_src, void* d_dst, uint64_t x, uint64_t y, uint32_t k,
+                  uint32_t band_rows, void* stream);
+
+/* Packs / unpacks a device cell grid (uint8, nonzero = alive) to / from
+ * device row words. x % 32 == 0. */
+int gol_pack_cells_device(const uint8_t* d_cells, void* d_words, uint64_t x, uint64_t y,
+                          void* stream);
+int gol_unpack_cells_device(const void* d_words, uint8_t* d_cells, uint64_t x, uint64_t y,
+                            void* stream);
+
+/* Measures the device's 32-bit LOP3 throughput (lane-ops/s) with a short
+ * register-only kernel: the integer-pipe roofline of the bit-sliced passes.
+ * Synchronizes `stream`. */
+int gol_probe_int_peak(double* lane_ops_per_s, void* stream);
+
+/* Library identification: ABI version and the sm arch it was built for. */
+int gol_abi_version(void);
+const char* gol_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GOL_B200_H */

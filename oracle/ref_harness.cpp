@@ -1,0 +1,158 @@
+// Test infrastructure, not product code.
+//
+// Builds the reference's own CPU path for bit-packed Game of Life into
+// oracle/_ref/libgolref.so, straight from the reference sources (compiled
+// where they lie, never copied), so tests can check the C restatement in
+// gol_oracle.c and the CUDA engine against the reference itself.
+//
+// Exposed (extern "C", plain pointers):
+//   ref_load_random_ones_zeros : RandomOnesZerosDataLoader<2,char>::load_data
+//                                (src/infrastructure/data_loader.hpp:57-75)
+//   ref_run_cpu_naive          : algorithms::GoLCpuNaive<char>, the
+//                                reference's default validator
+//                                (src/algorithms/cpu-naive/gol_cpu_naive.hpp:26-117,
+//                                src/infrastructure/experiment_params.hpp:43)
+//   ref_run_cpu_bitwise_adder  : algorithms::GoLCpuBitwise<char, 32|64, AdderOps>
+//                                (src/algorithms/cpu-bitwise-general/gol_cpu_bitwise_general.hpp:32-120)
+//   ref_pack_rows / ref_unpack_rows : GeneralBitGrid<uintW_t, AdderMode>
+//                                fill_grid / to_grid
+//                                (src/algorithms/_shared/bitwise/general_bit_grid.hpp:171-246)
+//
+// The algorithm phases are called directly in the order the reference's
+// ExperimentManager::perform_alg uses (experiment_manager.hpp:365-394);
+// TimedAlgorithm is skipped because its Timer synchronises a CUDA device
+// (timer.hpp:15-26) and this harness must run without one.
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <limits>
+#include <vector>
+
+#include "algorithms/_shared/bitwise/bitwise-ops/cpu-ops-interface.hpp"
+#include "algorithms/_shared/bitwise/general_bit_grid.hpp"
+#include "algorithms/cpu-bitwise-general/gol_cpu_bitwise_general.hpp"
+#include "algorithms/cpu-naive/gol_cpu_naive.hpp"
+#include "infrastructure/data_loader.hpp"
+#include "infrastructure/experiment_params.hpp"
+#include "infrastructure/grid.hpp"
+
+namespace {
+
+using CharGrid = infrastructure::Grid<2, char>;
+
+infrastructure::ExperimentParams make_params(std::size_t x, std::size_t y, std::size_t iters,
+                                             std::size_t seed) {
+    infrastructure::ExperimentParams p;
+    p.grid_dimensions = {x, y};
+    p.iterations = iters;
+    p.random_seed = seed;
+    p.animate_output = false;
+    p.max_runtime_seconds = infrastructure::StopWatch::MAX_TIME;
+    return p;
+}
+
+CharGrid grid_from(const uint8_t* cells, std::size_t x, std::size_t y) {
+    CharGrid g(x, y);
+    std::memcpy(g.data(), cells, x * y);
+    return g;
+}
+
+void grid_to(const CharGrid& g, uint8_t* out) {
+    std::memcpy(out, g.data(), g.size());
+}
+
+template <typename Alg>
+void run_phases(Alg& alg, const uint8_t* in, std::size_t x, std::size_t y, std::size_t iters,
+                uint8_t* out) {
+    alg.set_params(make_params(x, y, iters, 0));
+    alg.set_and_format_input_data(grid_from(in, x, y));
+    alg.initialize_data_structures();
+    alg.run(iters);
+    alg.finalize_data_structures();
+    grid_to(alg.fetch_result(), out);
+}
+
+template <typename word_t>
+using RowBitGrid = algorithms::GeneralBitGrid<word_t, algorithms::AdderMode>;
+
+} // namespace
+
+extern "C" {
+
+int ref_load_random_ones_zeros(uint64_t x, uint64_t y, uint64_t seed, uint8_t* out) {
+    try {
+        infrastructure::RandomOnesZerosDataLoader<2, char> loader;
+        auto g = loader.load_data(make_params(x, y, 0, seed));
+        grid_to(g, out);
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+int ref_run_cpu_naive(const uint8_t* in, uint64_t x, uint64_t y, uint64_t iters, uint8_t* out) {
+    try {
+        algorithms::GoLCpuNaive<char> alg;
+        run_phases(alg, in, x, y, iters, out);
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+int ref_run_cpu_bitwise_adder(int word_bits, const uint8_t* in, uint64_t x, uint64_t y,
+                              uint64_t iters, uint8_t* out) {
+    try {
+        if (word_bits == 64) {
+            algorithms::GoLCpuBitwise<char, 64, algorithms::AdderOps> alg;
+            run_phases(alg, in, x, y, iters, out);
+        } else if (word_bits == 32) {
+            algorithms::GoLCpuBitwise<char, 32, algorithms::AdderOps> alg;
+            run_phases(alg, in, x, y, iters, out);
+        } else {
+            return -2;
+        }
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+int ref_pack_rows(int word_bits, const uint8_t* cells, uint64_t x, uint64_t y, void* words) {
+    try {
+        auto g = grid_from(cells, x, y);
+        if (word_bits == 64) {
+            RowBitGrid<uint64_t> bg(g);
+            std::memcpy(words, bg.data(), bg.size() * sizeof(uint64_t));
+        } else if (word_bits == 32) {
+            RowBitGrid<uint32_t> bg(g);
+            std::memcpy(words, bg.data(), bg.size() * sizeof(uint32_t));
+        } else {
+            return -2;
+        }
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+int ref_unpack_rows(int word_bits, const void* words, uint64_t x, uint64_t y, uint8_t* cells) {
+    try {
+        if (word_bits == 64) {
+            RowBitGrid<uint64_t> bg(x, y);
+            std::memcpy(bg.data(), words, bg.size() * sizeof(uint64_t));
+            grid_to(bg.template to_grid<char>(), cells);
+        } else if (word_bits == 32) {
+            RowBitGrid<uint32_t> bg(x, y);
+            std::memcpy(bg.data(), words, bg.size() * sizeof(uint32_t));
+            grid_to(bg.template to_grid<char>(), cells);
+        } else {
+            return -2;
+        }
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+} // extern "C"

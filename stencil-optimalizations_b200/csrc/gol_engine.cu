@@ -1,0 +1,478 @@
+// The engine behind include/gol_b200.h: the reference's Algorithm phase
+// contract (src/infrastructure/algorithm.hpp:17-87) over device-resident,
+// row-packed grids, advanced by the temporal row-band kernel.
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "gol_b200.h"
+#include "gol_internal.h"
+
+#define GOL_STR_(v) #v
+#define GOL_STR(v) GOL_STR_(v)
+
+using golb200::RowsPlan;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+// Passes per captured CUDA graph (even, so a chunk ends on the same buffer
+// parity it started from and one executable graph per parity suffices).
+constexpr int kGraphPasses = 16;
+
+} // namespace
+
+struct gol_engine {
+    gol_config cfg{};
+    uint64_t x = 0, y = 0;
+    int W = 0, Y = 0;              // 32-bit words per row, rows
+
+    uint32_t* h_words = nullptr;   // host copy of the grid (input, then result)
+    size_t h_bytes = 0;
+    bool h_pinned = false;
+    bool has_host_grid = false;
+
+    bool initialized = false;
+    uint32_t* d[2] = {nullptr, nullptr};
+    int cur = 0;                   // buffer holding the current generation
+    uint64_t performed = 0;
+
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaStream_t capture_stream = nullptr;
+    cudaGraphExec_t chunk[2] = {nullptr, nullptr};
+
+    int k = 1;
+    RowsPlan plan{};
+    std::string err;
+
+    int fail(int code, const std::string& msg) {
+        err = msg;
+        return code;
+    }
+    int cuda_fail(cudaError_t e, const char* what) {
+        err = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+        return GOL_E_CUDA;
+    }
+};
+
+namespace {
+
+void release_graphs(gol_engine* e) {
+    for (auto& g : e->chunk) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+}
+
+void release_device(gol_engine* e) {
+    release_graphs(e);
+    for (auto& p : e->d) {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+    e->initialized = false;
+}
+
+void release_host(gol_engine* e) {
+    if (e->h_words) {
+        if (e->h_pinned)
+            cudaFreeHost(e->h_words);
+        else
+            std::free(e->h_words);
+    }
+    e->h_words = nullptr;
+    e->h_bytes = 0;
+    e->h_pinned = false;
+    e->has_host_grid = false;
+}
+
+int check_shape(gol_engine* e, uint64_t x, uint64_t y) {
+    if (x != e->x || y != e->y)
+        return e->fail(GOL_E_INVALID, "grid dimensions differ from the engine's configuration");
+    return GOL_OK;
+}
+
+// Host grid buffer, pinned when a device is available so H2D/D2H run at
+// full link speed; pageable otherwise (packing needs no device).
+int ensure_host(gol_engine* e) {
+    const size_t bytes = (size_t)e->W * (size_t)e->Y * sizeof(uint32_t);
+    if (e->h_words && e->h_bytes == bytes) return GOL_OK;
+    release_host(e);
+    void* p = nullptr;
+    if (bytes && cudaSetDevice(e->cfg.device) == cudaSuccess &&
+        cudaMallocHost(&p, bytes) == cudaSuccess) {
+        e->h_pinned = true;
+    } else {
+        cudaGetLastError();
+        p = std::malloc(bytes ? bytes : 4);
+        e->h_pinned = false;
+        if (!p) return e->fail(GOL_E_NOMEM, "host allocation failed");
+    }
+    e->h_words = static_cast<uint32_t*>(p);
+    e->h_bytes = bytes;
+    return GOL_OK;
+}
+
+int launch_pass(gol_engine* e, int k, cudaStream_t s, int from) {
+    RowsPlan p = e->plan;
+    if (k != e->k) {
+        if (!golb200::plan_rows(e->W, e->Y, k, (int)e->cfg.thread_block_size,
+                                golb200::device_sm_count(e->cfg.device), &p))
+            return e->fail(GOL_E_UNSUPPORTED, "no kernel plan for this width and depth");
+    }
+    cudaError_t ce = golb200::launch_rows_pass(e->d[from], e->d[from ^ 1], e->W, e->Y, k, p, s);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "rows pass launch");
+    return GOL_OK;
+}
+
+int build_chunk_graph(gol_engine* e, int parity) {
+    if (!e->capture_stream) {
+        cudaError_t ce = cudaStreamCreateWithFlags(&e->capture_stream, cudaStreamNonBlocking);
+        if (ce != cudaSuccess) return e->cuda_fail(ce, "capture stream");
+    }
+    cudaError_t ce = cudaStreamBeginCapture(e->capture_stream, cudaStreamCaptureModeThreadLocal);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "begin capture");
+    int from = parity;
+    int rc = GOL_OK;
+    for (int i = 0; i < kGraphPasses && rc == GOL_OK; ++i) {
+        rc = launch_pass(e, e->k, e->capture_stream, from);
+        from ^= 1;
+    }
+    cudaGraph_t graph = nullptr;
+    ce = cudaStreamEndCapture(e->capture_stream, &graph);
+    if (rc != GOL_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "end capture");
+    ce = cudaGraphInstantiate(&e->chunk[parity], graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "graph instantiate");
+    return GOL_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+void gol_config_init(gol_config* cfg, uint64_t x, uint64_t y) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->struct_size = sizeof(gol_config);
+    cfg->algorithm = GOL_ALG_AUTO;
+    cfg->x = x;
+    cfg->y = y;
+    cfg->word_bits = 64;
+}
+
+int gol_create(gol_engine** out, const gol_config* cfg) {
+    if (!out || !cfg) {
+        g_create_error = "null argument";
+        return GOL_E_INVALID;
+    }
+    *out = nullptr;
+    if (cfg->struct_size != sizeof(gol_config)) {
+        g_create_error = "gol_config.struct_size does not match this library's ABI";
+        return GOL_E_INVALID;
+    }
+    if (cfg->word_bits != 32 && cfg->word_bits != 64) {
+        g_create_error = "word_bits must be 32 or 64";
+        return GOL_E_INVALID;
+    }
+    if (cfg->x % cfg->word_bits != 0) {
+        g_create_error = "grid dimension x must be a multiple of word_bits";
+        return GOL_E_INVALID;
+    }
+    if (cfg->x / 32 > (uint64_t)1 << 30 || cfg->y > (uint64_t)1 << 30) {
+        g_create_error = "grid too large";
+        return GOL_E_INVALID;
+    }
+    if (cfg->temporal_steps > (uint32_t)golb200::kMaxTemporalSteps) {
+        g_create_error = "temporal_steps must be at most 16";
+        return GOL_E_INVALID;
+    }
+    if (cfg->algorithm > GOL_ALG_LOCAL) {
+        g_create_error = "unknown algorithm";
+        return GOL_E_INVALID;
+    }
+    gol_engine* e = new (std::nothrow) gol_engine();
+    if (!e) {
+        g_create_error = "out of host memory";
+        return GOL_E_NOMEM;
+    }
+    e->cfg = *cfg;
+    e->x = cfg->x;
+    e->y = cfg->y;
+    e->W = (int)(cfg->x / 32);
+    e->Y = (int)cfg->y;
+    *out = e;
+    return GOL_OK;
+}
+
+int gol_set_input_u8(gol_engine* e, const uint8_t* cells, uint64_t x, uint64_t y) {
+    if (!e) return GOL_E_INVALID;
+    if (!cells && x * y) return e->fail(GOL_E_INVALID, "null cells");
+    if (e->initialized) return e->fail(GOL_E_STATE, "set_input while device data is live");
+    int rc = check_shape(e, x, y);
+    if (rc) return rc;
+    if ((rc = ensure_host(e))) return rc;
+    golb200::host_pack_u8(cells, x, y, e->h_words);
+    e->has_host_grid = true;
+    e->performed = 0;
+    return GOL_OK;
+}
+
+int gol_set_input_i32(gol_engine* e, const int32_t* cells, uint64_t x, uint64_t y) {
+    if (!e) return GOL_E_INVALID;
+    if (!cells && x * y) return e->fail(GOL_E_INVALID, "null cells");
+    if (e->initialized) return e->fail(GOL_E_STATE, "set_input while device data is live");
+    int rc = check_shape(e, x, y);
+    if (rc) return rc;
+    if ((rc = ensure_host(e))) return rc;
+    golb200::host_pack_i32(cells, x, y, e->h_words);
+    e->has_host_grid = true;
+    e->performed = 0;
+    return GOL_OK;
+}
+
+int gol_set_input_words(gol_engine* e, const void* words, uint64_t x, uint64_t y,
+                        uint32_t word_bits) {
+    if (!e) return GOL_E_INVALID;
+    if (word_bits != 32 && word_bits != 64) return e->fail(GOL_E_INVALID, "word_bits must be 32 or 64");
+    if (x % word_bits) return e->fail(GOL_E_INVALID, "x must be a multiple of word_bits");
+    if (!words && x * y) return e->fail(GOL_E_INVALID, "null words");
+    if (e->initialized) return e->fail(GOL_E_STATE, "set_input while device data is live");
+    int rc = check_shape(e, x, y);
+    if (rc) return rc;
+    if ((rc = ensure_host(e))) return rc;
+    std::memcpy(e->h_words, words, e->h_bytes);   // same bytes for 32- and 64-bit rows
+    e->has_host_grid = true;
+    e->performed = 0;
+    return GOL_OK;
+}
+
+int gol_init(gol_engine* e) {
+    if (!e) return GOL_E_INVALID;
+    if (!e->has_host_grid) return e->fail(GOL_E_STATE, "initialize before set_input");
+    if (e->initialized) return e->fail(GOL_E_STATE, "already initialized");
+    if (e->cfg.algorithm == GOL_ALG_LOCAL)
+        return e->fail(GOL_E_UNSUPPORTED, "change-tracking engine is not available in this build");
+    cudaError_t ce = cudaSetDevice(e->cfg.device);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "cudaSetDevice");
+    if (!e->stream) {
+        if (e->cfg.stream) {
+            e->stream = static_cast<cudaStream_t>(e->cfg.stream);
+            e->own_stream = false;
+        } else {
+            ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+            if (ce != cudaSuccess) return e->cuda_fail(ce, "stream create");
+            e->own_stream = true;
+        }
+    }
+    int k = (int)e->cfg.temporal_steps;
+    if (k <= 0) k = 4;
+    const int sms = golb200::device_sm_count(e->cfg.device);
+    if (!golb200::plan_rows(e->W, e->Y, k, (int)e->cfg.thread_block_size, sms, &e->plan))
+        return e->fail(GOL_E_UNSUPPORTED, "no kernel plan for this width and depth");
+    e->k = k;
+    const size_t bytes = (size_t)e->W * e->Y * sizeof(uint32_t);
+    for (auto& p : e->d) {
+        ce = cudaMalloc(&p, bytes ? bytes : 4);
+        if (ce != cudaSuccess) {
+            release_device(e);
+            return ce == cudaErrorMemoryAllocation ? e->fail(GOL_E_NOMEM, "device allocation failed")
+                                                   : e->cuda_fail(ce, "cudaMalloc");
+        }
+    }
+    e->cur = 0;
+    ce = cudaMemcpyAsync(e->d[0], e->h_words, bytes, cudaMemcpyHostToDevice, e->stream);
+    if (ce != cudaSuccess) {
+        release_device(e);
+        return e->cuda_fail(ce, "H2D copy");
+    }
+    e->initialized = true;
+    e->performed = 0;
+    return GOL_OK;
+}
+
+int gol_run(gol_engine* e, uint64_t n) {
+    if (!e) return GOL_E_INVALID;
+    if (!e->initialized) return e->fail(GOL_E_STATE, "run before initialize");
+    e->performed = 0;
+    if (n == 0 || e->W == 0 || e->Y == 0) {
+        e->performed = n;
+        return GOL_OK;
+    }
+    const uint64_t budget = e->cfg.max_runtime_seconds;
+    const auto t0 = std::chrono::steady_clock::now();
+    auto time_is_up = [&]() {
+        if (budget == 0) return false;
+        auto s = std::chrono::duration_cast<std::chrono::seconds>(std::chrono::steady_clock::now() - t0);
+        return (uint64_t)s.count() >= budget;
+    };
+    const int k = e->k;
+    uint64_t passes = n / (uint64_t)k;
+    const int rem = (int)(n % (uint64_t)k);
+    int rc;
+    if (budget == 0 && passes >= 2 * (uint64_t)kGraphPasses) {
+        while (passes >= (uint64_t)kGraphPasses) {
+            if (!e->chunk[e->cur] && (rc = build_chunk_graph(e, e->cur))) return rc;
+            cudaError_t ce = cudaGraphLaunch(e->chunk[e->cur], e->stream);
+            if (ce != cudaSuccess) return e->cuda_fail(ce, "graph launch");
+            passes -= kGraphPasses;
+            e->performed += (uint64_t)kGraphPasses * k;
+        }
+    }
+    for (; passes > 0; --passes) {
+        if (time_is_up()) return GOL_OK;
+        if ((rc = launch_pass(e, k, e->stream, e->cur))) return rc;
+        e->cur ^= 1;
+        e->performed += k;
+    }
+    if (rem > 0) {
+        if (time_is_up()) return GOL_OK;
+        if ((rc = launch_pass(e, rem, e->stream, e->cur))) return rc;
+        e->cur ^= 1;
+        e->performed += rem;
+    }
+    return GOL_OK;
+}
+
+int gol_sync(gol_engine* e) {
+    if (!e) return GOL_E_INVALID;
+    if (!e->stream) return GOL_OK;
+    cudaError_t ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "stream synchronize");
+    return GOL_OK;
+}
+
+int gol_finalize(gol_engine* e) {
+    if (!e) return GOL_E_INVALID;
+    if (!e->initialized) return e->fail(GOL_E_STATE, "finalize before initialize");
+    cudaError_t ce = cudaMemcpyAsync(e->h_words, e->d[e->cur], e->h_bytes, cudaMemcpyDeviceToHost,
+                                     e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    release_device(e);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "D2H copy");
+    return GOL_OK;
+}
+
+int gol_fetch_u8(gol_engine* e, uint8_t* cells) {
+    if (!e) return GOL_E_INVALID;
+    if (!e->has_host_grid || e->initialized) return e->fail(GOL_E_STATE, "fetch before finalize");
+    if (!cells && e->x * e->y) return e->fail(GOL_E_INVALID, "null cells");
+    golb200::host_unpack_u8(e->h_words, e->x, e->y, cells);
+    return GOL_OK;
+}
+
+int gol_fetch_i32(gol_engine* e, int32_t* cells) {
+    if (!e) return GOL_E_INVALID;
+    if (!e->has_host_grid || e->initialized) return e->fail(GOL_E_STATE, "fetch before finalize");
+    if (!cells && e->x * e->y) return e->fail(GOL_E_INVALID, "null cells");
+    golb200::host_unpack_i32(e->h_words, e->x, e->y, cells);
+    return GOL_OK;
+}
+
+int gol_fetch_words(gol_engine* e, void* words, uint32_t word_bits) {
+    if (!e) return GOL_E_INVALID;
+    if (word_bits != 32 && word_bits != 64) return e->fail(GOL_E_INVALID, "word_bits must be 32 or 64");
+    if (e->x % word_bits) return e->fail(GOL_E_INVALID, "x must be a multiple of word_bits");
+    if (!e->has_host_grid || e->initialized) return e->fail(GOL_E_STATE, "fetch before finalize");
+    if (!words && e->h_bytes) return e->fail(GOL_E_INVALID, "null words");
+    std::memcpy(words, e->h_words, e->h_bytes);
+    return GOL_OK;
+}
+
+uint64_t gol_performed(const gol_engine* e) { return e ? e->performed : 0; }
+
+void gol_destroy(gol_engine* e) {
+    if (!e) return;
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    release_device(e);
+    release_host(e);
+    if (e->capture_stream) cudaStreamDestroy(e->capture_stream);
+    if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+const char* gol_last_error(const gol_engine* e) {
+    return e ? e->err.c_str() : g_create_error.c_str();
+}
+
+void* gol_device_grid(gol_engine* e) {
+    return (e && e->initialized) ? static_cast<void*>(e->d[e->cur]) : nullptr;
+}
+
+void* gol_stream(gol_engine* e) { return e ? static_cast<void*>(e->stream) : nullptr; }
+
+int gol_plan(const gol_engine* e, uint32_t* temporal_steps, uint32_t* band_rows,
+             uint32_t* words_per_lane) {
+    if (!e) return GOL_E_INVALID;
+    if (!e->initialized) return GOL_E_STATE;
+    if (temporal_steps) *temporal_steps = (uint32_t)e->k;
+    if (band_rows) *band_rows = (uint32_t)e->plan.band;
+    if (words_per_lane) *words_per_lane = (uint32_t)e->plan.wpl;
+    return GOL_OK;
+}
+
+int gol_rows_pass(const void* d_src, void* d_dst, uint64_t x, uint64_t y, uint32_t k,
+                  uint32_t band_rows, void* stream) {
+    if (!d_src || !d_dst || x % 32 || k < 1 || k > (uint32_t)golb200::kMaxTemporalSteps)
+        return GOL_E_INVALID;
+    if (x / 32 > (uint64_t)1 << 30 || y > (uint64_t)1 << 30) return GOL_E_INVALID;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return GOL_E_CUDA;
+    RowsPlan p;
+    if (!golb200::plan_rows((int)(x / 32), (int)y, (int)k, (int)band_rows,
+                            golb200::device_sm_count(dev), &p))
+        return GOL_E_UNSUPPORTED;
+    cudaError_t ce = golb200::launch_rows_pass(static_cast<const uint32_t*>(d_src),
+                                               static_cast<uint32_t*>(d_dst), (int)(x / 32), (int)y,
+                                               (int)k, p, static_cast<cudaStream_t>(stream));
+    return ce == cudaSuccess ? GOL_OK : GOL_E_CUDA;
+}
+
+int gol_pack_cells_device(const uint8_t* d_cells, void* d_words, uint64_t x, uint64_t y,
+                          void* stream) {
+    if ((!d_cells || !d_words) && x * y) return GOL_E_INVALID;
+    if (x % 32) return GOL_E_INVALID;
+    cudaError_t ce = golb200::launch_pack_cells(d_cells, static_cast<uint32_t*>(d_words), x, y,
+                                                static_cast<cudaStream_t>(stream));
+    return ce == cudaSuccess ? GOL_OK : GOL_E_CUDA;
+}
+
+int gol_unpack_cells_device(const void* d_words, uint8_t* d_cells, uint64_t x, uint64_t y,
+                            void* stream) {
+    if ((!d_cells || !d_words) && x * y) return GOL_E_INVALID;
+    if (x % 32) return GOL_E_INVALID;
+    cudaError_t ce = golb200::launch_unpack_cells(static_cast<const uint32_t*>(d_words), d_cells, x,
+                                                  y, static_cast<cudaStream_t>(stream));
+    return ce == cudaSuccess ? GOL_OK : GOL_E_CUDA;
+}
+
+int gol_load_random_ones_zeros(uint8_t* cells, uint64_t x, uint64_t y, uint64_t seed) {
+    if (!cells && x * y) return GOL_E_INVALID;
+    golb200::host_random_ones_zeros(cells, (size_t)(x * y), seed);
+    return GOL_OK;
+}
+
+int gol_probe_int_peak(double* lane_ops_per_s, void* stream) {
+    if (!lane_ops_per_s) return GOL_E_INVALID;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return GOL_E_CUDA;
+    cudaError_t ce = golb200::probe_lop3_rate(dev, static_cast<cudaStream_t>(stream), lane_ops_per_s);
+    return ce == cudaSuccess ? GOL_OK : GOL_E_CUDA;
+}
+
+int gol_abi_version(void) { return GOL_B200_ABI_VERSION; }
+
+const char* gol_build_info(void) {
+    return "golb200: sm_100a row-band temporal Game of Life engine, CUDA runtime " GOL_STR(CUDART_VERSION);
+}
+
+} // extern "C"

@@ -1,0 +1,53 @@
+// Internal declarations shared by the engine's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace golb200 {
+
+// Largest temporal depth instantiated for a given words-per-lane width.
+// The register rings grow as 8 * K * WPL words per thread, so K * WPL <= 16
+// keeps them well inside 255 registers.
+constexpr int kMaxKForWpl(int wpl) { return wpl == 4 ? 4 : (wpl == 2 ? 8 : 16); }
+constexpr int kMaxTemporalSteps = 16;
+
+struct RowsPlan {
+    int wpl = 0;       // 32-bit words per lane: 4, 2 or 1
+    int threads = 0;   // CTA size
+    int band = 0;      // output rows per CTA
+    int nbands = 0;    // CTAs along y
+    int slice = 0;     // words per x-slice (= W when one CTA spans the row)
+    int nslices = 0;   // CTAs along x
+    int halo = 0;      // x-halo words each side of a slice (0 when unsliced)
+};
+
+// Picks words-per-lane and CTA shape for a W-word by Y-row grid and depth k.
+// Returns false only for k outside 1..16.
+bool plan_rows(int W, int Y, int k, int band_rows, int num_sms, RowsPlan* plan);
+
+// One pass of k generations (1 <= k <= kMaxKForWpl(plan.wpl)).
+cudaError_t launch_rows_pass(const uint32_t* src, uint32_t* dst, int W, int Y, int k,
+                             const RowsPlan& plan, cudaStream_t stream);
+
+cudaError_t launch_pack_cells(const uint8_t* cells, uint32_t* words, size_t x, size_t y,
+                              cudaStream_t stream);
+cudaError_t launch_unpack_cells(const uint32_t* words, uint8_t* cells, size_t x, size_t y,
+                                cudaStream_t stream);
+
+// Host packing between a cell grid and 32-bit row words (multi-threaded).
+void host_pack_u8(const uint8_t* cells, size_t x, size_t y, uint32_t* words);
+void host_pack_i32(const int32_t* cells, size_t x, size_t y, uint32_t* words);
+void host_unpack_u8(const uint32_t* words, size_t x, size_t y, uint8_t* cells);
+void host_unpack_i32(const uint32_t* words, size_t x, size_t y, int32_t* cells);
+
+void host_random_ones_zeros(uint8_t* cells, size_t n, uint64_t seed);
+
+int device_sm_count(int device);
+
+// Measured LOP3 throughput of the device (32-bit lane-ops per second).
+cudaError_t probe_lop3_rate(int device, cudaStream_t stream, double* lane_ops_per_s);
+
+} // namespace golb200

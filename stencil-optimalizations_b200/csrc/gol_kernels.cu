@@ -1,0 +1,214 @@
+// Kernel instantiations and launch dispatch for the row-band temporal
+// kernel, plus device-side pack/unpack between uint8 cells and row words.
+#include <algorithm>
+
+#include "gol_internal.h"
+#include "gol_rows_temporal.cuh"
+#include "gol_word_ops.cuh"
+
+namespace golb200 {
+
+namespace {
+
+template <int WPL, int K>
+cudaError_t launch_one(const RowsLaunch& a, const RowsPlan& p, cudaStream_t stream) {
+    const size_t smem = temporal_smem_bytes(K, p.threads);
+    rows_temporal_kernel<WPL, K><<<dim3(p.nbands, p.nslices), p.threads, smem, stream>>>(a);
+    return cudaPeekAtLastError();
+}
+
+template <int WPL, int K>
+cudaError_t dispatch_k(int k, const RowsLaunch& a, const RowsPlan& p, cudaStream_t stream) {
+    if constexpr (K > kMaxKForWpl(WPL)) {
+        return cudaErrorInvalidValue;
+    } else {
+        if (k == K) return launch_one<WPL, K>(a, p, stream);
+        return dispatch_k<WPL, K + 1>(k, a, p, stream);
+    }
+}
+
+} // namespace
+
+int device_sm_count(int device) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) n = 148;
+    return n > 0 ? n : 148;
+}
+
+bool plan_rows(int W, int Y, int k, int band_rows, int num_sms, RowsPlan* plan) {
+    if (k < 1 || k > kMaxTemporalSteps || W <= 0) return false;
+    // Widest lane access whose register rings fit this depth.
+    int wpl = 0;
+    for (int cand : {4, 2, 1}) {
+        if (W % cand == 0 && k <= kMaxKForWpl(cand)) {
+            wpl = cand;
+            break;
+        }
+    }
+    if (wpl == 0) return false;
+    plan->wpl = wpl;
+    const int lanes = W / wpl;
+    if (lanes <= kTemporalMaxThreads) {
+        plan->slice = W;
+        plan->nslices = 1;
+        plan->halo = 0;
+        plan->threads = std::max(32, (lanes + 31) / 32 * 32);
+    } else {
+        const int per = kTemporalMaxThreads - 2;               // one halo lane each side
+        const int ns = (lanes + per - 1) / per;
+        const int slice_lanes = (lanes + ns - 1) / ns;
+        plan->slice = slice_lanes * wpl;
+        plan->nslices = (W + plan->slice - 1) / plan->slice;
+        plan->halo = wpl;
+        plan->threads = (slice_lanes + 2 + 31) / 32 * 32;
+    }
+    int band = band_rows;
+    if (band <= 0) {
+        // About two CTAs per SM; never thinner than a few times the depth,
+        // whose y-halo costs ~k extra rows per stage per band.
+        const int target = std::max(1, 2 * num_sms / plan->nslices);
+        band = (Y + target - 1) / target;
+        band = std::max(band, std::max(8, 4 * k));
+    }
+    band = std::min(band, std::max(Y, 1));
+    plan->band = band;
+    plan->nbands = (Y + band - 1) / band;
+    return true;
+}
+
+cudaError_t launch_rows_pass(const uint32_t* src, uint32_t* dst, int W, int Y, int k,
+                             const RowsPlan& p, cudaStream_t stream) {
+    if (Y <= 0 || W <= 0) return cudaSuccess;
+    RowsLaunch a{src, dst, W, Y, p.band, p.slice, p.halo};
+    switch (p.wpl) {
+        case 4: return dispatch_k<4, 1>(k, a, p, stream);
+        case 2: return dispatch_k<2, 1>(k, a, p, stream);
+        case 1: return dispatch_k<1, 1>(k, a, p, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Device pack / unpack (uint8 cell grid <-> row words), the device-side form
+// of GeneralBitGrid::fill_grid / to_grid (general_bit_grid.hpp:171-246).
+// ---------------------------------------------------------------------------
+
+namespace {
+
+// 8 cells (one byte each, nonzero = alive) -> 8 bits, cell i at bit i.
+__device__ __forceinline__ uint32_t pack8(unsigned long long v) {
+    v |= v >> 4;
+    v |= v >> 2;
+    v |= v >> 1;
+    v &= 0x0101010101010101ull;
+    return (uint32_t)((v * 0x0102040810204080ull) >> 56);
+}
+
+// 8 bits -> 8 cells of 0/1, bit i to byte i.
+__device__ __forceinline__ unsigned long long unpack8(uint32_t b) {
+    unsigned long long v = (unsigned long long)(b & 0xffu) * 0x0101010101010101ull;
+    v &= 0x8040201008040201ull;
+    return ((v + 0x7f7f7f7f7f7f7f7full) >> 7) & 0x0101010101010101ull;
+}
+
+__global__ void pack_cells_kernel(const uint8_t* __restrict__ cells, uint32_t* __restrict__ words,
+                                  size_t nwords) {
+    for (size_t w = blockIdx.x * (size_t)blockDim.x + threadIdx.x; w < nwords;
+         w += (size_t)gridDim.x * blockDim.x) {
+        const ulonglong2* p = reinterpret_cast<const ulonglong2*>(cells + w * 32);
+        const ulonglong2 a = p[0];
+        const ulonglong2 b = p[1];
+        words[w] = pack8(a.x) | (pack8(a.y) << 8) | (pack8(b.x) << 16) | (pack8(b.y) << 24);
+    }
+}
+
+__global__ void unpack_cells_kernel(const uint32_t* __restrict__ words, uint8_t* __restrict__ cells,
+                                    size_t nwords) {
+    for (size_t w = blockIdx.x * (size_t)blockDim.x + threadIdx.x; w < nwords;
+         w += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t v = words[w];
+        ulonglong2* p = reinterpret_cast<ulonglong2*>(cells + w * 32);
+        p[0] = make_ulonglong2(unpack8(v), unpack8(v >> 8));
+        p[1] = make_ulonglong2(unpack8(v >> 16), unpack8(v >> 24));
+    }
+}
+
+int grid_for(size_t n, int threads) {
+    size_t blocks = (n + threads - 1) / threads;
+    return (int)std::min<size_t>(std::max<size_t>(blocks, 1), 148 * 16);
+}
+
+} // namespace
+
+cudaError_t launch_pack_cells(const uint8_t* cells, uint32_t* words, size_t x, size_t y,
+                              cudaStream_t stream) {
+    const size_t n = x / 32 * y;
+    if (n == 0) return cudaSuccess;
+    pack_cells_kernel<<<grid_for(n, 256), 256, 0, stream>>>(cells, words, n);
+    return cudaPeekAtLastError();
+}
+
+cudaError_t launch_unpack_cells(const uint32_t* words, uint8_t* cells, size_t x, size_t y,
+                                cudaStream_t stream) {
+    const size_t n = x / 32 * y;
+    if (n == 0) return cudaSuccess;
+    unpack_cells_kernel<<<grid_for(n, 256), 256, 0, stream>>>(words, cells, n);
+    return cudaPeekAtLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Integer-pipe peak probe: independent LOP3 chains (8 per thread) with no
+// memory traffic, to measure the lane-ops/s ceiling the temporal kernel's
+// bit-sliced arithmetic is bounded by.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+__global__ void lop3_rate_kernel(uint32_t* sink, int iters, uint32_t seed) {
+    uint32_t v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[j] = (threadIdx.x + 1u) * (2u * j + 3u) ^ seed;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                v[j] = lop3<LUT_XOR3>(v[j], v[(j + 1) & 7], v[(j + 3) & 7]);
+        }
+    }
+    uint32_t acc = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc ^= v[j];
+    if (acc == 0x9e3779b9u) sink[blockIdx.x] = acc;   // keeps the chains live
+}
+
+} // namespace
+
+cudaError_t probe_lop3_rate(int device, cudaStream_t stream, double* lane_ops_per_s) {
+    const int sms = device_sm_count(device);
+    const int blocks = sms * 8, threads = 256, iters = 4096;
+    uint32_t* sink = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaError_t e = cudaMalloc(&sink, sizeof(uint32_t) * blocks);
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    if (e == cudaSuccess) {
+        lop3_rate_kernel<<<blocks, threads, 0, stream>>>(sink, iters / 8, 1u);   // warm-up
+        cudaEventRecord(a, stream);
+        lop3_rate_kernel<<<blocks, threads, 0, stream>>>(sink, iters, 2u);
+        cudaEventRecord(b, stream);
+        e = cudaEventSynchronize(b);
+    }
+    if (e == cudaSuccess) {
+        float ms = 0.f;
+        e = cudaEventElapsedTime(&ms, a, b);
+        const double ops = (double)blocks * threads * iters * 16.0 * 8.0;
+        *lane_ops_per_s = ops / (ms * 1e-3);
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (sink) cudaFree(sink);
+    return e;
+}
+
+} // namespace golb200

@@ -1,0 +1,292 @@
+"""Python front end of the B200 Game of Life engine (libgolb200.so, C ABI
+in include/gol_b200.h).
+
+``GolB200`` mirrors the reference's algorithm contract
+``infrastructure::Algorithm<2, cell_t>`` (src/infrastructure/algorithm.hpp:17-87)
+method for method — set_and_format_input_data, initialize_data_structures,
+run, finalize_data_structures, fetch_result, actually_performed_iterations,
+set_params — and raises RuntimeError where the reference throws
+(std::runtime_error / CudaError, cuch.hpp:42-52).
+
+There is no CPU fallback: if libgolb200.so is missing this module raises on
+first use, and every computation runs on the GPU through the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgolb200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "gol_b200.h")
+
+GOL_OK = 0
+GOL_E_INVALID = -1
+GOL_E_STATE = -2
+GOL_E_CUDA = -3
+GOL_E_NOMEM = -4
+GOL_E_UNSUPPORTED = -5
+
+ALGORITHMS = {"auto": 0, "rows": 1, "local": 2}
+
+
+class GolConfig(ctypes.Structure):
+    _fields_ = [
+        ("struct_size", ctypes.c_uint32),
+        ("algorithm", ctypes.c_uint32),
+        ("x", ctypes.c_uint64),
+        ("y", ctypes.c_uint64),
+        ("word_bits", ctypes.c_uint32),
+        ("temporal_steps", ctypes.c_uint32),
+        ("thread_block_size", ctypes.c_uint32),
+        ("tile_rows", ctypes.c_uint32),
+        ("max_runtime_seconds", ctypes.c_uint64),
+        ("device", ctypes.c_int32),
+        ("reserved", ctypes.c_uint32),
+        ("stream", ctypes.c_void_p),
+    ]
+
+
+_lib = None
+_vp = ctypes.c_void_p
+_u64 = ctypes.c_uint64
+_u32 = ctypes.c_uint32
+
+
+def lib():
+    """Loads libgolb200.so (building it first if this tree has nvcc)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is not built; run `python stencil-optimalizations_b200/build.py` "
+            "(the engine has no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    L.gol_config_init.argtypes = [ctypes.POINTER(GolConfig), _u64, _u64]
+    L.gol_config_init.restype = None
+    L.gol_create.argtypes = [ctypes.POINTER(_vp), ctypes.POINTER(GolConfig)]
+    L.gol_set_input_u8.argtypes = [_vp, _vp, _u64, _u64]
+    L.gol_set_input_i32.argtypes = [_vp, _vp, _u64, _u64]
+    L.gol_set_input_words.argtypes = [_vp, _vp, _u64, _u64, _u32]
+    L.gol_init.argtypes = [_vp]
+    L.gol_run.argtypes = [_vp, _u64]
+    L.gol_sync.argtypes = [_vp]
+    L.gol_finalize.argtypes = [_vp]
+    L.gol_fetch_u8.argtypes = [_vp, _vp]
+    L.gol_fetch_i32.argtypes = [_vp, _vp]
+    L.gol_fetch_words.argtypes = [_vp, _vp, _u32]
+    L.gol_performed.argtypes = [_vp]
+    L.gol_performed.restype = _u64
+    L.gol_destroy.argtypes = [_vp]
+    L.gol_destroy.restype = None
+    L.gol_last_error.argtypes = [_vp]
+    L.gol_last_error.restype = ctypes.c_char_p
+    L.gol_device_grid.argtypes = [_vp]
+    L.gol_device_grid.restype = _vp
+    L.gol_stream.argtypes = [_vp]
+    L.gol_stream.restype = _vp
+    L.gol_plan.argtypes = [_vp, ctypes.POINTER(_u32), ctypes.POINTER(_u32), ctypes.POINTER(_u32)]
+    L.gol_rows_pass.argtypes = [_vp, _vp, _u64, _u64, _u32, _u32, _vp]
+    L.gol_pack_cells_device.argtypes = [_vp, _vp, _u64, _u64, _vp]
+    L.gol_unpack_cells_device.argtypes = [_vp, _vp, _u64, _u64, _vp]
+    L.gol_load_random_ones_zeros.argtypes = [_vp, _u64, _u64, _u64]
+    L.gol_probe_int_peak.argtypes = [ctypes.POINTER(ctypes.c_double), _vp]
+    L.gol_abi_version.restype = ctypes.c_int
+    L.gol_build_info.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def declared_symbols() -> list[str]:
+    """Function names declared in include/gol_b200.h."""
+    import re
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(gol_[a-z0-9_]+)\s*\(", text)))
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_vp)
+
+
+@dataclass
+class ExperimentParams:
+    """The ExperimentParams fields the hot path reads
+    (src/infrastructure/experiment_params.hpp:21-116)."""
+    grid_dimensions: tuple = (0, 0)
+    iterations: int = 0
+    max_runtime_seconds: int = 0          # 0 = unlimited
+    state_bits_count: int = 64            # word width of the packed layout
+    thread_block_size: int = 0            # rows per CTA band (0 = auto)
+    temporal_steps: int = 0               # k (0 = auto)
+    algorithm: str = "auto"
+    device: int = 0
+    stream: int | None = None             # cudaStream_t as an integer
+    extra: dict = field(default_factory=dict)
+
+
+class GolB200:
+    """One grid advanced on the GPU, behind the reference's phase contract."""
+
+    def __init__(self, params: ExperimentParams | None = None, **kw):
+        self._e = _vp()
+        self._cells_dtype = np.uint8
+        self.params = params or ExperimentParams(**kw)
+        self._create()
+
+    # -- Algorithm::set_params (algorithm.hpp:76-78) -----------------------
+    def set_params(self, params: ExperimentParams) -> None:
+        self.close()
+        self.params = params
+        self._create()
+
+    def _create(self) -> None:
+        p = self.params
+        x, y = (int(v) for v in p.grid_dimensions)
+        cfg = GolConfig()
+        lib().gol_config_init(ctypes.byref(cfg), x, y)
+        cfg.algorithm = ALGORITHMS[p.algorithm]
+        cfg.word_bits = int(p.state_bits_count)
+        cfg.temporal_steps = int(p.temporal_steps)
+        cfg.thread_block_size = int(p.thread_block_size)
+        cfg.max_runtime_seconds = int(p.max_runtime_seconds)
+        cfg.device = int(p.device)
+        cfg.stream = p.stream
+        rc = lib().gol_create(ctypes.byref(self._e), ctypes.byref(cfg))
+        if rc != GOL_OK:
+            raise RuntimeError(f"gol_create: {lib().gol_last_error(None).decode()} ({rc})")
+        self.x, self.y = x, y
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != GOL_OK:
+            msg = lib().gol_last_error(self._e).decode()
+            raise RuntimeError(f"{what}: {msg} (status {rc})")
+
+    # -- the contract --------------------------------------------------------
+    def set_and_format_input_data(self, grid: np.ndarray) -> None:
+        g = np.ascontiguousarray(grid)
+        if g.shape != (self.y, self.x):
+            raise RuntimeError(f"grid shape {g.shape} != ({self.y}, {self.x})")
+        if g.dtype == np.int32:
+            self._cells_dtype = np.int32
+            self._check(lib().gol_set_input_i32(self._e, _ptr(g), self.x, self.y), "set_input")
+        else:
+            self._cells_dtype = np.uint8
+            g = g.astype(np.uint8, copy=False)
+            self._check(lib().gol_set_input_u8(self._e, _ptr(g), self.x, self.y), "set_input")
+
+    def set_input_words(self, words: np.ndarray, word_bits: int = 64) -> None:
+        w = np.ascontiguousarray(words)
+        self._check(lib().gol_set_input_words(self._e, _ptr(w), self.x, self.y, word_bits),
+                    "set_input_words")
+
+    def initialize_data_structures(self) -> None:
+        self._check(lib().gol_init(self._e), "initialize")
+
+    def run(self, iterations: int) -> None:
+        self._check(lib().gol_run(self._e, int(iterations)), "run")
+
+    def sync(self) -> None:
+        self._check(lib().gol_sync(self._e), "sync")
+
+    def finalize_data_structures(self) -> None:
+        self._check(lib().gol_finalize(self._e), "finalize")
+
+    def fetch_result(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((self.y, self.x), dtype=self._cells_dtype)
+        if out.dtype == np.int32:
+            self._check(lib().gol_fetch_i32(self._e, _ptr(out)), "fetch")
+        else:
+            self._check(lib().gol_fetch_u8(self._e, _ptr(out)), "fetch")
+        return out
+
+    def fetch_words(self, word_bits: int = 64) -> np.ndarray:
+        dt = np.uint64 if word_bits == 64 else np.uint32
+        out = np.empty((self.y, self.x // word_bits), dtype=dt)
+        self._check(lib().gol_fetch_words(self._e, _ptr(out), word_bits), "fetch_words")
+        return out
+
+    def actually_performed_iterations(self) -> int:
+        return int(lib().gol_performed(self._e))
+
+    # -- device-resident access ---------------------------------------------
+    def device_grid_ptr(self) -> int:
+        return int(lib().gol_device_grid(self._e) or 0)
+
+    def stream_ptr(self) -> int:
+        return int(lib().gol_stream(self._e) or 0)
+
+    def plan(self) -> dict:
+        k, b, w = _u32(), _u32(), _u32()
+        self._check(lib().gol_plan(self._e, ctypes.byref(k), ctypes.byref(b), ctypes.byref(w)),
+                    "plan")
+        return {"temporal_steps": k.value, "band_rows": b.value, "words_per_lane": w.value}
+
+    def close(self) -> None:
+        if self._e:
+            lib().gol_destroy(self._e)
+            self._e = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def run_generations(cells: np.ndarray, iterations: int, **kw) -> np.ndarray:
+    """Whole contract in one call: cells (uint8/int32 [y, x]) in, cells out."""
+    y, x = cells.shape
+    with GolB200(grid_dimensions=(x, y), **kw) as alg:
+        alg.set_and_format_input_data(cells)
+        alg.initialize_data_structures()
+        alg.run(iterations)
+        alg.finalize_data_structures()
+        return alg.fetch_result()
+
+
+def load_random_ones_zeros(x: int, y: int, seed: int) -> np.ndarray:
+    """RandomOnesZerosDataLoader: uint8[y, x] of 0/1 from std::mt19937(seed)."""
+    out = np.empty((y, x), dtype=np.uint8)
+    rc = lib().gol_load_random_ones_zeros(_ptr(out), x, y, seed)
+    if rc != GOL_OK:
+        raise RuntimeError(f"gol_load_random_ones_zeros failed with status {rc}")
+    return out
+
+
+def probe_int_peak(stream: int = 0) -> float:
+    """Measured 32-bit LOP3 lane-ops/s of the current device."""
+    v = ctypes.c_double()
+    rc = lib().gol_probe_int_peak(ctypes.byref(v), stream)
+    if rc != GOL_OK:
+        raise RuntimeError(f"gol_probe_int_peak failed with status {rc}")
+    return v.value
+
+
+def rows_pass(d_src: int, d_dst: int, x: int, y: int, k: int, band_rows: int = 0,
+              stream: int = 0) -> None:
+    rc = lib().gol_rows_pass(d_src, d_dst, x, y, k, band_rows, stream)
+    if rc != GOL_OK:
+        raise RuntimeError(f"gol_rows_pass failed with status {rc}")
+
+
+def pack_cells_device(d_cells: int, d_words: int, x: int, y: int, stream: int = 0) -> None:
+    rc = lib().gol_pack_cells_device(d_cells, d_words, x, y, stream)
+    if rc != GOL_OK:
+        raise RuntimeError(f"gol_pack_cells_device failed with status {rc}")
+
+
+def unpack_cells_device(d_words: int, d_cells: int, x: int, y: int, stream: int = 0) -> None:
+    rc = lib().gol_unpack_cells_device(d_words, d_cells, x, y, stream)
+    if rc != GOL_OK:
+        raise RuntimeError(f"gol_unpack_cells_device failed with status {rc}")
