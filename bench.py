@@ -57,8 +57,8 @@ ALG_INT_OPS_PER_CELL = 33.0 / 64.0
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--size", type=int, default=SIZE)
     ap.add_argument("--gens", type=int, default=GENS)
@@ -136,6 +136,14 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def wait_first_sample(self, timeout_s: float = 5.0):
+        t0 = time.time()
+        while self.proc and not self.lines and time.time() - t0 < timeout_s:
+            time.sleep(0.02)
+
+    def reset(self):
+        self.lines.clear()
+
     def stop(self) -> dict:
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -185,15 +193,19 @@ def cpu_baseline(grid: np.ndarray, target_s: float = 10.0) -> dict:
     run, kind, what = reference_runner()
     y, x = grid.shape
     t0 = time.perf_counter()
-    run(grid, 2)
-    dt = max(time.perf_counter() - t0, 1e-3)
-    gens = int(max(2, min(GENS, 2 * target_s / dt)))
+    run(grid, 1)
+    t1 = time.perf_counter()
+    run(grid, 3)
+    t2 = time.perf_counter()
+    per_gen = max((t2 - t1) - (t1 - t0), 1e-3) / 2.0     # minus the fixed pack/unpack cost
+    gens = int(max(2, min(GENS, target_s / per_gen)))
     t0 = time.perf_counter()
     run(grid, gens)
     dt = time.perf_counter() - t0
     return {"value": x * y * gens / dt / 1e9, "unit": UNIT, "cores": 1, "kind": kind,
-            "sample": f"{x}x{y} seed {SEED}, {gens} generations, single thread ({what}); "
-                      "the reference CPU path is single-threaded"}
+            "sample": f"{x}x{y} seed {SEED}, {gens} generations ({dt:.1f} s incl. the reference's "
+                      f"pack/unpack phases), single thread ({what}); the reference CPU path is "
+                      "single-threaded"}
 
 
 def run_reference_arm(args, d: Dist) -> None:
@@ -327,14 +339,16 @@ def run_ours(args, d: Dist) -> None:
     # -- headline: device-resident timed steps -------------------------------
     e = make_engine(best_k)
     plan = e.plan()
+    clocks = ClockSampler(d.local_rank)
+    clocks.start()
     for _ in range(args.warmup):
         e.run(gens)
         flush.zero_()
     torch.cuda.synchronize()
+    clocks.wait_first_sample()
+    clocks.reset()
     d.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(d.local_rank)
-    clocks.start()
     step_ms = []
     for _ in range(args.steps):
         step_ms.append(timed_run(e, gens))
@@ -465,6 +479,7 @@ def run_ours(args, d: Dist) -> None:
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": grid_bytes, "d2h_bytes_per_step": grid_bytes,
                     "phases_ms_median": {k: statistics.median(v) for k, v in phases.items()},
+                    "step_ms": [round(t * 1e3, 2) for t in e2e_times],
                     "path": "gol_set_input_u8 -> gol_init -> gol_run -> gol_finalize -> "
                             "gol_fetch_u8 (C ABI, host uint8 grid in and out)"},
             "gpu_launches": passes * args.steps,

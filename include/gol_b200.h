@@ -77,7 +77,7 @@ typedef struct gol_config {
     uint32_t tile_rows;             /* change-tracking tile height (0 = auto)    */
     uint64_t max_runtime_seconds;   /* 0 = unlimited                             */
     int32_t device;                 /* CUDA device ordinal                       */
-    uint32_t reserved;
+    uint32_t lane_words;            /* 32-bit words per lane: 1, 2, 4 (0 = auto) */
     void* stream;                   /* cudaStream_t to use; NULL = own stream    */
 } gol_config;
 
@@ -148,6 +148,9 @@ int gol_plan(const gol_engine* e, uint32_t* temporal_steps, uint32_t* band_rows,
  * Asynchronous on `stream`. */
 int gol_rows_pass(const void* d_src, void* d_dst, uint64_t x, uint64_t y, uint32_t k,
                   uint32_t band_rows, void* stream);
+/* Same with the lane width forced (lane_words 1, 2 or 4; 0 = auto). */
+int gol_rows_pass_ex(const void* d_src, void* d_dst, uint64_t x, uint64_t y, uint32_t k,
+                     uint32_t band_rows, uint32_t lane_words, void* stream);
 
 /* Packs / unpacks a device cell grid (uint8, nonzero = alive) to / from
  * device row words. x % 32 == 0. */

@@ -121,7 +121,7 @@ int ensure_host(gol_engine* e) {
 int launch_pass(gol_engine* e, int k, cudaStream_t s, int from) {
     RowsPlan p = e->plan;
     if (k != e->k) {
-        if (!golb200::plan_rows(e->W, e->Y, k, (int)e->cfg.thread_block_size,
+        if (!golb200::plan_rows(e->W, e->Y, k, (int)e->cfg.thread_block_size, 0,
                                 golb200::device_sm_count(e->cfg.device), &p))
             return e->fail(GOL_E_UNSUPPORTED, "no kernel plan for this width and depth");
     }
@@ -194,6 +194,11 @@ int gol_create(gol_engine** out, const gol_config* cfg) {
     }
     if (cfg->temporal_steps > (uint32_t)golb200::kMaxTemporalSteps) {
         g_create_error = "temporal_steps must be at most 16";
+        return GOL_E_INVALID;
+    }
+    if (cfg->lane_words != 0 && cfg->lane_words != 1 && cfg->lane_words != 2 &&
+        cfg->lane_words != 4) {
+        g_create_error = "lane_words must be 0, 1, 2 or 4";
         return GOL_E_INVALID;
     }
     if (cfg->algorithm > GOL_ALG_LOCAL) {
@@ -277,7 +282,8 @@ int gol_init(gol_engine* e) {
     int k = (int)e->cfg.temporal_steps;
     if (k <= 0) k = 4;
     const int sms = golb200::device_sm_count(e->cfg.device);
-    if (!golb200::plan_rows(e->W, e->Y, k, (int)e->cfg.thread_block_size, sms, &e->plan))
+    if (!golb200::plan_rows(e->W, e->Y, k, (int)e->cfg.thread_block_size,
+                            (int)e->cfg.lane_words, sms, &e->plan))
         return e->fail(GOL_E_UNSUPPORTED, "no kernel plan for this width and depth");
     e->k = k;
     const size_t bytes = (size_t)e->W * e->Y * sizeof(uint32_t);
@@ -422,13 +428,18 @@ int gol_plan(const gol_engine* e, uint32_t* temporal_steps, uint32_t* band_rows,
 
 int gol_rows_pass(const void* d_src, void* d_dst, uint64_t x, uint64_t y, uint32_t k,
                   uint32_t band_rows, void* stream) {
+    return gol_rows_pass_ex(d_src, d_dst, x, y, k, band_rows, 0, stream);
+}
+
+int gol_rows_pass_ex(const void* d_src, void* d_dst, uint64_t x, uint64_t y, uint32_t k,
+                     uint32_t band_rows, uint32_t lane_words, void* stream) {
     if (!d_src || !d_dst || x % 32 || k < 1 || k > (uint32_t)golb200::kMaxTemporalSteps)
         return GOL_E_INVALID;
     if (x / 32 > (uint64_t)1 << 30 || y > (uint64_t)1 << 30) return GOL_E_INVALID;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return GOL_E_CUDA;
     RowsPlan p;
-    if (!golb200::plan_rows((int)(x / 32), (int)y, (int)k, (int)band_rows,
+    if (!golb200::plan_rows((int)(x / 32), (int)y, (int)k, (int)band_rows, (int)lane_words,
                             golb200::device_sm_count(dev), &p))
         return GOL_E_UNSUPPORTED;
     cudaError_t ce = golb200::launch_rows_pass(static_cast<const uint32_t*>(d_src),

@@ -25,8 +25,9 @@ struct RowsPlan {
 };
 
 // Picks words-per-lane and CTA shape for a W-word by Y-row grid and depth k.
-// Returns false only for k outside 1..16.
-bool plan_rows(int W, int Y, int k, int band_rows, int num_sms, RowsPlan* plan);
+// wpl = 0 chooses the widest lane access whose rings fit k; 1, 2 or 4 forces
+// it. Returns false for k outside 1..16 or a wpl that W or k rules out.
+bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPlan* plan);
 
 // One pass of k generations (1 <= k <= kMaxKForWpl(plan.wpl)).
 cudaError_t launch_rows_pass(const uint32_t* src, uint32_t* dst, int W, int Y, int k,

@@ -35,17 +35,20 @@ int device_sm_count(int device) {
     return n > 0 ? n : 148;
 }
 
-bool plan_rows(int W, int Y, int k, int band_rows, int num_sms, RowsPlan* plan) {
+bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPlan* plan) {
     if (k < 1 || k > kMaxTemporalSteps || W <= 0) return false;
-    // Widest lane access whose register rings fit this depth.
-    int wpl = 0;
-    for (int cand : {4, 2, 1}) {
-        if (W % cand == 0 && k <= kMaxKForWpl(cand)) {
-            wpl = cand;
-            break;
+    if (wpl != 0) {
+        if ((wpl != 1 && wpl != 2 && wpl != 4) || W % wpl || k > kMaxKForWpl(wpl)) return false;
+    } else {
+        // Widest lane access whose register rings fit this depth.
+        for (int cand : {4, 2, 1}) {
+            if (W % cand == 0 && k <= kMaxKForWpl(cand)) {
+                wpl = cand;
+                break;
+            }
         }
+        if (wpl == 0) return false;
     }
-    if (wpl == 0) return false;
     plan->wpl = wpl;
     const int lanes = W / wpl;
     if (lanes <= kTemporalMaxThreads) {

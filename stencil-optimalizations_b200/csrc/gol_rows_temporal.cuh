@@ -27,9 +27,12 @@
 //     a tiny shared-memory "edge" table (first/last word of each warp's
 //     span, per stage, double-buffered by step parity). One __syncthreads
 //     per step publishes them.
+//   * Warm-up and drain steps test which stages are active and mask rows
+//     outside the grid; the steady-state steps between them run a branch-
+//     free body, so a step is one basic block whose K stages interleave.
 //
-// Ring indices depend on the step number mod 6, so the step body is a
-// template on that phase and the loop is unrolled by 6: all ring accesses
+// Ring indices depend on the step number mod 3, so the step body is a
+// template on that phase and the loop is unrolled by 3: all ring accesses
 // are compile-time register names, no moves.
 #pragma once
 
@@ -40,6 +43,9 @@
 namespace golb200 {
 
 constexpr int kTemporalMaxThreads = 256;
+#ifndef GOL_TEMPORAL_MIN_BLOCKS
+#define GOL_TEMPORAL_MIN_BLOCKS 1   // CTAs per SM the register budget is sized for
+#endif
 
 struct RowsLaunch {
     const uint32_t* src;   // gen-0 grid, W words per row, Y rows
@@ -80,39 +86,45 @@ struct TemporalRegs {
     uint32_t ld[3][WPL];          // stage-0 rows, slot = step % 3
     uint32_t h0[K][3][WPL];       // stage g's horizontal sums, bit plane 0
     uint32_t h1[K][3][WPL];       //                            bit plane 1
-    uint32_t o[K][2][WPL];        // stage g's output rows, slot = step % 2
+    uint32_t o[K][3][WPL];        // stage g's output rows, slot = step % 3
 };
+
+// Edge table layout: [EW padded warps][K producer stages][3 step slots]
+// [2 sides], then one dummy entry per warp. Every lane's read/write base is
+// loop-invariant and each stage/slot offset is a compile-time immediate.
+// Padded warps 0 and EW-1 stay zero: the dead cells beyond the CTA's
+// outermost words. Lanes 1..30 write their (unused) edge words to their
+// warp's dummy entry, so publishing needs no branch.
+__host__ __device__ constexpr int edge_off(int g, int slot) { return (g * 3 + slot) * 2; }
 
 struct TemporalCtx {
     const uint32_t* src;
     uint32_t* dst;
-    uint32_t* edges;   // [K][2][EW][2]
+    const uint32_t* erd;   // lane 0: left warp's side-1 entry; lane 31: right warp's side-0
+    uint32_t* ewr;         // lane 0 / 31: this warp's entry, side 0 / 1; others: dummy word
+    bool first_lane, last_lane;
     int W, Y, y0, y1, B;
-    int lane, warp, EW, base;
+    int lane, base;
     bool lane_ok;   // this lane's words lie inside the grid
     bool own;       // ... and inside this CTA's slice (not halo): stored
 };
 
-// Publishes the first and last word of this warp's span of a row.
-__device__ __forceinline__ void publish_edges(const TemporalCtx& c, uint32_t* slot, uint32_t first,
-                                              uint32_t last) {
-    if (c.lane == 0) slot[(c.warp + 1) * 2 + 0] = first;
-    if (c.lane == 31) slot[(c.warp + 1) * 2 + 1] = last;
-}
-
-template <int WPL, int K, int PH>
-__device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const TemporalCtx& c, int i) {
+// Step body. FAST = steady state: every stage active, every row inside the
+// grid, so no activity tests or row masks (the whole step is one basic
+// block and the K stages' independent chains interleave). LMASK forces the
+// out-of-grid lanes of a partial CTA to stay dead.
+template <int WPL, int K, int PH, bool FAST, bool LMASK>
+__device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const TemporalCtx& c, int i,
+                                              uint32_t lane_mask) {
     constexpr int NEW3 = PH % 3;          // ring-of-3 slot written at this step
     constexpr int PREV3 = (PH + 2) % 3;   // ... written one step ago
     constexpr int OLD3 = (PH + 1) % 3;    // ... written two steps ago
-    constexpr int NEW2 = PH % 2;
-    constexpr int PREV2 = (PH + 1) % 2;
 
     // Stages run high to low so that stage g reads stage g-1's rows from the
     // previous steps before stage g-1 overwrites its ring slot.
 #pragma unroll
     for (int g = K; g >= 1; --g) {
-        if (i >= 3 * g - 2 && i <= c.B + 2 * K + g - 1) {
+        if (FAST || (i >= 3 * g - 2 && i <= c.B + 2 * K + g - 1)) {
             // Intake row P (gen g-1, row r+1) and centre row C (gen g-1, row r).
             uint32_t P[WPL], C[WPL];
 #pragma unroll
@@ -121,17 +133,16 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
                     P[w] = s.ld[PREV3][w];
                     C[w] = s.ld[OLD3][w];
                 } else {
-                    P[w] = s.o[g - 2][PREV2][w];
-                    C[w] = s.o[g - 2][NEW2][w];
+                    P[w] = s.o[g - 2][PREV3][w];
+                    C[w] = s.o[g - 2][OLD3][w];
                 }
             }
             // Words just left and right of this lane's span.
             uint32_t lw = __shfl_up_sync(0xffffffffu, P[WPL - 1], 1);
             uint32_t rw = __shfl_down_sync(0xffffffffu, P[0], 1);
-            const uint32_t* e = c.edges + ((g - 1) * 2 + PREV2) * c.EW * 2;
-            const uint32_t ev = e[c.lane == 0 ? (c.warp * 2 + 1) : ((c.warp + 2) * 2 + 0)];
-            if (c.lane == 0) lw = ev;
-            if (c.lane == 31) rw = ev;
+            const uint32_t ev = c.erd[edge_off(g - 1, PREV3)];
+            lw = c.first_lane ? ev : lw;
+            rw = c.last_lane ? ev : rw;
 #pragma unroll
             for (int w = 0; w < WPL; ++w) {
                 const uint32_t l = (w == 0) ? lw : P[w - 1];
@@ -140,31 +151,35 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
             }
             // Output row r of gen g (garbage during warm-up, never consumed).
             const int row = c.y0 - K + i - 2 * g;
-            const uint32_t keep = (c.lane_ok && (unsigned)row < (unsigned)c.Y) ? 0xffffffffu : 0u;
+            uint32_t keep = lane_mask;
+            if (!FAST) keep = (c.lane_ok && (unsigned)row < (unsigned)c.Y) ? 0xffffffffu : 0u;
             uint32_t res[WPL];
 #pragma unroll
             for (int w = 0; w < WPL; ++w) {
                 res[w] = next_word(s.h0[g - 1][OLD3][w], s.h1[g - 1][OLD3][w],
                                    s.h0[g - 1][PREV3][w], s.h1[g - 1][PREV3][w],
-                                   s.h0[g - 1][NEW3][w], s.h1[g - 1][NEW3][w], C[w]) &
-                         keep;
+                                   s.h0[g - 1][NEW3][w], s.h1[g - 1][NEW3][w], C[w]);
+                if (!FAST || LMASK) res[w] &= keep;
             }
             if (g == K) {
-                if (row >= c.y0 && row < c.y1 && c.own)
+                if ((FAST || (row >= c.y0 && row < c.y1)) && c.own)
                     store_words<WPL>(c.dst + (size_t)row * c.W + c.base, res);
             } else {
 #pragma unroll
-                for (int w = 0; w < WPL; ++w) s.o[g - 1][NEW2][w] = res[w];
-                publish_edges(c, c.edges + ((g * 2) + NEW2) * c.EW * 2, res[0], res[WPL - 1]);
+                for (int w = 0; w < WPL; ++w) s.o[g - 1][NEW3][w] = res[w];
+                c.ewr[edge_off(g, NEW3)] = c.last_lane ? res[WPL - 1] : res[0];
             }
         }
     }
 
     // Stage 0: publish this step's loaded row, prefetch the next one.
-    if (i <= c.B + 2 * K - 1) {
-        publish_edges(c, c.edges + NEW2 * c.EW * 2, s.ld[NEW3][0], s.ld[NEW3][WPL - 1]);
+    if (FAST || i <= c.B + 2 * K - 1) {
+        c.ewr[edge_off(0, NEW3)] = c.last_lane ? s.ld[NEW3][WPL - 1] : s.ld[NEW3][0];
         const int nrow = c.y0 - K + i + 1;
-        if (i + 1 <= c.B + 2 * K - 1 && c.lane_ok && (unsigned)nrow < (unsigned)c.Y) {
+        if (FAST) {
+            if (!LMASK || c.lane_ok)
+                load_words<WPL>(c.src + (size_t)nrow * c.W + c.base, s.ld[(PH + 1) % 3]);
+        } else if (i + 1 <= c.B + 2 * K - 1 && c.lane_ok && (unsigned)nrow < (unsigned)c.Y) {
             load_words<WPL>(c.src + (size_t)nrow * c.W + c.base, s.ld[(PH + 1) % 3]);
         } else {
 #pragma unroll
@@ -174,28 +189,47 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
     __syncthreads();
 }
 
+template <int WPL, int K, bool FAST, bool LMASK>
+__device__ __forceinline__ void temporal_steps(TemporalRegs<WPL, K>& s, const TemporalCtx& c,
+                                               int i0, int i1, uint32_t lane_mask) {
+    for (int i = i0; i < i1; i += 3) {
+        temporal_step<WPL, K, 0, FAST, LMASK>(s, c, i + 0, lane_mask);
+        temporal_step<WPL, K, 1, FAST, LMASK>(s, c, i + 1, lane_mask);
+        temporal_step<WPL, K, 2, FAST, LMASK>(s, c, i + 2, lane_mask);
+    }
+}
+
 template <int WPL, int K>
-__global__ void __launch_bounds__(kTemporalMaxThreads)
+__global__ void __launch_bounds__(kTemporalMaxThreads, GOL_TEMPORAL_MIN_BLOCKS)
 rows_temporal_kernel(RowsLaunch a) {
     extern __shared__ uint32_t edges[];
+    constexpr int ESTRIDE = K * 6;            // words per padded-warp entry
     TemporalCtx c;
     c.src = a.src;
     c.dst = a.dst;
-    c.edges = edges;
     c.W = a.W;
     c.Y = a.Y;
     c.y0 = blockIdx.x * a.band;
     c.y1 = min(c.y0 + a.band, a.Y);
     c.B = c.y1 - c.y0;
     c.lane = threadIdx.x & 31;
-    c.warp = threadIdx.x >> 5;
-    c.EW = (blockDim.x >> 5) + 2;
+    const int warp = threadIdx.x >> 5;
+    const int EW = (blockDim.x >> 5) + 2;
+    c.first_lane = c.lane == 0;
+    c.last_lane = c.lane == 31;
+    c.erd = edges + (c.first_lane ? warp * ESTRIDE + 1 : (warp + 2) * ESTRIDE);
+    c.ewr = (c.first_lane || c.last_lane)
+                ? edges + (warp + 1) * ESTRIDE + (c.last_lane ? 1 : 0)
+                : edges + (EW + warp) * ESTRIDE;
     const int xs = blockIdx.y * a.slice;
-    c.base = xs - a.halo + (int)threadIdx.x * WPL;
+    const int x0 = xs - a.halo;
+    c.base = x0 + (int)threadIdx.x * WPL;
     c.lane_ok = c.base >= 0 && c.base < a.W;
     c.own = c.lane_ok && c.base >= xs && c.base < xs + a.slice;
+    const bool all_lanes_ok = x0 >= 0 && x0 + (int)blockDim.x * WPL <= a.W;
+    const uint32_t lane_mask = c.lane_ok ? 0xffffffffu : 0u;
 
-    for (int t = threadIdx.x; t < K * 2 * c.EW * 2; t += blockDim.x) edges[t] = 0u;
+    for (int t = threadIdx.x; t < EW * ESTRIDE; t += blockDim.x) edges[t] = 0u;
 
     TemporalRegs<WPL, K> s;
 #pragma unroll
@@ -205,7 +239,7 @@ rows_temporal_kernel(RowsLaunch a) {
         for (int g = 0; g < K; ++g) {
             s.h0[g][0][w] = s.h0[g][1][w] = s.h0[g][2][w] = 0u;
             s.h1[g][0][w] = s.h1[g][1][w] = s.h1[g][2][w] = 0u;
-            s.o[g][0][w] = s.o[g][1][w] = 0u;
+            s.o[g][0][w] = s.o[g][1][w] = s.o[g][2][w] = 0u;
         }
     }
     const int row0 = c.y0 - K;
@@ -213,20 +247,29 @@ rows_temporal_kernel(RowsLaunch a) {
         load_words<WPL>(c.src + (size_t)row0 * c.W + c.base, s.ld[0]);
     __syncthreads();
 
+    // Steps [f0, f1) run the steady-state body: all stages active (i >= 3K),
+    // the next load row exists (i + 1 <= B + 2K - 1) and lies inside the grid
+    // (y0 - K + i + 1 < Y), so no row computed there leaves the grid.
+    // Segment bounds are multiples of 3 to keep the ring phases aligned.
     const int nsteps = c.B + 3 * K;
-    for (int i = 0; i < nsteps; i += 6) {
-        temporal_step<WPL, K, 0>(s, c, i + 0);
-        temporal_step<WPL, K, 1>(s, c, i + 1);
-        temporal_step<WPL, K, 2>(s, c, i + 2);
-        temporal_step<WPL, K, 3>(s, c, i + 3);
-        temporal_step<WPL, K, 4>(s, c, i + 4);
-        temporal_step<WPL, K, 5>(s, c, i + 5);
+    const int f0 = 3 * K;
+    const int f1 = min(c.B + 2 * K - 1, c.Y - c.y0 + K - 1);
+    const int fast_end = f1 > f0 ? f0 + (f1 - f0) / 3 * 3 : f0;
+    if (fast_end > f0) {
+        temporal_steps<WPL, K, false, false>(s, c, 0, f0, lane_mask);
+        if (all_lanes_ok)
+            temporal_steps<WPL, K, true, false>(s, c, f0, fast_end, lane_mask);
+        else
+            temporal_steps<WPL, K, true, true>(s, c, f0, fast_end, lane_mask);
+        temporal_steps<WPL, K, false, false>(s, c, fast_end, nsteps, lane_mask);
+    } else {
+        temporal_steps<WPL, K, false, false>(s, c, 0, nsteps, lane_mask);
     }
 }
 
-// Shared memory a launch needs for its edge table.
+// Shared memory a launch needs: the edge table plus one dummy entry per warp.
 __host__ __device__ inline size_t temporal_smem_bytes(int K, int threads) {
-    return (size_t)K * 2 * ((threads >> 5) + 2) * 2 * sizeof(uint32_t);
+    return (size_t)(2 * (threads >> 5) + 2) * K * 6 * sizeof(uint32_t);
 }
 
 } // namespace golb200

@@ -20,7 +20,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libgolb200.so")
+LIB_PATH = os.environ.get("GOLB200_LIB") or os.path.join(HERE, "libgolb200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "gol_b200.h")
 
 GOL_OK = 0
@@ -45,7 +45,7 @@ class GolConfig(ctypes.Structure):
         ("tile_rows", ctypes.c_uint32),
         ("max_runtime_seconds", ctypes.c_uint64),
         ("device", ctypes.c_int32),
-        ("reserved", ctypes.c_uint32),
+        ("lane_words", ctypes.c_uint32),
         ("stream", ctypes.c_void_p),
     ]
 
@@ -91,6 +91,7 @@ def lib():
     L.gol_stream.restype = _vp
     L.gol_plan.argtypes = [_vp, ctypes.POINTER(_u32), ctypes.POINTER(_u32), ctypes.POINTER(_u32)]
     L.gol_rows_pass.argtypes = [_vp, _vp, _u64, _u64, _u32, _u32, _vp]
+    L.gol_rows_pass_ex.argtypes = [_vp, _vp, _u64, _u64, _u32, _u32, _u32, _vp]
     L.gol_pack_cells_device.argtypes = [_vp, _vp, _u64, _u64, _vp]
     L.gol_unpack_cells_device.argtypes = [_vp, _vp, _u64, _u64, _vp]
     L.gol_load_random_ones_zeros.argtypes = [_vp, _u64, _u64, _u64]
@@ -122,6 +123,7 @@ class ExperimentParams:
     state_bits_count: int = 64            # word width of the packed layout
     thread_block_size: int = 0            # rows per CTA band (0 = auto)
     temporal_steps: int = 0               # k (0 = auto)
+    lane_words: int = 0                   # 32-bit words per lane (0 = auto)
     algorithm: str = "auto"
     device: int = 0
     stream: int | None = None             # cudaStream_t as an integer
@@ -151,6 +153,7 @@ class GolB200:
         cfg.algorithm = ALGORITHMS[p.algorithm]
         cfg.word_bits = int(p.state_bits_count)
         cfg.temporal_steps = int(p.temporal_steps)
+        cfg.lane_words = int(p.lane_words)
         cfg.thread_block_size = int(p.thread_block_size)
         cfg.max_runtime_seconds = int(p.max_runtime_seconds)
         cfg.device = int(p.device)
@@ -274,8 +277,8 @@ def probe_int_peak(stream: int = 0) -> float:
 
 
 def rows_pass(d_src: int, d_dst: int, x: int, y: int, k: int, band_rows: int = 0,
-              stream: int = 0) -> None:
-    rc = lib().gol_rows_pass(d_src, d_dst, x, y, k, band_rows, stream)
+              stream: int = 0, lane_words: int = 0) -> None:
+    rc = lib().gol_rows_pass_ex(d_src, d_dst, x, y, k, band_rows, lane_words, stream)
     if rc != GOL_OK:
         raise RuntimeError(f"gol_rows_pass failed with status {rc}")
 
