@@ -107,7 +107,9 @@ int gol_run(gol_engine* e, uint64_t n);
 /* Waits for the engine's queued device work. */
 int gol_sync(gol_engine* e);
 
-/* finalize_data_structures: waits, copies the grid back, frees device memory. */
+/* finalize_data_structures: waits and copies the grid back. The engine keeps
+ * its two device grids (and captured graphs) for the next round; gol_destroy
+ * frees them. */
 int gol_finalize(gol_engine* e);
 
 /* fetch_result: unpacks the finalized grid into the caller's buffer. */
@@ -131,6 +133,16 @@ const char* gol_last_error(const gol_engine* e);
  * cell, raster order (cells[cy*x + cx]). Host only. */
 int gol_load_random_ones_zeros(uint8_t* cells, uint64_t x, uint64_t y, uint64_t seed);
 
+/* Sparse/settling input: all dead except floor(S * fraction) of the S
+ * aligned patch-by-patch slots, filled with Bernoulli(density) cells. The
+ * draw order is fixed (std::mt19937_64(seed); Fisher-Yates over slot
+ * indices, j = rng() % (i+1) from the back; chosen slots sorted; cells of
+ * each chosen slot row by row, alive iff (rng() >> 11) * 2^-53 < density).
+ * x, y multiples of patch. Returns the number of filled slots (>= 0) or
+ * GOL_E_INVALID. Host only. */
+int gol_load_sparse_patches(uint8_t* cells, uint64_t x, uint64_t y, uint64_t seed, uint32_t patch,
+                            double fraction, double density);
+
 /* --- Device-resident access (between gol_init and gol_finalize) ---------- */
 
 /* Device pointer to the current grid (x/32 uint32 words per row). */
@@ -140,6 +152,14 @@ void* gol_stream(gol_engine* e);
 /* Temporal depth and band height gol_run uses (after gol_init). */
 int gol_plan(const gol_engine* e, uint32_t* temporal_steps, uint32_t* band_rows,
              uint32_t* words_per_lane);
+
+/* Change-tracking census of the last gol_run with GOL_ALG_LOCAL (the
+ * reference's --collect-touched-tiles-stats, cuda_local_one_cell.hpp:61-71,
+ * 186-289): passes run, tiles per pass, tiles computed over all passes, and
+ * up to max_entries per-pass computed-tile counts (the rest untouched: this
+ * engine never copies skipped tiles). Synchronizes the engine's stream. */
+int gol_local_stats(gol_engine* e, uint64_t* passes, uint64_t* tiles_per_pass,
+                    uint64_t* computed_total, uint32_t* per_pass, uint64_t max_entries);
 
 /* --- Stateless device entry points -------------------------------------- */
 

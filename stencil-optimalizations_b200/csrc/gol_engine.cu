@@ -1,6 +1,7 @@
 // The engine behind include/gol_b200.h: the reference's Algorithm phase
 // contract (src/infrastructure/algorithm.hpp:17-87) over device-resident,
 // row-packed grids, advanced by the temporal row-band kernel.
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -48,6 +49,14 @@ struct gol_engine {
 
     int k = 1;
     RowsPlan plan{};
+
+    // change tracking (GOL_ALG_LOCAL)
+    bool local = false;
+    golb200::LocalPlan lplan{};
+    golb200::LocalState lst{};
+    int lparity = 0;                       // pass parity of the change flags
+    cudaGraphExec_t lchunk[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [cur][lparity]
+
     std::string err;
 
     int fail(int code, const std::string& msg) {
@@ -67,15 +76,62 @@ void release_graphs(gol_engine* e) {
         if (g) cudaGraphExecDestroy(g);
         g = nullptr;
     }
+    for (auto& row : e->lchunk)
+        for (auto& g : row) {
+            if (g) cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+void release_local(gol_engine* e) {
+    golb200::LocalState& s = e->lst;
+    for (auto& p : s.changed) {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+    if (s.list) cudaFree(s.list);
+    if (s.count) cudaFree(s.count);
+    if (s.census) cudaFree(s.census);
+    if (s.pass_no) cudaFree(s.pass_no);
+    s = golb200::LocalState{};
 }
 
 void release_device(gol_engine* e) {
     release_graphs(e);
+    release_local(e);
     for (auto& p : e->d) {
         if (p) cudaFree(p);
         p = nullptr;
     }
     e->initialized = false;
+}
+
+constexpr uint32_t kCensusCap = 1u << 20;   // passes recorded per run (4 MiB)
+
+int alloc_local(gol_engine* e) {
+    golb200::LocalState& s = e->lst;
+    const size_t nt = (size_t)e->lplan.tiles_x * e->lplan.tiles_y;
+    cudaError_t ce = cudaSuccess;
+    if (!s.list) {
+        for (auto& p : s.changed)
+            if (ce == cudaSuccess) ce = cudaMalloc(&p, nt);
+        if (ce == cudaSuccess) ce = cudaMalloc(&s.list, nt * sizeof(int));
+        if (ce == cudaSuccess) ce = cudaMalloc(&s.count, sizeof(int));
+        if (ce == cudaSuccess) ce = cudaMalloc(&s.census, kCensusCap * sizeof(uint32_t));
+        if (ce == cudaSuccess) ce = cudaMalloc(&s.pass_no, sizeof(uint32_t));
+        s.census_cap = kCensusCap;
+        if (ce != cudaSuccess) {
+            release_local(e);
+            return e->cuda_fail(ce, "change-tracking allocation");
+        }
+    }
+    // First pass of a round: every tile counts as changed.
+    ce = cudaMemsetAsync(s.changed[1], 1, nt, e->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(s.changed[0], 0, nt, e->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(s.pass_no, 0, sizeof(uint32_t), e->stream);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "change-tracking reset");
+    e->lparity = 0;
+    return GOL_OK;
 }
 
 void release_host(gol_engine* e) {
@@ -127,6 +183,39 @@ int launch_pass(gol_engine* e, int k, cudaStream_t s, int from) {
     }
     cudaError_t ce = golb200::launch_rows_pass(e->d[from], e->d[from ^ 1], e->W, e->Y, k, p, s);
     if (ce != cudaSuccess) return e->cuda_fail(ce, "rows pass launch");
+    return GOL_OK;
+}
+
+int launch_local(gol_engine* e, cudaStream_t s, int from, int parity) {
+    cudaError_t ce = golb200::launch_local_pass(e->d[from], e->d[from ^ 1], e->W, e->Y, e->k,
+                                                e->lplan, e->lst, parity, s);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "change-tracking pass launch");
+    return GOL_OK;
+}
+
+int build_local_graph(gol_engine* e, int cur, int parity) {
+    if (!e->capture_stream) {
+        cudaError_t ce = cudaStreamCreateWithFlags(&e->capture_stream, cudaStreamNonBlocking);
+        if (ce != cudaSuccess) return e->cuda_fail(ce, "capture stream");
+    }
+    cudaError_t ce = cudaStreamBeginCapture(e->capture_stream, cudaStreamCaptureModeThreadLocal);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "begin capture");
+    int rc = GOL_OK;
+    for (int i = 0; i < kGraphPasses && rc == GOL_OK; ++i) {
+        rc = launch_local(e, e->capture_stream, cur, parity);
+        cur ^= 1;
+        parity ^= 1;
+    }
+    cudaGraph_t graph = nullptr;
+    ce = cudaStreamEndCapture(e->capture_stream, &graph);
+    if (rc != GOL_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "end capture");
+    ce = cudaGraphInstantiate(&e->lchunk[cur][parity], graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "graph instantiate");
     return GOL_OK;
 }
 
@@ -265,8 +354,6 @@ int gol_init(gol_engine* e) {
     if (!e) return GOL_E_INVALID;
     if (!e->has_host_grid) return e->fail(GOL_E_STATE, "initialize before set_input");
     if (e->initialized) return e->fail(GOL_E_STATE, "already initialized");
-    if (e->cfg.algorithm == GOL_ALG_LOCAL)
-        return e->fail(GOL_E_UNSUPPORTED, "change-tracking engine is not available in this build");
     cudaError_t ce = cudaSetDevice(e->cfg.device);
     if (ce != cudaSuccess) return e->cuda_fail(ce, "cudaSetDevice");
     if (!e->stream) {
@@ -285,9 +372,18 @@ int gol_init(gol_engine* e) {
     if (!golb200::plan_rows(e->W, e->Y, k, (int)e->cfg.thread_block_size,
                             (int)e->cfg.lane_words, sms, &e->plan))
         return e->fail(GOL_E_UNSUPPORTED, "no kernel plan for this width and depth");
+    e->local = e->cfg.algorithm == GOL_ALG_LOCAL;
+    if (e->local && !golb200::plan_local_tiles(e->W, e->Y, k, (int)e->cfg.tile_rows,
+                                               (int)e->cfg.lane_words, sms, &e->lplan))
+        return e->fail(GOL_E_UNSUPPORTED,
+                       "no change-tracking tile plan (tile_rows must be >= temporal_steps)");
     e->k = k;
+    // The two device grids live from the first init to gol_destroy, so an
+    // instance reused round after round (as ExperimentManager reuses its
+    // algorithms) allocates once and keeps its captured graphs valid.
     const size_t bytes = (size_t)e->W * e->Y * sizeof(uint32_t);
     for (auto& p : e->d) {
+        if (p) continue;
         ce = cudaMalloc(&p, bytes ? bytes : 4);
         if (ce != cudaSuccess) {
             release_device(e);
@@ -300,6 +396,10 @@ int gol_init(gol_engine* e) {
     if (ce != cudaSuccess) {
         release_device(e);
         return e->cuda_fail(ce, "H2D copy");
+    }
+    if (e->local) {
+        int rc = alloc_local(e);
+        if (rc) return rc;
     }
     e->initialized = true;
     e->performed = 0;
@@ -325,6 +425,37 @@ int gol_run(gol_engine* e, uint64_t n) {
     uint64_t passes = n / (uint64_t)k;
     const int rem = (int)(n % (uint64_t)k);
     int rc;
+    if (e->local) {
+        if (budget == 0) {
+            while (passes >= (uint64_t)kGraphPasses) {
+                auto& g = e->lchunk[e->cur][e->lparity];
+                if (!g && (rc = build_local_graph(e, e->cur, e->lparity))) return rc;
+                cudaError_t ce = cudaGraphLaunch(g, e->stream);
+                if (ce != cudaSuccess) return e->cuda_fail(ce, "graph launch");
+                passes -= kGraphPasses;          // even: cur and lparity come back
+                e->performed += (uint64_t)kGraphPasses * k;
+            }
+        }
+        for (; passes > 0; --passes) {
+            if (time_is_up()) return GOL_OK;
+            if ((rc = launch_local(e, e->stream, e->cur, e->lparity))) return rc;
+            e->cur ^= 1;
+            e->lparity ^= 1;
+            e->performed += k;
+        }
+        if (rem > 0) {
+            // A shorter pass is not covered by the k-generation change flags:
+            // advance every tile, then let the next pass start from "all changed".
+            if (time_is_up()) return GOL_OK;
+            if ((rc = launch_pass(e, rem, e->stream, e->cur))) return rc;
+            e->cur ^= 1;
+            e->performed += rem;
+            const size_t nt = (size_t)e->lplan.tiles_x * e->lplan.tiles_y;
+            cudaError_t ce = cudaMemsetAsync(e->lst.changed[e->lparity ^ 1], 1, nt, e->stream);
+            if (ce != cudaSuccess) return e->cuda_fail(ce, "change-flag reset");
+        }
+        return GOL_OK;
+    }
     if (budget == 0 && passes >= 2 * (uint64_t)kGraphPasses) {
         while (passes >= (uint64_t)kGraphPasses) {
             if (!e->chunk[e->cur] && (rc = build_chunk_graph(e, e->cur))) return rc;
@@ -363,8 +494,11 @@ int gol_finalize(gol_engine* e) {
     cudaError_t ce = cudaMemcpyAsync(e->h_words, e->d[e->cur], e->h_bytes, cudaMemcpyDeviceToHost,
                                      e->stream);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
-    release_device(e);
-    if (ce != cudaSuccess) return e->cuda_fail(ce, "D2H copy");
+    e->initialized = false;
+    if (ce != cudaSuccess) {
+        release_device(e);
+        return e->cuda_fail(ce, "D2H copy");
+    }
     return GOL_OK;
 }
 
@@ -470,6 +604,41 @@ int gol_load_random_ones_zeros(uint8_t* cells, uint64_t x, uint64_t y, uint64_t 
     if (!cells && x * y) return GOL_E_INVALID;
     golb200::host_random_ones_zeros(cells, (size_t)(x * y), seed);
     return GOL_OK;
+}
+
+int gol_local_stats(gol_engine* e, uint64_t* passes, uint64_t* tiles_per_pass,
+                    uint64_t* computed_total, uint32_t* per_pass, uint64_t max_entries) {
+    if (!e) return GOL_E_INVALID;
+    if (!e->local || !e->lst.pass_no) return e->fail(GOL_E_STATE, "no change-tracking run");
+    uint32_t n = 0;
+    cudaError_t ce = cudaStreamSynchronize(e->stream);
+    if (ce == cudaSuccess) ce = cudaMemcpy(&n, e->lst.pass_no, sizeof(n), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "census read");
+    const uint32_t rec = n < e->lst.census_cap ? n : e->lst.census_cap;
+    uint64_t sum = 0;
+    if (rec) {
+        uint32_t* tmp = static_cast<uint32_t*>(std::malloc(rec * sizeof(uint32_t)));
+        if (!tmp) return e->fail(GOL_E_NOMEM, "host allocation failed");
+        ce = cudaMemcpy(tmp, e->lst.census, rec * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) {
+            std::free(tmp);
+            return e->cuda_fail(ce, "census read");
+        }
+        for (uint32_t i = 0; i < rec; ++i) sum += tmp[i];
+        if (per_pass) std::memcpy(per_pass, tmp, (size_t)std::min<uint64_t>(rec, max_entries) * 4);
+        std::free(tmp);
+    }
+    if (passes) *passes = n;
+    if (tiles_per_pass) *tiles_per_pass = (uint64_t)e->lplan.tiles_x * e->lplan.tiles_y;
+    if (computed_total) *computed_total = sum;
+    return GOL_OK;
+}
+
+int gol_load_sparse_patches(uint8_t* cells, uint64_t x, uint64_t y, uint64_t seed, uint32_t patch,
+                            double fraction, double density) {
+    if (!cells && x * y) return GOL_E_INVALID;
+    const int n = golb200::host_sparse_patches(cells, x, y, seed, patch, fraction, density);
+    return n < 0 ? GOL_E_INVALID : n;
 }
 
 int gol_probe_int_peak(double* lane_ops_per_s, void* stream) {

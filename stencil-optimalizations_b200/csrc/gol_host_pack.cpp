@@ -14,6 +14,11 @@
 
 #include "gol_internal.h"
 
+#if defined(__x86_64__) || defined(_M_X64)
+#include <emmintrin.h>
+#define GOL_HAVE_STREAM_STORES 1
+#endif
+
 namespace golb200 {
 
 namespace {
@@ -91,6 +96,25 @@ void host_pack_i32(const int32_t* cells, size_t x, size_t y, uint32_t* words) {
 void host_unpack_u8(const uint32_t* words, size_t x, size_t y, uint8_t* cells) {
     const size_t W = x / 32;
     parallel_rows(y, x, [=](size_t y0, size_t y1) {
+#ifdef GOL_HAVE_STREAM_STORES
+        // The output is written once and not read back here: stream it past
+        // the caches (no read-for-ownership of every line).
+        if ((reinterpret_cast<uintptr_t>(cells) & 15u) == 0) {
+            for (size_t r = y0; r < y1; ++r) {
+                const uint32_t* in = words + r * W;
+                __m128i* row = reinterpret_cast<__m128i*>(cells + r * x);
+                for (size_t w = 0; w < W; ++w) {
+                    const uint32_t v = in[w];
+                    _mm_stream_si128(row + 2 * w, _mm_set_epi64x((long long)unpack8(v >> 8),
+                                                                 (long long)unpack8(v)));
+                    _mm_stream_si128(row + 2 * w + 1, _mm_set_epi64x((long long)unpack8(v >> 24),
+                                                                     (long long)unpack8(v >> 16)));
+                }
+            }
+            _mm_sfence();
+            return;
+        }
+#endif
         for (size_t r = y0; r < y1; ++r) {
             const uint32_t* in = words + r * W;
             uint8_t* row = cells + r * x;
@@ -125,6 +149,39 @@ void host_random_ones_zeros(uint8_t* cells, size_t n, uint64_t seed) {
     std::mt19937 rng(static_cast<std::mt19937::result_type>(seed));
     std::uniform_int_distribution<int> dist(0, 1);
     for (size_t i = 0; i < n; ++i) cells[i] = static_cast<uint8_t>(dist(rng));
+}
+
+// Sparse/settling workload: an all-dead grid whose aligned patch x patch
+// tile slots are chosen at random and filled with Bernoulli(density) cells.
+// Fully specified so any implementation can reproduce it:
+//   rng = std::mt19937_64(seed);
+//   slots = 0 .. S-1 (row-major over the (x/patch) x (y/patch) slots),
+//   Fisher-Yates from the back: for i = S-1 .. 1: j = rng() % (i + 1), swap;
+//   the first floor(S * fraction) slots are chosen, then sorted ascending;
+//   each chosen slot's cells, row by row, x fastest: alive iff
+//   (rng() >> 11) * 2^-53 < density.
+int host_sparse_patches(uint8_t* cells, size_t x, size_t y, uint64_t seed, size_t patch,
+                        double fraction, double density) {
+    if (patch == 0 || x % patch || y % patch || fraction < 0 || fraction > 1) return -1;
+    std::memset(cells, 0, x * y);
+    const size_t sx = x / patch, sy = y / patch, S = sx * sy;
+    std::vector<uint32_t> slots(S);
+    for (size_t i = 0; i < S; ++i) slots[i] = (uint32_t)i;
+    std::mt19937_64 rng(seed);
+    for (size_t i = S; i > 1; --i) {
+        const size_t j = (size_t)(rng() % (uint64_t)i);
+        std::swap(slots[i - 1], slots[j]);
+    }
+    const size_t chosen = (size_t)((double)S * fraction);
+    std::sort(slots.begin(), slots.begin() + chosen);
+    for (size_t c = 0; c < chosen; ++c) {
+        const size_t ox = slots[c] % sx * patch, oy = slots[c] / sx * patch;
+        for (size_t r = 0; r < patch; ++r)
+            for (size_t q = 0; q < patch; ++q)
+                cells[(oy + r) * x + ox + q] =
+                    (double)(rng() >> 11) * 0x1.0p-53 < density ? 1 : 0;
+    }
+    return (int)chosen;
 }
 
 } // namespace golb200

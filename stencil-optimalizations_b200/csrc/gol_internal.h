@@ -33,6 +33,30 @@ bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPla
 cudaError_t launch_rows_pass(const uint32_t* src, uint32_t* dst, int W, int Y, int k,
                              const RowsPlan& plan, cudaStream_t stream);
 
+// Change-tracking tiles (GOL_ALG_LOCAL): tile = x-slice x row band.
+struct LocalPlan {
+    RowsPlan rows;     // slice/band geometry of one tile, one warp per tile
+    int tiles_x = 0, tiles_y = 0;
+    int ctas = 0;      // persistent CTAs of the tile kernel
+};
+
+struct LocalState {
+    uint8_t* changed[2] = {nullptr, nullptr};   // per tile, by pass parity
+    int* list = nullptr;                        // active tiles of the current pass
+    int* count = nullptr;                       // its length
+    uint32_t* census = nullptr;                 // active tiles per pass
+    uint32_t census_cap = 0;
+    uint32_t* pass_no = nullptr;                // passes recorded so far
+};
+
+bool plan_local_tiles(int W, int Y, int k, int tile_rows, int wpl, int num_sms, LocalPlan* lp);
+
+// One change-tracking pass: plan (reads changed[parity ^ 1], clears
+// changed[parity]) then the tile kernel (writes changed[parity]).
+cudaError_t launch_local_pass(const uint32_t* src, uint32_t* dst, int W, int Y, int k,
+                              const LocalPlan& lp, const LocalState& st, int parity,
+                              cudaStream_t stream);
+
 cudaError_t launch_pack_cells(const uint8_t* cells, uint32_t* words, size_t x, size_t y,
                               cudaStream_t stream);
 cudaError_t launch_unpack_cells(const uint32_t* words, uint8_t* cells, size_t x, size_t y,
@@ -45,6 +69,8 @@ void host_unpack_u8(const uint32_t* words, size_t x, size_t y, uint8_t* cells);
 void host_unpack_i32(const uint32_t* words, size_t x, size_t y, int32_t* cells);
 
 void host_random_ones_zeros(uint8_t* cells, size_t n, uint64_t seed);
+int host_sparse_patches(uint8_t* cells, size_t x, size_t y, uint64_t seed, size_t patch,
+                        double fraction, double density);
 
 int device_sm_count(int device);
 

@@ -12,7 +12,7 @@ namespace {
 
 template <int WPL, int K>
 cudaError_t launch_one(const RowsLaunch& a, const RowsPlan& p, cudaStream_t stream) {
-    const size_t smem = temporal_smem_bytes(K, p.threads);
+    const size_t smem = temporal_smem_bytes(K, p.threads, WPL);
     rows_temporal_kernel<WPL, K><<<dim3(p.nbands, p.nslices), p.threads, smem, stream>>>(a);
     return cudaPeekAtLastError();
 }

@@ -81,8 +81,53 @@ __device__ __forceinline__ void store_words(uint32_t* p, const uint32_t (&v)[WPL
     }
 }
 
+// Rows for stage 0 are staged through a shared-memory ring with cp.async:
+// kRowRing slots, kRowsInFlight rows issued ahead of use. Each lane copies
+// and later reads back only its own words, so a per-thread
+// cp.async.wait_group (a hardware wait, no spin) orders the two. Rows and
+// lanes outside the grid are zero-filled by the copy itself (src-size 0).
+constexpr int kRowRing = 6;
+constexpr int kRowsInFlight = kRowRing - 1;
+
+template <int WPL>
+__device__ __forceinline__ void cp_async_words(uint32_t saddr, const uint32_t* g, bool valid) {
+    const int bytes = valid ? WPL * 4 : 0;
+    if constexpr (WPL == 4) {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(saddr), "l"(g), "r"(bytes)
+                     : "memory");
+    } else if constexpr (WPL == 2) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(g), "r"(bytes)
+                     : "memory");
+    } else {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(saddr), "l"(g), "r"(bytes)
+                     : "memory");
+    }
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <int WPL>
+__device__ __forceinline__ void lds_words(const uint32_t* p, uint32_t (&v)[WPL]) {
+    if constexpr (WPL == 4) {
+        const uint4 t = *reinterpret_cast<const uint4*>(p);
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    } else if constexpr (WPL == 2) {
+        const uint2 t = *reinterpret_cast<const uint2*>(p);
+        v[0] = t.x; v[1] = t.y;
+    } else {
+        v[0] = *p;
+    }
+}
+
 template <int WPL, int K>
 struct TemporalRegs {
+    int rd_slot;                  // ring slot of the row stage 0 reads next
+    uint32_t diff;                // change tracking: OR of (new ^ old) over stored words
     uint32_t ld[3][WPL];          // stage-0 rows, slot = step % 3
     uint32_t h0[K][3][WPL];       // stage g's horizontal sums, bit plane 0
     uint32_t h1[K][3][WPL];       //                            bit plane 1
@@ -103,17 +148,31 @@ struct TemporalCtx {
     const uint32_t* erd;   // lane 0: left warp's side-1 entry; lane 31: right warp's side-0
     uint32_t* ewr;         // lane 0 / 31: this warp's entry, side 0 / 1; others: dummy word
     bool first_lane, last_lane;
+    const uint32_t* ring;  // this lane's words in ring slot 0 (shared memory)
+    uint32_t ring_saddr;   // same, as a shared-window address for cp.async
+    int ring_stride;       // words per ring slot (blockDim.x * WPL)
     int W, Y, y0, y1, B;
     int lane, base;
     bool lane_ok;   // this lane's words lie inside the grid
     bool own;       // ... and inside this CTA's slice (not halo): stored
 };
 
+// Copies the row stage 0 consumes at step j (grid row y0 - K + j) into ring
+// slot `slot`, zero-filled outside the grid; commits it as one group.
+template <int WPL, int K>
+__device__ __forceinline__ void issue_row(const TemporalCtx& c, int j, int slot) {
+    const int r = c.y0 - K + j;
+    const bool v = c.lane_ok && (unsigned)r < (unsigned)c.Y;
+    const uint32_t* g = v ? c.src + (size_t)r * c.W + c.base : c.src;
+    cp_async_words<WPL>(c.ring_saddr + (uint32_t)(slot * c.ring_stride) * 4u, g, v);
+    cp_async_commit();
+}
+
 // Step body. FAST = steady state: every stage active, every row inside the
 // grid, so no activity tests or row masks (the whole step is one basic
 // block and the K stages' independent chains interleave). LMASK forces the
 // out-of-grid lanes of a partial CTA to stay dead.
-template <int WPL, int K, int PH, bool FAST, bool LMASK>
+template <int WPL, int K, int PH, bool FAST, bool LMASK, bool TRACK>
 __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const TemporalCtx& c, int i,
                                               uint32_t lane_mask) {
     constexpr int NEW3 = PH % 3;          // ring-of-3 slot written at this step
@@ -162,8 +221,15 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
                 if (!FAST || LMASK) res[w] &= keep;
             }
             if (g == K) {
-                if ((FAST || (row >= c.y0 && row < c.y1)) && c.own)
+                if ((FAST || (row >= c.y0 && row < c.y1)) && c.own) {
                     store_words<WPL>(c.dst + (size_t)row * c.W + c.base, res);
+                    if (TRACK) {   // compare with the same row before the pass
+                        uint32_t old[WPL];
+                        load_words<WPL>(c.src + (size_t)row * c.W + c.base, old);
+#pragma unroll
+                        for (int w = 0; w < WPL; ++w) s.diff |= res[w] ^ old[w];
+                    }
+                }
             } else {
 #pragma unroll
                 for (int w = 0; w < WPL; ++w) s.o[g - 1][NEW3][w] = res[w];
@@ -172,44 +238,47 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
         }
     }
 
-    // Stage 0: publish this step's loaded row, prefetch the next one.
-    if (FAST || i <= c.B + 2 * K - 1) {
-        c.ewr[edge_off(0, NEW3)] = c.last_lane ? s.ld[NEW3][WPL - 1] : s.ld[NEW3][0];
-        const int nrow = c.y0 - K + i + 1;
-        if (FAST) {
-            if (!LMASK || c.lane_ok)
-                load_words<WPL>(c.src + (size_t)nrow * c.W + c.base, s.ld[(PH + 1) % 3]);
-        } else if (i + 1 <= c.B + 2 * K - 1 && c.lane_ok && (unsigned)nrow < (unsigned)c.Y) {
-            load_words<WPL>(c.src + (size_t)nrow * c.W + c.base, s.ld[(PH + 1) % 3]);
-        } else {
-#pragma unroll
-            for (int w = 0; w < WPL; ++w) s.ld[(PH + 1) % 3][w] = 0u;
-        }
-    }
+    // Stage 0 (every step, so each step commits exactly one copy group):
+    // publish this step's row, issue the row kRowsInFlight steps ahead, and
+    // read the next step's row out of the ring.
+    c.ewr[edge_off(0, NEW3)] = c.last_lane ? s.ld[NEW3][WPL - 1] : s.ld[NEW3][0];
+    // rd_slot holds step i+1's row; step i+kRowsInFlight's row goes kRowsInFlight-1
+    // slots further on, into the slot read two steps ago.
+    const int wr_slot = s.rd_slot + (kRowsInFlight - 1) - (s.rd_slot >= kRowRing - (kRowsInFlight - 1) ? kRowRing : 0);
+    issue_row<WPL, K>(c, i + kRowsInFlight, wr_slot);
+    cp_async_wait<kRowsInFlight - 1>();
+    lds_words<WPL>(c.ring + s.rd_slot * c.ring_stride, s.ld[(PH + 1) % 3]);
+    s.rd_slot = s.rd_slot == kRowRing - 1 ? 0 : s.rd_slot + 1;
     __syncthreads();
 }
 
-template <int WPL, int K, bool FAST, bool LMASK>
+template <int WPL, int K, bool FAST, bool LMASK, bool TRACK>
 __device__ __forceinline__ void temporal_steps(TemporalRegs<WPL, K>& s, const TemporalCtx& c,
                                                int i0, int i1, uint32_t lane_mask) {
     for (int i = i0; i < i1; i += 3) {
-        temporal_step<WPL, K, 0, FAST, LMASK>(s, c, i + 0, lane_mask);
-        temporal_step<WPL, K, 1, FAST, LMASK>(s, c, i + 1, lane_mask);
-        temporal_step<WPL, K, 2, FAST, LMASK>(s, c, i + 2, lane_mask);
+        temporal_step<WPL, K, 0, FAST, LMASK, TRACK>(s, c, i + 0, lane_mask);
+        temporal_step<WPL, K, 1, FAST, LMASK, TRACK>(s, c, i + 1, lane_mask);
+        temporal_step<WPL, K, 2, FAST, LMASK, TRACK>(s, c, i + 2, lane_mask);
     }
 }
 
-template <int WPL, int K>
-__global__ void __launch_bounds__(kTemporalMaxThreads, GOL_TEMPORAL_MIN_BLOCKS)
-rows_temporal_kernel(RowsLaunch a) {
-    extern __shared__ uint32_t edges[];
+// One tile of one pass: output rows [band*a.band, +a.band) of x-slice
+// `slice_idx`, K generations from a.src into a.dst. The CTA's shared memory
+// (temporal_smem_bytes) is reused from call to call: every copy is drained
+// before returning. With TRACK, returns this thread's OR of (new ^ old) over
+// the words it stored (0 when its part of the tile did not change).
+template <int WPL, int K, bool TRACK>
+__device__ __forceinline__ uint32_t band_tile(const RowsLaunch& a, int band, int slice_idx,
+                                              uint32_t* smem) {
     constexpr int ESTRIDE = K * 6;            // words per padded-warp entry
+    uint32_t* ring = smem;                    // kRowRing slots of blockDim.x * WPL words
+    uint32_t* edges = smem + kRowRing * blockDim.x * WPL;
     TemporalCtx c;
     c.src = a.src;
     c.dst = a.dst;
     c.W = a.W;
     c.Y = a.Y;
-    c.y0 = blockIdx.x * a.band;
+    c.y0 = band * a.band;
     c.y1 = min(c.y0 + a.band, a.Y);
     c.B = c.y1 - c.y0;
     c.lane = threadIdx.x & 31;
@@ -221,7 +290,7 @@ rows_temporal_kernel(RowsLaunch a) {
     c.ewr = (c.first_lane || c.last_lane)
                 ? edges + (warp + 1) * ESTRIDE + (c.last_lane ? 1 : 0)
                 : edges + (EW + warp) * ESTRIDE;
-    const int xs = blockIdx.y * a.slice;
+    const int xs = slice_idx * a.slice;
     const int x0 = xs - a.halo;
     c.base = x0 + (int)threadIdx.x * WPL;
     c.lane_ok = c.base >= 0 && c.base < a.W;
@@ -242,9 +311,14 @@ rows_temporal_kernel(RowsLaunch a) {
             s.o[g][0][w] = s.o[g][1][w] = s.o[g][2][w] = 0u;
         }
     }
-    const int row0 = c.y0 - K;
-    if (c.lane_ok && (unsigned)row0 < (unsigned)c.Y)
-        load_words<WPL>(c.src + (size_t)row0 * c.W + c.base, s.ld[0]);
+    c.ring = ring + threadIdx.x * WPL;
+    c.ring_saddr = (uint32_t)__cvta_generic_to_shared(c.ring);
+    c.ring_stride = blockDim.x * WPL;
+    for (int j = 0; j < kRowsInFlight; ++j) issue_row<WPL, K>(c, j, j);
+    cp_async_wait<kRowsInFlight - 1>();
+    lds_words<WPL>(c.ring, s.ld[0]);
+    s.rd_slot = 1;
+    s.diff = 0u;
     __syncthreads();
 
     // Steps [f0, f1) run the steady-state body: all stages active (i >= 3K),
@@ -256,20 +330,62 @@ rows_temporal_kernel(RowsLaunch a) {
     const int f1 = min(c.B + 2 * K - 1, c.Y - c.y0 + K - 1);
     const int fast_end = f1 > f0 ? f0 + (f1 - f0) / 3 * 3 : f0;
     if (fast_end > f0) {
-        temporal_steps<WPL, K, false, false>(s, c, 0, f0, lane_mask);
+        temporal_steps<WPL, K, false, false, TRACK>(s, c, 0, f0, lane_mask);
         if (all_lanes_ok)
-            temporal_steps<WPL, K, true, false>(s, c, f0, fast_end, lane_mask);
+            temporal_steps<WPL, K, true, false, TRACK>(s, c, f0, fast_end, lane_mask);
         else
-            temporal_steps<WPL, K, true, true>(s, c, f0, fast_end, lane_mask);
-        temporal_steps<WPL, K, false, false>(s, c, fast_end, nsteps, lane_mask);
+            temporal_steps<WPL, K, true, true, TRACK>(s, c, f0, fast_end, lane_mask);
+        temporal_steps<WPL, K, false, false, TRACK>(s, c, fast_end, nsteps, lane_mask);
     } else {
-        temporal_steps<WPL, K, false, false>(s, c, 0, nsteps, lane_mask);
+        temporal_steps<WPL, K, false, false, TRACK>(s, c, 0, nsteps, lane_mask);
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");   // no copy outlives the tile
+    return s.diff;
+}
+
+template <int WPL, int K>
+__global__ void __launch_bounds__(kTemporalMaxThreads, GOL_TEMPORAL_MIN_BLOCKS)
+rows_temporal_kernel(RowsLaunch a) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    band_tile<WPL, K, false>(a, blockIdx.x, blockIdx.y, smem);
+}
+
+// Change-tracking pass over a list of tiles (tile = x-slice x row band,
+// index band * tiles_x + slice). Persistent CTAs walk the list, which the
+// plan kernel built on the device; each writes changed[tile] = 1 iff any
+// cell of its tile differs after the pass.
+struct TileList {
+    const int* list;        // active tile indices
+    const int* count;       // number of entries in `list`
+    uint8_t* changed;       // per tile, this pass
+    int tiles_x;
+};
+
+template <int WPL, int K>
+__global__ void __launch_bounds__(kTemporalMaxThreads, GOL_TEMPORAL_MIN_BLOCKS)
+rows_tiles_kernel(RowsLaunch a, TileList t) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    __shared__ int tile_changed;
+    const int n = *t.count;
+    for (int idx = blockIdx.x; idx < n; idx += gridDim.x) {
+        const int tile = t.list[idx];
+        if (threadIdx.x == 0) tile_changed = 0;
+        __syncthreads();
+        const uint32_t d = band_tile<WPL, K, true>(a, tile / t.tiles_x, tile % t.tiles_x, smem);
+        if (__any_sync(0xffffffffu, d != 0u) && (threadIdx.x & 31) == 0) tile_changed = 1;
+        __syncthreads();
+        if (threadIdx.x == 0) t.changed[tile] = (uint8_t)tile_changed;
+        __syncthreads();
     }
 }
 
-// Shared memory a launch needs: the edge table plus one dummy entry per warp.
-__host__ __device__ inline size_t temporal_smem_bytes(int K, int threads) {
-    return (size_t)(2 * (threads >> 5) + 2) * K * 6 * sizeof(uint32_t);
+
+
+// Shared memory a launch needs: the row ring, the edge table and one dummy
+// edge entry per warp.
+__host__ __device__ inline size_t temporal_smem_bytes(int K, int threads, int wpl) {
+    return ((size_t)kRowRing * threads * wpl + (size_t)(2 * (threads >> 5) + 2) * K * 6) *
+           sizeof(uint32_t);
 }
 
 } // namespace golb200

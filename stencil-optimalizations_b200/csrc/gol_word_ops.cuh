@@ -39,6 +39,7 @@ constexpr unsigned LUT_AND_OR = 0xEA;      // (a & b) | c
 // Horizontal 3-cell sum of one row word: (left + centre + right) per cell as
 // two bit planes. `lw` is the word to the left (its bit 31 is the cell just
 // left of bit 0), `rw` the word to the right (its bit 0 follows bit 31).
+
 __device__ __forceinline__ void hsum(uint32_t lw, uint32_t c, uint32_t rw, uint32_t& h0,
                                      uint32_t& h1) {
     const uint32_t l = __funnelshift_l(lw, c, 1);   // cell x-1 aligned to x

@@ -95,6 +95,10 @@ def lib():
     L.gol_pack_cells_device.argtypes = [_vp, _vp, _u64, _u64, _vp]
     L.gol_unpack_cells_device.argtypes = [_vp, _vp, _u64, _u64, _vp]
     L.gol_load_random_ones_zeros.argtypes = [_vp, _u64, _u64, _u64]
+    L.gol_local_stats.argtypes = [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64),
+                                  ctypes.POINTER(_u64), _vp, _u64]
+    L.gol_load_sparse_patches.argtypes = [_vp, _u64, _u64, _u64, _u32, ctypes.c_double,
+                                          ctypes.c_double]
     L.gol_probe_int_peak.argtypes = [ctypes.POINTER(ctypes.c_double), _vp]
     L.gol_abi_version.restype = ctypes.c_int
     L.gol_build_info.restype = ctypes.c_char_p
@@ -229,6 +233,18 @@ class GolB200:
                     "plan")
         return {"temporal_steps": k.value, "band_rows": b.value, "words_per_lane": w.value}
 
+    def local_stats(self, max_entries: int = 0) -> dict:
+        """Change-tracking census (GOL_ALG_LOCAL): passes, tiles, computed tiles."""
+        p, t, c = _u64(), _u64(), _u64()
+        per = np.zeros(max_entries, dtype=np.uint32)
+        self._check(lib().gol_local_stats(self._e, ctypes.byref(p), ctypes.byref(t), ctypes.byref(c),
+                                          _ptr(per) if max_entries else None, max_entries),
+                    "local_stats")
+        out = {"passes": p.value, "tiles_per_pass": t.value, "computed_tiles": c.value}
+        if max_entries:
+            out["per_pass"] = per[:min(p.value, max_entries)]
+        return out
+
     def close(self) -> None:
         if self._e:
             lib().gol_destroy(self._e)
@@ -264,6 +280,17 @@ def load_random_ones_zeros(x: int, y: int, seed: int) -> np.ndarray:
     rc = lib().gol_load_random_ones_zeros(_ptr(out), x, y, seed)
     if rc != GOL_OK:
         raise RuntimeError(f"gol_load_random_ones_zeros failed with status {rc}")
+    return out
+
+
+def load_sparse_patches(x: int, y: int, seed: int, patch: int = 64, fraction: float = 0.01,
+                        density: float = 0.35) -> np.ndarray:
+    """All-dead grid with a seeded `fraction` of patch x patch slots filled
+    with Bernoulli(density) cells (the sparse/settling workload)."""
+    out = np.empty((y, x), dtype=np.uint8)
+    rc = lib().gol_load_sparse_patches(_ptr(out), x, y, seed, patch, fraction, density)
+    if rc < 0:
+        raise RuntimeError(f"gol_load_sparse_patches failed with status {rc}")
     return out
 
 
