@@ -128,6 +128,7 @@ class ExperimentParams:
     thread_block_size: int = 0            # rows per CTA band (0 = auto)
     temporal_steps: int = 0               # k (0 = auto)
     lane_words: int = 0                   # 32-bit words per lane (0 = auto)
+    tile_rows: int = 0                    # change-tracking tile height (0 = auto)
     algorithm: str = "auto"
     device: int = 0
     stream: int | None = None             # cudaStream_t as an integer
@@ -158,6 +159,7 @@ class GolB200:
         cfg.word_bits = int(p.state_bits_count)
         cfg.temporal_steps = int(p.temporal_steps)
         cfg.lane_words = int(p.lane_words)
+        cfg.tile_rows = int(p.tile_rows)
         cfg.thread_block_size = int(p.thread_block_size)
         cfg.max_runtime_seconds = int(p.max_runtime_seconds)
         cfg.device = int(p.device)
