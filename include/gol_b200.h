@@ -55,7 +55,8 @@ enum gol_status {
     GOL_E_STATE = -2,        /* call out of the contract's phase order          */
     GOL_E_CUDA = -3,         /* CUDA runtime error (message in gol_last_error)  */
     GOL_E_NOMEM = -4,        /* host or device allocation failed                */
-    GOL_E_UNSUPPORTED = -5   /* shape/parameters outside what the kernels cover */
+    GOL_E_UNSUPPORTED = -5,  /* shape/parameters outside what the kernels cover */
+    GOL_E_TIMEOUT = -6       /* a device-side wait gave up (bounded spin)       */
 };
 
 /* Which kernel family gol_run uses. */
@@ -143,6 +144,21 @@ int gol_load_random_ones_zeros(uint8_t* cells, uint64_t x, uint64_t y, uint64_t 
 int gol_load_sparse_patches(uint8_t* cells, uint64_t x, uint64_t y, uint64_t seed, uint32_t patch,
                             double fraction, double density);
 
+/* Uneven multi-grid workloads (batched and serving configurations), drawn
+ * from one std::mt19937_64(seed) stream with u = (rng() >> 11) * 2^-53, per
+ * grid in order: x = multiple * llround(exp(ln min + u (ln max - ln min)) /
+ * multiple) clamped to [min, max]; y likewise; density = lo + u (hi - lo);
+ * gens = llround(exp(ln glo + u (ln ghi - ln glo))); cell_seed = rng(). */
+int gol_workload_uneven(uint64_t seed, uint32_t n, uint32_t min_side, uint32_t max_side,
+                        uint32_t multiple, double density_lo, double density_hi, uint64_t gens_lo,
+                        uint64_t gens_hi, uint64_t* xs, uint64_t* ys, double* densities,
+                        uint64_t* gens, uint64_t* cell_seeds);
+/* Bernoulli(density) cells, raster order, alive iff (rng() >> 11) * 2^-53 <
+ * density for std::mt19937_64(seed). */
+int gol_load_bernoulli(uint8_t* cells, uint64_t x, uint64_t y, uint64_t seed, double density);
+/* Poisson arrival times (seconds): exponential gaps -ln(1 - u) / rate. */
+int gol_poisson_arrivals(uint64_t seed, uint32_t n, double rate, double* times);
+
 /* --- Device-resident access (between gol_init and gol_finalize) ---------- */
 
 /* Device pointer to the current grid (x/32 uint32 words per row). */
@@ -183,6 +199,39 @@ int gol_unpack_cells_device(const void* d_words, uint8_t* d_cells, uint64_t x, u
  * register-only kernel: the integer-pipe roofline of the bit-sliced passes.
  * Synchronizes `stream`. */
 int gol_probe_int_peak(double* lane_ops_per_s, void* stream);
+
+/* --- Batched uneven grids (one persistent launch) ------------------------ */
+
+/* Many independent grids, each with its own size and generation count,
+ * advanced together by one persistent kernel launch (captured as a CUDA
+ * graph). Per grid an autotuner picks words per lane, temporal depth and
+ * band height; gol_batch_set_plan overrides it. No reference counterpart:
+ * the reference runs one grid per invocation (experiment_manager.hpp:365-394). */
+typedef struct gol_batch gol_batch;
+
+int gol_batch_create(gol_batch** out, int32_t device, void* stream);
+/* Adds a host cell grid (x % 32 == 0) to run `generations`. */
+int gol_batch_add(gol_batch* b, const uint8_t* cells, uint64_t x, uint64_t y, uint64_t generations,
+                  int32_t* grid_id);
+int gol_batch_set_plan(gol_batch* b, int32_t grid_id, uint32_t lane_words, uint32_t temporal_steps,
+                       uint32_t band_rows);
+int gol_batch_plan(const gol_batch* b, int32_t grid_id, uint32_t* lane_words,
+                   uint32_t* temporal_steps, uint32_t* band_rows, uint32_t* segments);
+/* Plans all grids and copies inputs and the work list to the device. */
+int gol_batch_upload(gol_batch* b);
+/* Runs every grid to its generation count in one persistent launch
+ * (asynchronous; gol_batch_sync waits). Re-running restarts from the inputs. */
+int gol_batch_run(gol_batch* b);
+/* Baseline: the same grids one after another through the single-grid pass
+ * kernel, one launch per k-generation pass per grid. */
+int gol_batch_run_plain(gol_batch* b, uint32_t temporal_steps);
+/* Waits; GOL_E_TIMEOUT if the persistent kernel gave up a dependency wait. */
+int gol_batch_sync(gol_batch* b);
+int gol_batch_fetch(gol_batch* b, int32_t grid_id, uint8_t* cells);
+int gol_batch_info(const gol_batch* b, uint64_t* grids, uint64_t* items, uint64_t* cell_updates);
+void* gol_batch_stream(gol_batch* b);
+const char* gol_batch_last_error(const gol_batch* b);
+void gol_batch_destroy(gol_batch* b);
 
 /* Library identification: ABI version and the sm arch it was built for. */
 int gol_abi_version(void);

@@ -1,0 +1,624 @@
+// Batched uneven grids in one persistent launch.
+//
+// The reference advances one grid per run (ExperimentManager::perform_alg,
+// experiment_manager.hpp:365-394). Here many grids of different sizes and
+// generation counts advance together:
+//
+//   work item   (grid, x-slice, band group, pass): one pass of k generations
+//               on one warp. Narrow grids (W / WPL <= 32 lanes) have one
+//               slice and cut the warp into S segments of L = W / WPL lanes
+//               (any L, so narrow grids keep most lanes busy), each segment
+//               streaming its own band through the K-stage pipeline
+//               (band_tile's step code in segmented mode). Wider grids are
+//               cut into slices of 30 lanes plus a halo lane each side
+//               (errors from the unknown cells beyond the halo move one cell
+//               per generation and stay in the halo for k <= 32).
+//   order       items are numbered pass-major (all pass-0 items of every
+//               grid, then pass 1, ...); persistent one-warp CTAs take
+//               tickets from an atomic counter.
+//   dependency  (g, s, j, p) needs (g, s-1..s+1, j-1..j+1, p-1) finished:
+//               that is every word it reads, and it also ends every read of
+//               the buffer it overwrites. A per-group counter holds the passes done; the
+//               waiting lane polls it with ld.acquire, bounded: after
+//               kSpinLimit polls the CTA records GOL_E_TIMEOUT and stops.
+//               Every dependency has a smaller ticket, held by a CTA that is
+//               resident and never waits on a larger one, so the wait always
+//               ends; the bound is only a guard.
+//   release     each lane fences its stores, the warp syncs, lane 0 stores
+//               the new pass count with st.release.
+//
+// Rows are read through cp.async after the acquire; a weak load ordered
+// after an acquire observes the released data (PTX memory model), so L1
+// cannot serve a stale line of a buffer rewritten in this same launch.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "gol_b200.h"
+#include "gol_internal.h"
+#include "gol_rows_temporal.cuh"
+
+namespace golb200 {
+
+struct BatchGrid {
+    uint32_t* buf[2];      // ping-pong device grids (W words per row)
+    int W, Y;              // words per row, rows
+    int wpl;               // words per lane
+    int k;                 // depth of full passes
+    int last_k;            // depth of the final pass
+    int passes;            // passes to run (0 = nothing to do)
+    int band;              // rows per segment
+    int seg_lanes;         // L lanes per segment (W / wpl, or 32 when sliced)
+    int segs;              // S segments per warp (1 when sliced)
+    int ngroups;           // band groups
+    int slice;             // words per x-slice (W when unsliced)
+    int nslices;
+    int halo;              // halo words each side of a slice (0 when unsliced)
+    int done_base;         // offset of this grid's (group, slice) counters
+};
+
+struct BatchItem {
+    int grid, group, slice, pass;
+};
+
+constexpr int kBatchMaxK = 4;
+constexpr long long kSpinLimit = 1ll << 24;   // polls of >= 100 ns: a few-second guard
+
+namespace {
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(int* p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+template <int WPL, int K>
+__device__ __forceinline__ void seg_group(const BatchGrid& G, int group, int slice_idx,
+                                          const uint32_t* src, uint32_t* dst, uint32_t* ring) {
+    const int lane = threadIdx.x & 31;
+    const int L = G.seg_lanes;
+    const int seg = lane / L, q = lane - seg * L;
+    const int xs = slice_idx * G.slice;
+    TemporalCtx c;
+    c.src = src;
+    c.dst = dst;
+    c.W = G.W;
+    c.Y = G.Y;
+    c.B = G.band;
+    c.y0 = (group * G.segs + seg) * G.band;
+    c.y1 = min(c.y0 + G.band, G.Y);
+    c.lane = lane;
+    c.base = xs - G.halo + q * WPL;
+    c.lane_ok = seg < G.segs && c.y0 < G.Y && c.base >= 0 && c.base < G.W;
+    c.own = c.lane_ok && c.base >= xs && c.base < xs + G.slice;
+    c.first_lane = q == 0;
+    c.last_lane = q == L - 1;
+    c.src_l = max(lane - 1, 0);
+    c.src_r = min(lane + 1, 31);
+    c.erd = nullptr;
+    c.ewr = nullptr;
+    c.ring = ring + lane * WPL;
+    c.ring_saddr = (uint32_t)__cvta_generic_to_shared(c.ring);
+    c.ring_stride = 32 * WPL;
+    const uint32_t lane_mask = c.lane_ok ? 0xffffffffu : 0u;
+
+    TemporalRegs<WPL, K> s;
+#pragma unroll
+    for (int w = 0; w < WPL; ++w) {
+        s.ld[0][w] = s.ld[1][w] = s.ld[2][w] = 0u;
+#pragma unroll
+        for (int g = 0; g < K; ++g) {
+            s.h0[g][0][w] = s.h0[g][1][w] = s.h0[g][2][w] = 0u;
+            s.h1[g][0][w] = s.h1[g][1][w] = s.h1[g][2][w] = 0u;
+            s.o[g][0][w] = s.o[g][1][w] = s.o[g][2][w] = 0u;
+        }
+    }
+    for (int j = 0; j < kRowsInFlight; ++j) issue_row<WPL, K>(c, j, j);
+    cp_async_wait<kRowsInFlight - 1>();
+    lds_words<WPL>(c.ring, s.ld[0]);
+    s.rd_slot = 1;
+    s.diff = 0u;
+
+    // Steady state while every active segment's rows stay inside the grid:
+    // the deepest active segment bounds the window.
+    const int active = min(G.segs, (G.Y - group * G.segs * G.band + G.band - 1) / G.band);
+    const int y0_last = (group * G.segs + active - 1) * G.band;
+    const int nsteps = G.band + 3 * K;
+    const int f0 = 3 * K;
+    const int f1 = min(G.band + 2 * K - 1, G.Y - y0_last + K - 1);
+    const int fast_end = f1 > f0 ? f0 + (f1 - f0) / 3 * 3 : f0;
+    if (fast_end > f0) {
+        temporal_steps<WPL, K, false, false, false, true>(s, c, 0, f0, lane_mask);
+        temporal_steps<WPL, K, true, true, false, true>(s, c, f0, fast_end, lane_mask);
+        temporal_steps<WPL, K, false, false, false, true>(s, c, fast_end, nsteps, lane_mask);
+    } else {
+        temporal_steps<WPL, K, false, false, false, true>(s, c, 0, nsteps, lane_mask);
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+template <int WPL>
+__device__ __forceinline__ void seg_dispatch(int k, const BatchGrid& G, int group, int slice,
+                                             const uint32_t* src, uint32_t* dst, uint32_t* ring) {
+    switch (k) {
+        case 1: seg_group<WPL, 1>(G, group, slice, src, dst, ring); break;
+        case 2: seg_group<WPL, 2>(G, group, slice, src, dst, ring); break;
+        case 3: seg_group<WPL, 3>(G, group, slice, src, dst, ring); break;
+        default: seg_group<WPL, 4>(G, group, slice, src, dst, ring); break;
+    }
+}
+
+__global__ void __launch_bounds__(32) batch_kernel(const BatchGrid* __restrict__ grids,
+                                                   const BatchItem* __restrict__ items, int nitems,
+                                                   int* ticket, int* done, int* status) {
+    __shared__ __align__(16) uint32_t ring[kRowRing * 32 * 4];
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(ticket, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= nitems) return;
+        const BatchItem it = items[t];
+        const BatchGrid G = grids[it.grid];
+        int* mine = done + G.done_base + it.group * G.nslices + it.slice;
+        if (it.pass > 0) {
+            // Every lane acquires every counter it depends on, so each lane's
+            // own copies below are ordered after the producers' releases.
+            bool ok = true;
+            const int jlo = max(it.group - 1, 0), jhi = min(it.group + 1, G.ngroups - 1);
+            const int slo = max(it.slice - 1, 0), shi = min(it.slice + 1, G.nslices - 1);
+            for (int j = jlo; j <= jhi && ok; ++j) {
+                for (int sl = slo; sl <= shi && ok; ++sl) {
+                    const int* p = done + G.done_base + j * G.nslices + sl;
+                    long long spins = 0;
+                    while (ld_acquire(p) < it.pass) {
+                        if (++spins > kSpinLimit || *(volatile int*)status != 0) {
+                            ok = false;
+                            break;
+                        }
+                        __nanosleep(100);
+                    }
+                }
+            }
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0) atomicCAS(status, 0, GOL_E_TIMEOUT);
+                return;
+            }
+        }
+        const int k = it.pass == G.passes - 1 ? G.last_k : G.k;
+        const uint32_t* src = G.buf[it.pass & 1];
+        uint32_t* dst = G.buf[(it.pass + 1) & 1];
+        switch (G.wpl) {
+            case 4: seg_dispatch<4>(k, G, it.group, it.slice, src, dst, ring); break;
+            case 2: seg_dispatch<2>(k, G, it.group, it.slice, src, dst, ring); break;
+            default: seg_dispatch<1>(k, G, it.group, it.slice, src, dst, ring); break;
+        }
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) st_release(mine, it.pass + 1);
+    }
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// Autotuner: per grid, pick (words per lane, depth, band height).
+//
+// Model: a work item costs (band + 3k) pipeline steps of k stages on one
+// warp, and a stage-step on a WPL-wide lane costs c[WPL] (relative warp
+// time, from calibration). A grid's cost is
+//     passes * nslices * ngroups * (band + 3k) * k * c[WPL]
+// for passes = ceil(gens / k), ngroups = ceil(Y / (S * band)). The candidate
+// set is WPL in {1, 2, 4} (W % WPL == 0), k in 1..4, band in
+// {16, 24, 32, 48, 64} with band >= 2k; the cheapest wins.
+// ---------------------------------------------------------------------------
+
+struct BatchTuning {
+    double c[5] = {0, 1.0, 1.15, 0, 1.45};   // relative cost per stage-step by WPL
+};
+
+static BatchTuning g_tuning;
+
+struct GridChoice {
+    int wpl, k, band, seg_lanes, segs, ngroups, passes, last_k, slice, nslices, halo;
+    double cost;
+};
+
+static bool choose(int W, int Y, uint64_t gens, int force_wpl, int force_k, int force_band,
+                   GridChoice* out) {
+    bool found = false;
+    for (int wpl : {1, 2, 4}) {
+        if (force_wpl && wpl != force_wpl) continue;
+        if (W % wpl) continue;
+        const bool sliced = W / wpl > 32;
+        const int L = sliced ? 32 : W / wpl;
+        const int slice = sliced ? 30 * wpl : W;
+        const int nslices = (W + slice - 1) / slice;
+        for (int k = 1; k <= kBatchMaxK; ++k) {
+            if (force_k && k != force_k) continue;
+            for (int band : {16, 24, 32, 48, 64}) {
+                if (force_band) band = force_band;
+                if (band < 2 * k && !force_band) continue;
+                const int S = sliced ? 1 : std::max(1, std::min(32 / L, (Y + band - 1) / band));
+                const int ngroups = (Y + S * band - 1) / (S * band);
+                const uint64_t passes = (gens + k - 1) / k;
+                const double cost = (double)passes * nslices * ngroups * (band + 3 * k) * k *
+                                    g_tuning.c[wpl];
+                if (!found || cost < out->cost) {
+                    found = true;
+                    out->wpl = wpl;
+                    out->k = k;
+                    out->band = band;
+                    out->seg_lanes = L;
+                    out->segs = S;
+                    out->ngroups = ngroups;
+                    out->passes = (int)passes;
+                    out->last_k = gens % k ? (int)(gens % k) : k;
+                    out->slice = slice;
+                    out->nslices = nslices;
+                    out->halo = sliced ? wpl : 0;
+                    out->cost = cost;
+                }
+                if (force_band) break;
+            }
+        }
+    }
+    return found;
+}
+
+} // namespace golb200
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+using golb200::BatchGrid;
+using golb200::BatchItem;
+
+struct gol_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int num_sms = 148;
+
+    struct Entry {
+        uint64_t x, y, gens;
+        int W, Y;
+        std::vector<uint32_t> words;      // packed input (host)
+        golb200::GridChoice choice{};
+        int force_wpl = 0, force_k = 0, force_band = 0;
+        size_t offset = 0;                // word offset of buf[0] in the arena
+        int result_buf = 0;               // buffer holding the last run's result
+    };
+    std::vector<Entry> grids;
+
+    uint32_t* arena = nullptr;            // all grids' ping-pong buffers
+    size_t arena_words = 0;
+    BatchGrid* d_grids = nullptr;
+    BatchItem* d_items = nullptr;
+    int* d_done = nullptr;
+    int* d_ticket = nullptr;
+    int* d_status = nullptr;
+    int nitems = 0, ngroups_total = 0;
+    bool uploaded = false, ran = false;
+    cudaGraphExec_t graph = nullptr;
+    double last_ms = 0;
+    std::string err;
+
+    int fail(int code, const std::string& m) {
+        err = m;
+        return code;
+    }
+    int cuda_fail(cudaError_t e, const char* what) {
+        err = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+        return GOL_E_CUDA;
+    }
+};
+
+namespace {
+
+void batch_free_device(gol_batch* b) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    for (void* p : {(void*)b->arena, (void*)b->d_grids, (void*)b->d_items, (void*)b->d_done,
+                    (void*)b->d_ticket, (void*)b->d_status})
+        if (p) cudaFree(p);
+    b->arena = nullptr;
+    b->d_grids = nullptr;
+    b->d_items = nullptr;
+    b->d_done = nullptr;
+    b->d_ticket = nullptr;
+    b->d_status = nullptr;
+    b->uploaded = false;
+}
+
+} // namespace
+
+extern "C" {
+
+int gol_batch_create(gol_batch** out, int32_t device, void* stream) {
+    if (!out) return GOL_E_INVALID;
+    gol_batch* b = new (std::nothrow) gol_batch();
+    if (!b) return GOL_E_NOMEM;
+    b->device = device;
+    cudaError_t ce = cudaSetDevice(device);
+    if (ce == cudaSuccess) {
+        if (stream) {
+            b->stream = static_cast<cudaStream_t>(stream);
+        } else {
+            ce = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+            b->own_stream = ce == cudaSuccess;
+        }
+    }
+    if (ce != cudaSuccess) {
+        delete b;
+        return GOL_E_CUDA;
+    }
+    b->num_sms = golb200::device_sm_count(device);
+    *out = b;
+    return GOL_OK;
+}
+
+int gol_batch_add(gol_batch* b, const uint8_t* cells, uint64_t x, uint64_t y, uint64_t generations,
+                  int32_t* grid_id) {
+    if (!b) return GOL_E_INVALID;
+    if (x == 0 || y == 0 || x % 32) return b->fail(GOL_E_INVALID, "x must be a positive multiple of 32");
+    if (y > (1u << 30) || generations > (1ull << 31))
+        return b->fail(GOL_E_INVALID, "grid or generation count too large");
+    if (!cells) return b->fail(GOL_E_INVALID, "null cells");
+    gol_batch::Entry e;
+    e.x = x;
+    e.y = y;
+    e.gens = generations;
+    e.W = (int)(x / 32);
+    e.Y = (int)y;
+    e.words.resize((size_t)e.W * e.Y);
+    golb200::host_pack_u8(cells, x, y, e.words.data());
+    b->grids.push_back(std::move(e));
+    b->uploaded = false;
+    if (grid_id) *grid_id = (int32_t)b->grids.size() - 1;
+    return GOL_OK;
+}
+
+int gol_batch_set_plan(gol_batch* b, int32_t grid_id, uint32_t lane_words, uint32_t temporal_steps,
+                       uint32_t band_rows) {
+    if (!b || grid_id < 0 || grid_id >= (int)b->grids.size()) return GOL_E_INVALID;
+    if (temporal_steps > golb200::kBatchMaxK) return b->fail(GOL_E_INVALID, "temporal_steps > 4");
+    auto& e = b->grids[grid_id];
+    e.force_wpl = (int)lane_words;
+    e.force_k = (int)temporal_steps;
+    e.force_band = (int)band_rows;
+    b->uploaded = false;
+    return GOL_OK;
+}
+
+int gol_batch_plan(const gol_batch* b, int32_t grid_id, uint32_t* lane_words,
+                   uint32_t* temporal_steps, uint32_t* band_rows, uint32_t* segments) {
+    if (!b || grid_id < 0 || grid_id >= (int)b->grids.size()) return GOL_E_INVALID;
+    const auto& e = b->grids[grid_id];
+    golb200::GridChoice ch;
+    if (!golb200::choose(e.W, e.Y, e.gens, e.force_wpl, e.force_k, e.force_band, &ch))
+        return GOL_E_UNSUPPORTED;
+    if (lane_words) *lane_words = ch.wpl;
+    if (temporal_steps) *temporal_steps = ch.k;
+    if (band_rows) *band_rows = ch.band;
+    if (segments) *segments = ch.segs;
+    return GOL_OK;
+}
+
+// Plans every grid, uploads inputs and the work list (host -> device).
+int gol_batch_upload(gol_batch* b) {
+    if (!b) return GOL_E_INVALID;
+    cudaError_t ce = cudaSetDevice(b->device);
+    if (ce != cudaSuccess) return b->cuda_fail(ce, "cudaSetDevice");
+    batch_free_device(b);
+    std::vector<BatchGrid> hg;
+    size_t words = 0;
+    int groups = 0, max_passes = 0;
+    for (auto& e : b->grids) {
+        if (!golb200::choose(e.W, e.Y, e.gens, e.force_wpl, e.force_k, e.force_band, &e.choice))
+            return b->fail(GOL_E_UNSUPPORTED, "no batched plan for a grid");
+        if (e.gens == 0) e.choice.passes = 0;
+        e.offset = words;
+        words += 2 * (size_t)e.W * e.Y;
+        BatchGrid g{};
+        g.W = e.W;
+        g.Y = e.Y;
+        g.wpl = e.choice.wpl;
+        g.k = e.choice.k;
+        g.last_k = e.choice.last_k;
+        g.passes = e.choice.passes;
+        g.band = e.choice.band;
+        g.seg_lanes = e.choice.seg_lanes;
+        g.segs = e.choice.segs;
+        g.ngroups = e.choice.ngroups;
+        g.slice = e.choice.slice;
+        g.nslices = e.choice.nslices;
+        g.halo = e.choice.halo;
+        g.done_base = groups;
+        groups += g.ngroups * g.nslices;
+        max_passes = std::max(max_passes, g.passes);
+        hg.push_back(g);
+    }
+    std::vector<BatchItem> items;
+    for (int p = 0; p < max_passes; ++p)
+        for (size_t gi = 0; gi < hg.size(); ++gi)
+            if (p < hg[gi].passes)
+                for (int j = 0; j < hg[gi].ngroups; ++j)
+                    for (int sl = 0; sl < hg[gi].nslices; ++sl) items.push_back({(int)gi, j, sl, p});
+    b->nitems = (int)items.size();
+    b->ngroups_total = groups;
+    b->arena_words = words;
+    ce = cudaMalloc(&b->arena, std::max<size_t>(words, 1) * sizeof(uint32_t));
+    if (ce == cudaSuccess) ce = cudaMalloc(&b->d_grids, std::max<size_t>(hg.size(), 1) * sizeof(BatchGrid));
+    if (ce == cudaSuccess) ce = cudaMalloc(&b->d_items, std::max<size_t>(items.size(), 1) * sizeof(BatchItem));
+    if (ce == cudaSuccess) ce = cudaMalloc(&b->d_done, std::max(groups, 1) * sizeof(int));
+    if (ce == cudaSuccess) ce = cudaMalloc(&b->d_ticket, sizeof(int));
+    if (ce == cudaSuccess) ce = cudaMalloc(&b->d_status, sizeof(int));
+    if (ce != cudaSuccess) {
+        batch_free_device(b);
+        return ce == cudaErrorMemoryAllocation ? b->fail(GOL_E_NOMEM, "device allocation failed")
+                                               : b->cuda_fail(ce, "cudaMalloc");
+    }
+    for (size_t gi = 0; gi < hg.size(); ++gi) {
+        auto& e = b->grids[gi];
+        hg[gi].buf[0] = b->arena + e.offset;
+        hg[gi].buf[1] = b->arena + e.offset + (size_t)e.W * e.Y;
+        ce = cudaMemcpyAsync(hg[gi].buf[0], e.words.data(), e.words.size() * sizeof(uint32_t),
+                             cudaMemcpyHostToDevice, b->stream);
+        if (ce != cudaSuccess) break;
+    }
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(b->d_grids, hg.data(), hg.size() * sizeof(BatchGrid),
+                             cudaMemcpyHostToDevice, b->stream);
+    if (ce == cudaSuccess && !items.empty())
+        ce = cudaMemcpyAsync(b->d_items, items.data(), items.size() * sizeof(BatchItem),
+                             cudaMemcpyHostToDevice, b->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(b->stream);
+    if (ce != cudaSuccess) {
+        batch_free_device(b);
+        return b->cuda_fail(ce, "batch upload");
+    }
+    b->uploaded = true;
+    b->ran = false;
+    return GOL_OK;
+}
+
+// Resets inputs on the device (buf[0] = uploaded input) without re-planning.
+static int batch_reset_inputs(gol_batch* b) {
+    for (auto& e : b->grids) {
+        cudaError_t ce = cudaMemcpyAsync(b->arena + e.offset, e.words.data(),
+                                         e.words.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                         b->stream);
+        if (ce != cudaSuccess) return b->cuda_fail(ce, "batch input copy");
+    }
+    return GOL_OK;
+}
+
+// All grids, all generations: one persistent launch (captured once as a
+// CUDA graph together with the counter resets). Asynchronous; gol_batch_sync
+// waits and reports a timeout recorded by the kernel.
+int gol_batch_run(gol_batch* b) {
+    if (!b) return GOL_E_INVALID;
+    int rc;
+    if (!b->uploaded && (rc = gol_batch_upload(b))) return rc;
+    if (b->ran && (rc = batch_reset_inputs(b))) return rc;
+    if (!b->graph) {
+        cudaStream_t cs = nullptr;
+        cudaError_t ce = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+        if (ce != cudaSuccess) return b->cuda_fail(ce, "capture stream");
+        ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_done, 0, std::max(b->ngroups_total, 1) * sizeof(int), cs);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_ticket, 0, sizeof(int), cs);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_status, 0, sizeof(int), cs);
+        if (ce == cudaSuccess && b->nitems > 0) {
+            int per_sm = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, golb200::batch_kernel, 32, 0);
+            per_sm = std::max(1, per_sm);
+            const int ctas = std::min(b->nitems, b->num_sms * per_sm);   // all resident
+            golb200::batch_kernel<<<ctas, 32, 0, cs>>>(b->d_grids, b->d_items, b->nitems,
+                                                       b->d_ticket, b->d_done, b->d_status);
+            ce = cudaPeekAtLastError();
+        }
+        cudaGraph_t g = nullptr;
+        cudaError_t ce2 = cudaStreamEndCapture(cs, &g);
+        if (ce == cudaSuccess) ce = ce2;
+        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&b->graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        cudaStreamDestroy(cs);
+        if (ce != cudaSuccess) return b->cuda_fail(ce, "batch graph");
+    }
+    cudaError_t ce = cudaGraphLaunch(b->graph, b->stream);
+    if (ce != cudaSuccess) return b->cuda_fail(ce, "batch launch");
+    for (auto& e : b->grids) e.result_buf = e.choice.passes & 1;
+    b->ran = true;
+    return GOL_OK;
+}
+
+int gol_batch_sync(gol_batch* b) {
+    if (!b) return GOL_E_INVALID;
+    cudaError_t ce = cudaStreamSynchronize(b->stream);
+    if (ce != cudaSuccess) return b->cuda_fail(ce, "batch synchronize");
+    if (b->d_status) {
+        int st = 0;
+        ce = cudaMemcpy(&st, b->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) return b->cuda_fail(ce, "batch status");
+        if (st != 0) return b->fail(st, "batched kernel gave up waiting on a dependency");
+    }
+    return GOL_OK;
+}
+
+// Baseline: the same grids with the single-grid path, one after another:
+// every grid gets its own kernel launches (one per k-generation pass), as a
+// caller of the one-grid contract would run them.
+int gol_batch_run_plain(gol_batch* b, uint32_t temporal_steps) {
+    if (!b) return GOL_E_INVALID;
+    int rc;
+    if (!b->uploaded && (rc = gol_batch_upload(b))) return rc;
+    if ((rc = batch_reset_inputs(b))) return rc;
+    const int k0 = temporal_steps ? (int)temporal_steps : 4;
+    for (auto& e : b->grids) {
+        uint32_t* buf[2] = {b->arena + e.offset, b->arena + e.offset + (size_t)e.W * e.Y};
+        int cur = 0;
+        uint64_t left = e.gens;
+        while (left > 0) {
+            const int k = (int)std::min<uint64_t>(left, (uint64_t)k0);
+            golb200::RowsPlan p;
+            if (!golb200::plan_rows(e.W, e.Y, k, 0, 0, b->num_sms, &p))
+                return b->fail(GOL_E_UNSUPPORTED, "no plan");
+            cudaError_t ce = golb200::launch_rows_pass(buf[cur], buf[cur ^ 1], e.W, e.Y, k, p, b->stream);
+            if (ce != cudaSuccess) return b->cuda_fail(ce, "plain launch");
+            cur ^= 1;
+            left -= k;
+        }
+        e.result_buf = cur;
+    }
+    b->ran = true;
+    return GOL_OK;
+}
+
+int gol_batch_fetch(gol_batch* b, int32_t grid_id, uint8_t* cells) {
+    if (!b || grid_id < 0 || grid_id >= (int)b->grids.size() || !cells) return GOL_E_INVALID;
+    if (!b->uploaded) return b->fail(GOL_E_STATE, "fetch before run");
+    auto& e = b->grids[grid_id];
+    const int which = e.result_buf;
+    std::vector<uint32_t> words((size_t)e.W * e.Y);
+    cudaError_t ce = cudaMemcpyAsync(words.data(), b->arena + e.offset + (size_t)which * e.W * e.Y,
+                                     words.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                     b->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(b->stream);
+    if (ce != cudaSuccess) return b->cuda_fail(ce, "batch fetch");
+    golb200::host_unpack_u8(words.data(), e.x, e.y, cells);
+    return GOL_OK;
+}
+
+int gol_batch_info(const gol_batch* b, uint64_t* grids, uint64_t* items, uint64_t* cell_updates) {
+    if (!b) return GOL_E_INVALID;
+    uint64_t cu = 0;
+    for (const auto& e : b->grids) cu += e.x * e.y * e.gens;
+    if (grids) *grids = b->grids.size();
+    if (items) *items = (uint64_t)b->nitems;
+    if (cell_updates) *cell_updates = cu;
+    return GOL_OK;
+}
+
+void* gol_batch_stream(gol_batch* b) { return b ? static_cast<void*>(b->stream) : nullptr; }
+
+const char* gol_batch_last_error(const gol_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+void gol_batch_destroy(gol_batch* b) {
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_free_device(b);
+    if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+} // extern "C"

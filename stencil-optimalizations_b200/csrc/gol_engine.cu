@@ -641,6 +641,30 @@ int gol_load_sparse_patches(uint8_t* cells, uint64_t x, uint64_t y, uint64_t see
     return n < 0 ? GOL_E_INVALID : n;
 }
 
+int gol_workload_uneven(uint64_t seed, uint32_t n, uint32_t min_side, uint32_t max_side,
+                        uint32_t multiple, double density_lo, double density_hi, uint64_t gens_lo,
+                        uint64_t gens_hi, uint64_t* xs, uint64_t* ys, double* densities,
+                        uint64_t* gens, uint64_t* cell_seeds) {
+    if (!xs || !ys || !densities || !gens || !cell_seeds || multiple == 0 || min_side == 0 ||
+        min_side > max_side || gens_lo == 0 || gens_lo > gens_hi)
+        return GOL_E_INVALID;
+    golb200::host_workload_uneven(seed, n, min_side, max_side, multiple, density_lo, density_hi,
+                                  gens_lo, gens_hi, xs, ys, densities, gens, cell_seeds);
+    return GOL_OK;
+}
+
+int gol_load_bernoulli(uint8_t* cells, uint64_t x, uint64_t y, uint64_t seed, double density) {
+    if (!cells && x * y) return GOL_E_INVALID;
+    golb200::host_bernoulli(cells, (size_t)(x * y), seed, density);
+    return GOL_OK;
+}
+
+int gol_poisson_arrivals(uint64_t seed, uint32_t n, double rate, double* times) {
+    if (!times || !(rate > 0)) return GOL_E_INVALID;
+    golb200::host_poisson_arrivals(seed, n, rate, times);
+    return GOL_OK;
+}
+
 int gol_probe_int_peak(double* lane_ops_per_s, void* stream) {
     if (!lane_ops_per_s) return GOL_E_INVALID;
     int dev = 0;

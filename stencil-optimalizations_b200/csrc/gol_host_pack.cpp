@@ -7,6 +7,7 @@
 // Eight cells are handled per 64-bit operation (a byte-to-bit multiply
 // gather), and rows are split across hardware threads.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <random>
 #include <thread>
@@ -182,6 +183,50 @@ int host_sparse_patches(uint8_t* cells, size_t x, size_t y, uint64_t seed, size_
                     (double)(rng() >> 11) * 0x1.0p-53 < density ? 1 : 0;
     }
     return (int)chosen;
+}
+
+// Uneven multi-grid workloads (batched and serving configurations). One
+// std::mt19937_64(seed) stream, u = (rng() >> 11) * 2^-53, per grid in order:
+//   x = mult * llround(exp(ln lo + u * (ln hi - ln lo)) / mult), clamped to [lo, hi]
+//   y likewise (next draw), density = dlo + u * (dhi - dlo),
+//   gens = llround(exp(ln glo + u * (ln ghi - ln glo))), cell_seed = rng().
+static inline double unit(std::mt19937_64& r) { return (double)(r() >> 11) * 0x1.0p-53; }
+
+void host_workload_uneven(uint64_t seed, uint32_t n, uint32_t lo, uint32_t hi, uint32_t mult,
+                          double dlo, double dhi, uint64_t glo, uint64_t ghi, uint64_t* xs,
+                          uint64_t* ys, double* dens, uint64_t* gens, uint64_t* cell_seeds) {
+    std::mt19937_64 rng(seed);
+    auto side = [&](double u) {
+        const double v = std::exp(std::log((double)lo) + u * (std::log((double)hi) - std::log((double)lo)));
+        long long s = std::llround(v / mult) * (long long)mult;
+        return (uint64_t)std::min<long long>(std::max<long long>(s, lo), hi);
+    };
+    for (uint32_t i = 0; i < n; ++i) {
+        xs[i] = side(unit(rng));
+        ys[i] = side(unit(rng));
+        dens[i] = dlo + unit(rng) * (dhi - dlo);
+        const double g = std::exp(std::log((double)glo) + unit(rng) * (std::log((double)ghi) - std::log((double)glo)));
+        gens[i] = (uint64_t)std::llround(g);
+        cell_seeds[i] = rng();
+    }
+}
+
+// Bernoulli(density) cells in raster order from std::mt19937_64(seed):
+// alive iff (rng() >> 11) * 2^-53 < density.
+void host_bernoulli(uint8_t* cells, size_t n, uint64_t seed, double density) {
+    std::mt19937_64 rng(seed);
+    for (size_t i = 0; i < n; ++i) cells[i] = unit(rng) < density ? 1 : 0;
+}
+
+// Poisson arrivals: t_0 = 0-based exponential gaps of mean 1/rate from
+// std::mt19937_64(seed): t_i = t_{i-1} - ln(1 - u) / rate.
+void host_poisson_arrivals(uint64_t seed, uint32_t n, double rate, double* t) {
+    std::mt19937_64 rng(seed);
+    double now = 0.0;
+    for (uint32_t i = 0; i < n; ++i) {
+        now += -std::log(1.0 - unit(rng)) / rate;
+        t[i] = now;
+    }
 }
 
 } // namespace golb200

@@ -69,6 +69,11 @@ void host_unpack_u8(const uint32_t* words, size_t x, size_t y, uint8_t* cells);
 void host_unpack_i32(const uint32_t* words, size_t x, size_t y, int32_t* cells);
 
 void host_random_ones_zeros(uint8_t* cells, size_t n, uint64_t seed);
+void host_workload_uneven(uint64_t seed, uint32_t n, uint32_t lo, uint32_t hi, uint32_t mult,
+                          double dlo, double dhi, uint64_t glo, uint64_t ghi, uint64_t* xs,
+                          uint64_t* ys, double* dens, uint64_t* gens, uint64_t* cell_seeds);
+void host_bernoulli(uint8_t* cells, size_t n, uint64_t seed, double density);
+void host_poisson_arrivals(uint64_t seed, uint32_t n, double rate, double* t);
 int host_sparse_patches(uint8_t* cells, size_t x, size_t y, uint64_t seed, size_t patch,
                         double fraction, double density);
 

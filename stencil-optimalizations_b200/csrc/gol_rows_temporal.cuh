@@ -155,6 +155,7 @@ struct TemporalCtx {
     int lane, base;
     bool lane_ok;   // this lane's words lie inside the grid
     bool own;       // ... and inside this CTA's slice (not halo): stored
+    int src_l, src_r;   // segmented warps: lanes holding the words left / right
 };
 
 // Copies the row stage 0 consumes at step j (grid row y0 - K + j) into ring
@@ -171,8 +172,12 @@ __device__ __forceinline__ void issue_row(const TemporalCtx& c, int j, int slot)
 // Step body. FAST = steady state: every stage active, every row inside the
 // grid, so no activity tests or row masks (the whole step is one basic
 // block and the K stages' independent chains interleave). LMASK forces the
-// out-of-grid lanes of a partial CTA to stay dead.
-template <int WPL, int K, int PH, bool FAST, bool LMASK, bool TRACK>
+// out-of-grid lanes of a partial CTA to stay dead. SEG = segmented warp: the
+// CTA is one warp cut into segments that each span a whole (narrow) grid
+// row for their own band; neighbours come from explicit shuffle source
+// lanes, segment ends see dead cells, and no shared-memory edge table or
+// barrier is needed (y0/y1 are then per lane, B the common band height).
+template <int WPL, int K, int PH, bool FAST, bool LMASK, bool TRACK, bool SEG = false>
 __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const TemporalCtx& c, int i,
                                               uint32_t lane_mask) {
     constexpr int NEW3 = PH % 3;          // ring-of-3 slot written at this step
@@ -197,11 +202,19 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
                 }
             }
             // Words just left and right of this lane's span.
-            uint32_t lw = __shfl_up_sync(0xffffffffu, P[WPL - 1], 1);
-            uint32_t rw = __shfl_down_sync(0xffffffffu, P[0], 1);
-            const uint32_t ev = c.erd[edge_off(g - 1, PREV3)];
-            lw = c.first_lane ? ev : lw;
-            rw = c.last_lane ? ev : rw;
+            uint32_t lw, rw;
+            if (SEG) {
+                lw = __shfl_sync(0xffffffffu, P[WPL - 1], c.src_l);
+                rw = __shfl_sync(0xffffffffu, P[0], c.src_r);
+                lw = c.first_lane ? 0u : lw;
+                rw = c.last_lane ? 0u : rw;
+            } else {
+                lw = __shfl_up_sync(0xffffffffu, P[WPL - 1], 1);
+                rw = __shfl_down_sync(0xffffffffu, P[0], 1);
+                const uint32_t ev = c.erd[edge_off(g - 1, PREV3)];
+                lw = c.first_lane ? ev : lw;
+                rw = c.last_lane ? ev : rw;
+            }
 #pragma unroll
             for (int w = 0; w < WPL; ++w) {
                 const uint32_t l = (w == 0) ? lw : P[w - 1];
@@ -233,7 +246,7 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
             } else {
 #pragma unroll
                 for (int w = 0; w < WPL; ++w) s.o[g - 1][NEW3][w] = res[w];
-                c.ewr[edge_off(g, NEW3)] = c.last_lane ? res[WPL - 1] : res[0];
+                if (!SEG) c.ewr[edge_off(g, NEW3)] = c.last_lane ? res[WPL - 1] : res[0];
             }
         }
     }
@@ -241,7 +254,7 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
     // Stage 0 (every step, so each step commits exactly one copy group):
     // publish this step's row, issue the row kRowsInFlight steps ahead, and
     // read the next step's row out of the ring.
-    c.ewr[edge_off(0, NEW3)] = c.last_lane ? s.ld[NEW3][WPL - 1] : s.ld[NEW3][0];
+    if (!SEG) c.ewr[edge_off(0, NEW3)] = c.last_lane ? s.ld[NEW3][WPL - 1] : s.ld[NEW3][0];
     // rd_slot holds step i+1's row; step i+kRowsInFlight's row goes kRowsInFlight-1
     // slots further on, into the slot read two steps ago.
     const int wr_slot = s.rd_slot + (kRowsInFlight - 1) - (s.rd_slot >= kRowRing - (kRowsInFlight - 1) ? kRowRing : 0);
@@ -249,16 +262,16 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
     cp_async_wait<kRowsInFlight - 1>();
     lds_words<WPL>(c.ring + s.rd_slot * c.ring_stride, s.ld[(PH + 1) % 3]);
     s.rd_slot = s.rd_slot == kRowRing - 1 ? 0 : s.rd_slot + 1;
-    __syncthreads();
+    if (!SEG) __syncthreads();
 }
 
-template <int WPL, int K, bool FAST, bool LMASK, bool TRACK>
+template <int WPL, int K, bool FAST, bool LMASK, bool TRACK, bool SEG = false>
 __device__ __forceinline__ void temporal_steps(TemporalRegs<WPL, K>& s, const TemporalCtx& c,
                                                int i0, int i1, uint32_t lane_mask) {
     for (int i = i0; i < i1; i += 3) {
-        temporal_step<WPL, K, 0, FAST, LMASK, TRACK>(s, c, i + 0, lane_mask);
-        temporal_step<WPL, K, 1, FAST, LMASK, TRACK>(s, c, i + 1, lane_mask);
-        temporal_step<WPL, K, 2, FAST, LMASK, TRACK>(s, c, i + 2, lane_mask);
+        temporal_step<WPL, K, 0, FAST, LMASK, TRACK, SEG>(s, c, i + 0, lane_mask);
+        temporal_step<WPL, K, 1, FAST, LMASK, TRACK, SEG>(s, c, i + 1, lane_mask);
+        temporal_step<WPL, K, 2, FAST, LMASK, TRACK, SEG>(s, c, i + 2, lane_mask);
     }
 }
 

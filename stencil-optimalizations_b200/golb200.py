@@ -99,6 +99,27 @@ def lib():
                                   ctypes.POINTER(_u64), _vp, _u64]
     L.gol_load_sparse_patches.argtypes = [_vp, _u64, _u64, _u64, _u32, ctypes.c_double,
                                           ctypes.c_double]
+    L.gol_workload_uneven.argtypes = [_u64, _u32, _u32, _u32, _u32, ctypes.c_double,
+                                      ctypes.c_double, _u64, _u64, _vp, _vp, _vp, _vp, _vp]
+    L.gol_load_bernoulli.argtypes = [_vp, _u64, _u64, _u64, ctypes.c_double]
+    L.gol_poisson_arrivals.argtypes = [_u64, _u32, ctypes.c_double, _vp]
+    L.gol_batch_create.argtypes = [ctypes.POINTER(_vp), ctypes.c_int32, _vp]
+    L.gol_batch_add.argtypes = [_vp, _vp, _u64, _u64, _u64, ctypes.POINTER(ctypes.c_int32)]
+    L.gol_batch_set_plan.argtypes = [_vp, ctypes.c_int32, _u32, _u32, _u32]
+    L.gol_batch_plan.argtypes = [_vp, ctypes.c_int32, ctypes.POINTER(_u32), ctypes.POINTER(_u32),
+                                 ctypes.POINTER(_u32), ctypes.POINTER(_u32)]
+    L.gol_batch_upload.argtypes = [_vp]
+    L.gol_batch_run.argtypes = [_vp]
+    L.gol_batch_run_plain.argtypes = [_vp, _u32]
+    L.gol_batch_sync.argtypes = [_vp]
+    L.gol_batch_fetch.argtypes = [_vp, ctypes.c_int32, _vp]
+    L.gol_batch_info.argtypes = [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u64)]
+    L.gol_batch_stream.argtypes = [_vp]
+    L.gol_batch_stream.restype = _vp
+    L.gol_batch_last_error.argtypes = [_vp]
+    L.gol_batch_last_error.restype = ctypes.c_char_p
+    L.gol_batch_destroy.argtypes = [_vp]
+    L.gol_batch_destroy.restype = None
     L.gol_probe_int_peak.argtypes = [ctypes.POINTER(ctypes.c_double), _vp]
     L.gol_abi_version.restype = ctypes.c_int
     L.gol_build_info.restype = ctypes.c_char_p
@@ -322,3 +343,121 @@ def unpack_cells_device(d_words: int, d_cells: int, x: int, y: int, stream: int 
     rc = lib().gol_unpack_cells_device(d_words, d_cells, x, y, stream)
     if rc != GOL_OK:
         raise RuntimeError(f"gol_unpack_cells_device failed with status {rc}")
+
+
+# ---------------------------------------------------------------------------
+# multi-grid workloads and the batched engine
+# ---------------------------------------------------------------------------
+
+def workload_uneven(seed: int, n: int, min_side: int, max_side: int, multiple: int = 64,
+                    density=(0.2, 0.5), gens=(64, 4096)) -> list[dict]:
+    """The documented uneven workload draw (gol_workload_uneven)."""
+    xs = np.empty(n, np.uint64)
+    ys = np.empty(n, np.uint64)
+    ds = np.empty(n, np.float64)
+    gs = np.empty(n, np.uint64)
+    cs = np.empty(n, np.uint64)
+    rc = lib().gol_workload_uneven(seed, n, min_side, max_side, multiple, density[0], density[1],
+                                   gens[0], gens[1], _ptr(xs), _ptr(ys), _ptr(ds), _ptr(gs),
+                                   _ptr(cs))
+    if rc != GOL_OK:
+        raise RuntimeError(f"gol_workload_uneven failed with status {rc}")
+    return [{"x": int(xs[i]), "y": int(ys[i]), "density": float(ds[i]), "gens": int(gs[i]),
+             "cell_seed": int(cs[i])} for i in range(n)]
+
+
+def load_bernoulli(x: int, y: int, seed: int, density: float) -> np.ndarray:
+    out = np.empty((y, x), dtype=np.uint8)
+    rc = lib().gol_load_bernoulli(_ptr(out), x, y, seed, density)
+    if rc != GOL_OK:
+        raise RuntimeError(f"gol_load_bernoulli failed with status {rc}")
+    return out
+
+
+def poisson_arrivals(seed: int, n: int, rate: float) -> np.ndarray:
+    out = np.empty(n, np.float64)
+    rc = lib().gol_poisson_arrivals(seed, n, rate, _ptr(out))
+    if rc != GOL_OK:
+        raise RuntimeError(f"gol_poisson_arrivals failed with status {rc}")
+    return out
+
+
+class GolBatch:
+    """Many grids advanced together by one persistent launch (gol_batch_*)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        self._b = _vp()
+        rc = lib().gol_batch_create(ctypes.byref(self._b), device, stream)
+        if rc != GOL_OK:
+            raise RuntimeError(f"gol_batch_create failed with status {rc}")
+        self.shapes: list[tuple[int, int]] = []
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != GOL_OK:
+            raise RuntimeError(f"{what}: {lib().gol_batch_last_error(self._b).decode()} "
+                               f"(status {rc})")
+
+    def add(self, cells: np.ndarray, generations: int) -> int:
+        g = np.ascontiguousarray(cells, dtype=np.uint8)
+        y, x = g.shape
+        gid = ctypes.c_int32()
+        self._check(lib().gol_batch_add(self._b, _ptr(g), x, y, int(generations),
+                                        ctypes.byref(gid)), "batch_add")
+        self.shapes.append((y, x))
+        return gid.value
+
+    def set_plan(self, gid: int, lane_words: int = 0, temporal_steps: int = 0,
+                 band_rows: int = 0) -> None:
+        self._check(lib().gol_batch_set_plan(self._b, gid, lane_words, temporal_steps, band_rows),
+                    "batch_set_plan")
+
+    def plan(self, gid: int) -> dict:
+        w, k, b, s = _u32(), _u32(), _u32(), _u32()
+        self._check(lib().gol_batch_plan(self._b, gid, ctypes.byref(w), ctypes.byref(k),
+                                         ctypes.byref(b), ctypes.byref(s)), "batch_plan")
+        return {"lane_words": w.value, "temporal_steps": k.value, "band_rows": b.value,
+                "segments": s.value}
+
+    def upload(self) -> None:
+        self._check(lib().gol_batch_upload(self._b), "batch_upload")
+
+    def run(self) -> None:
+        self._check(lib().gol_batch_run(self._b), "batch_run")
+
+    def run_plain(self, temporal_steps: int = 4) -> None:
+        self._check(lib().gol_batch_run_plain(self._b, temporal_steps), "batch_run_plain")
+
+    def sync(self) -> None:
+        self._check(lib().gol_batch_sync(self._b), "batch_sync")
+
+    def fetch(self, gid: int) -> np.ndarray:
+        y, x = self.shapes[gid]
+        out = np.empty((y, x), np.uint8)
+        self._check(lib().gol_batch_fetch(self._b, gid, _ptr(out)), "batch_fetch")
+        return out
+
+    def info(self) -> dict:
+        g, i, c = _u64(), _u64(), _u64()
+        self._check(lib().gol_batch_info(self._b, ctypes.byref(g), ctypes.byref(i), ctypes.byref(c)),
+                    "batch_info")
+        return {"grids": g.value, "items": i.value, "cell_updates": c.value}
+
+    def stream_ptr(self) -> int:
+        return int(lib().gol_batch_stream(self._b) or 0)
+
+    def close(self) -> None:
+        if self._b:
+            lib().gol_batch_destroy(self._b)
+            self._b = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

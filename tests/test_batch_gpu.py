@@ -1,0 +1,85 @@
+"""Batched uneven grids in one persistent launch, on a GPU: every grid's
+result is bit-exact against the oracle (and against the one-launch-per-pass
+baseline), for autotuned and forced plans, narrow (segmented warps) and
+wide (x-sliced) grids, and uneven generation counts."""
+import numpy as np
+import pytest
+
+import golb200
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def small_workload(seed, n, lo=64, hi=1024, gens=(1, 300)):
+    w = golb200.workload_uneven(seed, n, lo, hi, 32, (0.1, 0.5), gens)
+    return [(golb200.load_bernoulli(d["x"], d["y"], d["cell_seed"], d["density"]), d["gens"])
+            for d in w]
+
+
+def test_batch_uneven_vs_oracle():
+    work = small_workload(1, 40)
+    with golb200.GolBatch() as b:
+        ids = [b.add(c, n) for c, n in work]
+        b.run()
+        b.sync()
+        for gid, (c, n) in zip(ids, work):
+            assert np.array_equal(b.fetch(gid), oracle.life_cells(c, n)), (gid, c.shape, n)
+
+
+@pytest.mark.parametrize("wpl,k,band", [(1, 1, 16), (1, 3, 24), (2, 2, 16), (2, 4, 64),
+                                        (4, 4, 32), (4, 1, 48), (1, 4, 8)])
+def test_batch_forced_plans(wpl, k, band):
+    work = small_workload(2 + wpl * 10 + k, 12, lo=128, hi=768, gens=(1, 97))
+    with golb200.GolBatch() as b:
+        ids = []
+        for c, n in work:
+            if c.shape[1] // 32 % wpl:
+                continue
+            gid = b.add(c, n)
+            b.set_plan(gid, wpl, k, band)
+            ids.append((gid, c, n))
+        b.run()
+        b.sync()
+        for gid, c, n in ids:
+            assert np.array_equal(b.fetch(gid), oracle.life_cells(c, n)), (gid, c.shape, n)
+
+
+def test_batch_wide_sliced_and_tiny_grids():
+    work = [(oracle.random_ones_zeros(5120, 40, 3), 37),        # 160 words: x-sliced
+            (oracle.random_ones_zeros(8192, 24, 4), 21),
+            (oracle.random_ones_zeros(32, 1, 5), 9),             # one word, one row
+            (oracle.random_ones_zeros(64, 3, 6), 0),             # zero generations
+            (oracle.random_ones_zeros(4096, 70, 7), 64),
+            (oracle.random_ones_zeros(96, 500, 8), 130)]
+    with golb200.GolBatch() as b:
+        ids = [b.add(c, n) for c, n in work]
+        b.run()
+        b.sync()
+        for gid, (c, n) in zip(ids, work):
+            assert np.array_equal(b.fetch(gid), oracle.life_cells(c, n)), (c.shape, n)
+
+
+def test_batch_matches_plain_and_reruns():
+    work = small_workload(9, 24, lo=256, hi=2048, gens=(10, 400))
+    with golb200.GolBatch() as b:
+        ids = [b.add(c, n) for c, n in work]
+        b.run_plain(4)
+        b.sync()
+        plain = [b.fetch(g) for g in ids]
+        for _ in range(2):                       # re-running restarts from the inputs
+            b.run()
+            b.sync()
+            for g, p in zip(ids, plain):
+                assert np.array_equal(b.fetch(g), p)
+    for (c, n), p in list(zip(work, plain))[:6]:
+        assert np.array_equal(p, oracle.life_cells(c, n))
+
+
+def test_autotuner_uses_segments_for_narrow_grids():
+    with golb200.GolBatch() as b:
+        gid = b.add(np.zeros((2048, 256), np.uint8), 1000)
+        p = b.plan(gid)
+        assert p["segments"] > 1 and p["lane_words"] * (256 // 32 // p["lane_words"]) == 8
+        gid2 = b.add(np.zeros((64, 8192), np.uint8), 10)
+        assert b.plan(gid2)["segments"] == 1
