@@ -180,16 +180,16 @@ int gol_local_stats(gol_engine* e, uint64_t* passes, uint64_t* tiles_per_pass,
 /* --- Stateless device entry points -------------------------------------- */
 
 /* One pass of k generations, d_src -> d_dst (device row grids, x/32 words
- * per row, must not overlap). k in 1..16. band_rows = 0 picks a default.
- * Asynchronous on `stream`. */
+ * per row, 16-byte aligned, must not overlap). k in 1..16. band_rows = 0
+ * picks a default. Asynchronous on `stream`. */
 int gol_rows_pass(const void* d_src, void* d_dst, uint64_t x, uint64_t y, uint32_t k,
                   uint32_t band_rows, void* stream);
 /* Same with the lane width forced (lane_words 1, 2 or 4; 0 = auto). */
 int gol_rows_pass_ex(const void* d_src, void* d_dst, uint64_t x, uint64_t y, uint32_t k,
                      uint32_t band_rows, uint32_t lane_words, void* stream);
 
-/* Packs / unpacks a device cell grid (uint8, nonzero = alive) to / from
- * device row words. x % 32 == 0. */
+/* Packs / unpacks a device cell grid (uint8, nonzero = alive, 16-byte
+ * aligned) to / from device row words. x % 32 == 0. */
 int gol_pack_cells_device(const uint8_t* d_cells, void* d_words, uint64_t x, uint64_t y,
                           void* stream);
 int gol_unpack_cells_device(const void* d_words, uint8_t* d_cells, uint64_t x, uint64_t y,

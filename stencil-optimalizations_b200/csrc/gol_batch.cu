@@ -295,6 +295,7 @@ struct gol_batch {
         golb200::GridChoice choice{};
         int force_wpl = 0, force_k = 0, force_band = 0;
         size_t offset = 0;                // word offset of buf[0] in the arena
+        size_t stride = 0;                // words from buf[0] to buf[1]
         int result_buf = 0;               // buffer holding the last run's result
     };
     std::vector<Entry> grids;
@@ -426,8 +427,11 @@ int gol_batch_upload(gol_batch* b) {
         if (!golb200::choose(e.W, e.Y, e.gens, e.force_wpl, e.force_k, e.force_band, &e.choice))
             return b->fail(GOL_E_UNSUPPORTED, "no batched plan for a grid");
         if (e.gens == 0) e.choice.passes = 0;
+        // Every buffer starts on a 256-byte boundary: lanes move up to 16
+        // bytes at once (uint4 / 16-byte cp.async), whatever the grid sizes.
+        e.stride = ((size_t)e.W * e.Y + 63) / 64 * 64;
         e.offset = words;
-        words += 2 * (size_t)e.W * e.Y;
+        words += 2 * e.stride;
         BatchGrid g{};
         g.W = e.W;
         g.Y = e.Y;
@@ -470,7 +474,7 @@ int gol_batch_upload(gol_batch* b) {
     for (size_t gi = 0; gi < hg.size(); ++gi) {
         auto& e = b->grids[gi];
         hg[gi].buf[0] = b->arena + e.offset;
-        hg[gi].buf[1] = b->arena + e.offset + (size_t)e.W * e.Y;
+        hg[gi].buf[1] = b->arena + e.offset + e.stride;
         ce = cudaMemcpyAsync(hg[gi].buf[0], e.words.data(), e.words.size() * sizeof(uint32_t),
                              cudaMemcpyHostToDevice, b->stream);
         if (ce != cudaSuccess) break;
@@ -565,7 +569,7 @@ int gol_batch_run_plain(gol_batch* b, uint32_t temporal_steps) {
     if ((rc = batch_reset_inputs(b))) return rc;
     const int k0 = temporal_steps ? (int)temporal_steps : 4;
     for (auto& e : b->grids) {
-        uint32_t* buf[2] = {b->arena + e.offset, b->arena + e.offset + (size_t)e.W * e.Y};
+        uint32_t* buf[2] = {b->arena + e.offset, b->arena + e.offset + e.stride};
         int cur = 0;
         uint64_t left = e.gens;
         while (left > 0) {
@@ -590,7 +594,7 @@ int gol_batch_fetch(gol_batch* b, int32_t grid_id, uint8_t* cells) {
     auto& e = b->grids[grid_id];
     const int which = e.result_buf;
     std::vector<uint32_t> words((size_t)e.W * e.Y);
-    cudaError_t ce = cudaMemcpyAsync(words.data(), b->arena + e.offset + (size_t)which * e.W * e.Y,
+    cudaError_t ce = cudaMemcpyAsync(words.data(), b->arena + e.offset + (size_t)which * e.stride,
                                      words.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                                      b->stream);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(b->stream);

@@ -569,6 +569,7 @@ int gol_rows_pass_ex(const void* d_src, void* d_dst, uint64_t x, uint64_t y, uin
                      uint32_t band_rows, uint32_t lane_words, void* stream) {
     if (!d_src || !d_dst || x % 32 || k < 1 || k > (uint32_t)golb200::kMaxTemporalSteps)
         return GOL_E_INVALID;
+    if (((uintptr_t)d_src | (uintptr_t)d_dst) & 15u) return GOL_E_INVALID;   // 16-byte lane accesses
     if (x / 32 > (uint64_t)1 << 30 || y > (uint64_t)1 << 30) return GOL_E_INVALID;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return GOL_E_CUDA;
@@ -585,7 +586,7 @@ int gol_rows_pass_ex(const void* d_src, void* d_dst, uint64_t x, uint64_t y, uin
 int gol_pack_cells_device(const uint8_t* d_cells, void* d_words, uint64_t x, uint64_t y,
                           void* stream) {
     if ((!d_cells || !d_words) && x * y) return GOL_E_INVALID;
-    if (x % 32) return GOL_E_INVALID;
+    if (x % 32 || ((uintptr_t)d_cells & 15u) || ((uintptr_t)d_words & 3u)) return GOL_E_INVALID;
     cudaError_t ce = golb200::launch_pack_cells(d_cells, static_cast<uint32_t*>(d_words), x, y,
                                                 static_cast<cudaStream_t>(stream));
     return ce == cudaSuccess ? GOL_OK : GOL_E_CUDA;
@@ -594,7 +595,7 @@ int gol_pack_cells_device(const uint8_t* d_cells, void* d_words, uint64_t x, uin
 int gol_unpack_cells_device(const void* d_words, uint8_t* d_cells, uint64_t x, uint64_t y,
                             void* stream) {
     if ((!d_cells || !d_words) && x * y) return GOL_E_INVALID;
-    if (x % 32) return GOL_E_INVALID;
+    if (x % 32 || ((uintptr_t)d_cells & 15u) || ((uintptr_t)d_words & 3u)) return GOL_E_INVALID;
     cudaError_t ce = golb200::launch_unpack_cells(static_cast<const uint32_t*>(d_words), d_cells, x,
                                                   y, static_cast<cudaStream_t>(stream));
     return ce == cudaSuccess ? GOL_OK : GOL_E_CUDA;

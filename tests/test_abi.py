@@ -86,6 +86,8 @@ def test_stateless_entry_points_validate_arguments():
     assert L.gol_rows_pass(1, 2, 64, 64, 0, 0, None) == golb200.GOL_E_INVALID
     assert L.gol_rows_pass(1, 2, 64, 64, 17, 0, None) == golb200.GOL_E_INVALID
     assert L.gol_pack_cells_device(1, 2, 33, 1, None) == golb200.GOL_E_INVALID
+    assert L.gol_rows_pass(16 + 8, 64, 64, 64, 1, 0, None) == golb200.GOL_E_INVALID   # misaligned
+    assert L.gol_pack_cells_device(24, 64, 64, 1, None) == golb200.GOL_E_INVALID
 
 
 def test_product_loader_matches_reference_generator(golden_cases):
