@@ -188,6 +188,26 @@ int gol_rows_pass(const void* d_src, void* d_dst, uint64_t x, uint64_t y, uint32
 int gol_rows_pass_ex(const void* d_src, void* d_dst, uint64_t x, uint64_t y, uint32_t k,
                      uint32_t band_rows, uint32_t lane_words, void* stream);
 
+/* No counterpart in the reference (its algorithms always cudaMalloc their own
+ * grids in initialize_data_structures). For callers that cannot allocate
+ * device memory (a framework that owns all memory through its own pool, a
+ * real-time loop that cannot absorb the synchronisation cudaMalloc/cudaFree
+ * can cause, a plugin host that forbids foreign allocations): advances n
+ * generations from d_in into d_out (device row grids, x/32 uint32 words per
+ * row, 16-byte aligned, distinct, not overlapping) and calls no cudaMalloc,
+ * cudaFree or allocating library routine. The passes' ping-pong partner is
+ * a fixed 32 MiB array inside the library (GOL_NOALLOC_MAX_BYTES): grids of
+ * more than that many bytes (x*y/8, e.g. above 16384 x 16384) are rejected
+ * with GOL_E_UNSUPPORTED. Every GPU that loads the library holds that array
+ * until the process exits. The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress, with that device current); make that
+ * first call before any stream capture. All calls share the one array:
+ * calls that overlap on the GPU (other streams, other threads) race and must
+ * be serialised by the caller. k = 0 picks 4. Asynchronous on `stream`. */
+#define GOL_NOALLOC_MAX_BYTES (32u << 20)
+int gol_rows_run_noalloc(const void* d_in, void* d_out, uint64_t x, uint64_t y, uint64_t n,
+                         uint32_t k, void* stream);
+
 /* Packs / unpacks a device cell grid (uint8, nonzero = alive, 16-byte
  * aligned) to / from device row words. x % 32 == 0. */
 int gol_pack_cells_device(const uint8_t* d_cells, void* d_words, uint64_t x, uint64_t y,

@@ -120,6 +120,7 @@ def lib():
     L.gol_batch_last_error.restype = ctypes.c_char_p
     L.gol_batch_destroy.argtypes = [_vp]
     L.gol_batch_destroy.restype = None
+    L.gol_rows_run_noalloc.argtypes = [_vp, _vp, _u64, _u64, _u64, _u32, _vp]
     L.gol_probe_int_peak.argtypes = [ctypes.POINTER(ctypes.c_double), _vp]
     L.gol_abi_version.restype = ctypes.c_int
     L.gol_build_info.restype = ctypes.c_char_p
