@@ -156,6 +156,10 @@ int gol_workload_uneven(uint64_t seed, uint32_t n, uint32_t min_side, uint32_t m
 /* Bernoulli(density) cells, raster order, alive iff (rng() >> 11) * 2^-53 <
  * density for std::mt19937_64(seed). */
 int gol_load_bernoulli(uint8_t* cells, uint64_t x, uint64_t y, uint64_t seed, double density);
+/* Counter-based Bernoulli cells (the serving loop's device-generated inputs):
+ * cell i alive iff (mix64(seed + (i + 1) * 0x9E3779B97F4A7C15) >> 11) * 2^-53
+ * < density. Host only. */
+int gol_load_hash_bernoulli(uint8_t* cells, uint64_t x, uint64_t y, uint64_t seed, double density);
 /* Poisson arrival times (seconds): exponential gaps -ln(1 - u) / rate. */
 int gol_poisson_arrivals(uint64_t seed, uint32_t n, double rate, double* times);
 
@@ -252,6 +256,45 @@ int gol_batch_info(const gol_batch* b, uint64_t* grids, uint64_t* items, uint64_
 void* gol_batch_stream(gol_batch* b);
 const char* gol_batch_last_error(const gol_batch* b);
 void gol_batch_destroy(gol_batch* b);
+
+/* --- Serving: continuous batching of simulations --------------------------- */
+
+/* No reference counterpart. A server owns a device arena (arena_bytes; 0 =
+ * half the free HBM at creation) in which admitted requests keep their two
+ * grid buffers until fetched. gol_serve_step admits queued requests that fit
+ * (arrival order, first fit) and queues one persistent batch launch that
+ * advances every admitted request by up to `quantum` generations (0 = 128);
+ * up to three rounds are queued at once, so requests arriving meanwhile join
+ * the next round while the GPU keeps working. */
+typedef struct gol_server gol_server;
+
+int gol_serve_create(gol_server** out, int32_t device, uint64_t arena_bytes, uint32_t quantum,
+                     void* stream);
+/* Queues a request (host cells, x % 32 == 0); *id identifies it. */
+int gol_serve_submit(gol_server* s, const uint8_t* cells, uint64_t x, uint64_t y,
+                     uint64_t generations, uint64_t* id);
+/* Queues a request whose input is generated on the device at admission:
+ * cell i (raster order) alive iff (mix64(seed + (i + 1) * 0x9E3779B97F4A7C15)
+ * >> 11) * 2^-53 < density, mix64 the SplitMix64 finaliser; the same cells
+ * on the host: gol_load_hash_bernoulli. */
+int gol_serve_submit_random(gol_server* s, uint64_t x, uint64_t y, uint64_t generations,
+                            uint64_t seed, double density, uint64_t* id);
+int gol_serve_step(gol_server* s);
+/* Ids of requests finished since the last call (results ready). */
+int gol_serve_finished(gol_server* s, uint64_t* ids, uint32_t max_ids, uint32_t* count);
+/* Copies a finished request's cells out and frees its arena slot. */
+int gol_serve_fetch(gol_server* s, uint64_t id, uint8_t* cells);
+/* The packed result (x/32 uint32 words per row); frees the slot. */
+int gol_serve_fetch_words(gol_server* s, uint64_t id, void* words);
+/* Drops a finished request without copying it out. */
+int gol_serve_release(gol_server* s, uint64_t id);
+int gol_serve_stats(const gol_server* s, uint64_t* queued, uint64_t* running, uint64_t* rounds,
+                    uint64_t* cell_updates, uint64_t* arena_free_bytes);
+/* Waits for every queued round. */
+int gol_serve_drain(gol_server* s);
+const char* gol_serve_last_error(const gol_server* s);
+void* gol_serve_stream(gol_server* s);
+void gol_serve_destroy(gol_server* s);
 
 /* Library identification: ABI version and the sm arch it was built for. */
 int gol_abi_version(void);

@@ -43,28 +43,6 @@
 
 namespace golb200 {
 
-struct BatchGrid {
-    uint32_t* buf[2];      // ping-pong device grids (W words per row)
-    int W, Y;              // words per row, rows
-    int wpl;               // words per lane
-    int k;                 // depth of full passes
-    int last_k;            // depth of the final pass
-    int passes;            // passes to run (0 = nothing to do)
-    int band;              // rows per segment
-    int seg_lanes;         // L lanes per segment (W / wpl, or 32 when sliced)
-    int segs;              // S segments per warp (1 when sliced)
-    int ngroups;           // band groups
-    int slice;             // words per x-slice (W when unsliced)
-    int nslices;
-    int halo;              // halo words each side of a slice (0 when unsliced)
-    int done_base;         // offset of this grid's (group, slice) counters
-};
-
-struct BatchItem {
-    int grid, group, slice, pass;
-};
-
-constexpr int kBatchMaxK = 4;
 constexpr long long kSpinLimit = 1ll << 24;   // polls of >= 100 ns: a few-second guard
 
 namespace {
@@ -193,8 +171,8 @@ __global__ void __launch_bounds__(32) batch_kernel(const BatchGrid* __restrict__
             }
         }
         const int k = it.pass == G.passes - 1 ? G.last_k : G.k;
-        const uint32_t* src = G.buf[it.pass & 1];
-        uint32_t* dst = G.buf[(it.pass + 1) & 1];
+        const uint32_t* src = G.buf[(G.parity0 + it.pass) & 1];
+        uint32_t* dst = G.buf[(G.parity0 + it.pass + 1) & 1];
         switch (G.wpl) {
             case 4: seg_dispatch<4>(k, G, it.group, it.slice, src, dst, ring); break;
             case 2: seg_dispatch<2>(k, G, it.group, it.slice, src, dst, ring); break;
@@ -226,13 +204,8 @@ struct BatchTuning {
 
 static BatchTuning g_tuning;
 
-struct GridChoice {
-    int wpl, k, band, seg_lanes, segs, ngroups, passes, last_k, slice, nslices, halo;
-    double cost;
-};
-
-static bool choose(int W, int Y, uint64_t gens, int force_wpl, int force_k, int force_band,
-                   GridChoice* out) {
+bool choose_batch_plan(int W, int Y, uint64_t gens, int force_wpl, int force_k, int force_band,
+                       GridChoice* out) {
     bool found = false;
     for (int wpl : {1, 2, 4}) {
         if (force_wpl && wpl != force_wpl) continue;
@@ -271,6 +244,35 @@ static bool choose(int W, int Y, uint64_t gens, int force_wpl, int force_k, int 
         }
     }
     return found;
+}
+
+void batch_grid_from_choice(const GridChoice& ch, int W, int Y, BatchGrid* g) {
+    g->W = W;
+    g->Y = Y;
+    g->wpl = ch.wpl;
+    g->k = ch.k;
+    g->last_k = ch.last_k;
+    g->passes = ch.passes;
+    g->band = ch.band;
+    g->seg_lanes = ch.seg_lanes;
+    g->segs = ch.segs;
+    g->ngroups = ch.ngroups;
+    g->slice = ch.slice;
+    g->nslices = ch.nslices;
+    g->halo = ch.halo;
+}
+
+cudaError_t launch_batch_kernel(const BatchGrid* d_grids, const BatchItem* d_items, int nitems,
+                                int* d_ticket, int* d_done, int* d_status, int num_sms,
+                                cudaStream_t stream) {
+    if (nitems <= 0) return cudaSuccess;
+    int per_sm = 0;
+    cudaError_t ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, 32, 0);
+    if (ce != cudaSuccess) return ce;
+    per_sm = std::max(1, per_sm);
+    const int ctas = std::min(nitems, num_sms * per_sm);   // every CTA resident at once
+    batch_kernel<<<ctas, 32, 0, stream>>>(d_grids, d_items, nitems, d_ticket, d_done, d_status);
+    return cudaPeekAtLastError();
 }
 
 } // namespace golb200
@@ -405,7 +407,7 @@ int gol_batch_plan(const gol_batch* b, int32_t grid_id, uint32_t* lane_words,
     if (!b || grid_id < 0 || grid_id >= (int)b->grids.size()) return GOL_E_INVALID;
     const auto& e = b->grids[grid_id];
     golb200::GridChoice ch;
-    if (!golb200::choose(e.W, e.Y, e.gens, e.force_wpl, e.force_k, e.force_band, &ch))
+    if (!golb200::choose_batch_plan(e.W, e.Y, e.gens, e.force_wpl, e.force_k, e.force_band, &ch))
         return GOL_E_UNSUPPORTED;
     if (lane_words) *lane_words = ch.wpl;
     if (temporal_steps) *temporal_steps = ch.k;
@@ -424,7 +426,7 @@ int gol_batch_upload(gol_batch* b) {
     size_t words = 0;
     int groups = 0, max_passes = 0;
     for (auto& e : b->grids) {
-        if (!golb200::choose(e.W, e.Y, e.gens, e.force_wpl, e.force_k, e.force_band, &e.choice))
+        if (!golb200::choose_batch_plan(e.W, e.Y, e.gens, e.force_wpl, e.force_k, e.force_band, &e.choice))
             return b->fail(GOL_E_UNSUPPORTED, "no batched plan for a grid");
         if (e.gens == 0) e.choice.passes = 0;
         // Every buffer starts on a 256-byte boundary: lanes move up to 16
@@ -433,19 +435,8 @@ int gol_batch_upload(gol_batch* b) {
         e.offset = words;
         words += 2 * e.stride;
         BatchGrid g{};
-        g.W = e.W;
-        g.Y = e.Y;
-        g.wpl = e.choice.wpl;
-        g.k = e.choice.k;
-        g.last_k = e.choice.last_k;
-        g.passes = e.choice.passes;
-        g.band = e.choice.band;
-        g.seg_lanes = e.choice.seg_lanes;
-        g.segs = e.choice.segs;
-        g.ngroups = e.choice.ngroups;
-        g.slice = e.choice.slice;
-        g.nslices = e.choice.nslices;
-        g.halo = e.choice.halo;
+        golb200::batch_grid_from_choice(e.choice, e.W, e.Y, &g);
+        g.parity0 = 0;
         g.done_base = groups;
         groups += g.ngroups * g.nslices;
         max_passes = std::max(max_passes, g.passes);
@@ -522,15 +513,9 @@ int gol_batch_run(gol_batch* b) {
         if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_done, 0, std::max(b->ngroups_total, 1) * sizeof(int), cs);
         if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_ticket, 0, sizeof(int), cs);
         if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_status, 0, sizeof(int), cs);
-        if (ce == cudaSuccess && b->nitems > 0) {
-            int per_sm = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, golb200::batch_kernel, 32, 0);
-            per_sm = std::max(1, per_sm);
-            const int ctas = std::min(b->nitems, b->num_sms * per_sm);   // all resident
-            golb200::batch_kernel<<<ctas, 32, 0, cs>>>(b->d_grids, b->d_items, b->nitems,
-                                                       b->d_ticket, b->d_done, b->d_status);
-            ce = cudaPeekAtLastError();
-        }
+        if (ce == cudaSuccess)
+            ce = golb200::launch_batch_kernel(b->d_grids, b->d_items, b->nitems, b->d_ticket,
+                                              b->d_done, b->d_status, b->num_sms, cs);
         cudaGraph_t g = nullptr;
         cudaError_t ce2 = cudaStreamEndCapture(cs, &g);
         if (ce == cudaSuccess) ce = ce2;

@@ -666,6 +666,12 @@ int gol_poisson_arrivals(uint64_t seed, uint32_t n, double rate, double* times) 
     return GOL_OK;
 }
 
+int gol_load_hash_bernoulli(uint8_t* cells, uint64_t x, uint64_t y, uint64_t seed, double density) {
+    if (!cells && x * y) return GOL_E_INVALID;
+    golb200::host_hash_bernoulli(cells, (size_t)(x * y), seed, density);
+    return GOL_OK;
+}
+
 int gol_probe_int_peak(double* lane_ops_per_s, void* stream) {
     if (!lane_ops_per_s) return GOL_E_INVALID;
     int dev = 0;

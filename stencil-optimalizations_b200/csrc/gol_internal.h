@@ -57,8 +57,56 @@ cudaError_t launch_local_pass(const uint32_t* src, uint32_t* dst, int W, int Y, 
                               const LocalPlan& lp, const LocalState& st, int parity,
                               cudaStream_t stream);
 
+// Batched uneven grids (one persistent launch over a work list).
+struct BatchGrid {
+    uint32_t* buf[2];      // ping-pong device grids (W words per row)
+    int W, Y;              // words per row, rows
+    int wpl;               // words per lane
+    int k;                 // depth of full passes
+    int last_k;            // depth of the final pass
+    int passes;            // passes to run (0 = nothing to do)
+    int band;              // rows per segment
+    int seg_lanes;         // L lanes per segment (W / wpl, or 32 when sliced)
+    int segs;              // S segments per warp (1 when sliced)
+    int ngroups;           // band groups
+    int slice;             // words per x-slice (W when unsliced)
+    int nslices;
+    int halo;              // halo words each side of a slice (0 when unsliced)
+    int done_base;         // offset of this grid's (group, slice) counters
+    int parity0;           // buffer holding the grid at the start of the launch
+};
+
+struct BatchItem {
+    int grid, group, slice, pass;
+};
+
+constexpr int kBatchMaxK = 4;
+
+struct GridChoice {
+    int wpl, k, band, seg_lanes, segs, ngroups, passes, last_k, slice, nslices, halo;
+    double cost;
+};
+
+// The batched autotuner: words per lane, depth and band height for one grid.
+bool choose_batch_plan(int W, int Y, uint64_t gens, int force_wpl, int force_k, int force_band,
+                       GridChoice* out);
+
+// Fills a descriptor from a plan (buffers, progress base and parity set by the caller).
+void batch_grid_from_choice(const GridChoice& ch, int W, int Y, BatchGrid* g);
+
+// Launches the persistent batch kernel over `nitems` items (pass-major
+// order); done[] and *ticket, *status must be zero. All CTAs fit at once.
+cudaError_t launch_batch_kernel(const BatchGrid* d_grids, const BatchItem* d_items, int nitems,
+                                int* d_ticket, int* d_done, int* d_status, int num_sms,
+                                cudaStream_t stream);
+
 cudaError_t launch_pack_cells(const uint8_t* cells, uint32_t* words, size_t x, size_t y,
                               cudaStream_t stream);
+// Counter-based Bernoulli grid written straight into device row words, and
+// the same cells on the host (mix64 hash of the seed and the cell index).
+cudaError_t launch_hash_bernoulli(uint32_t* words, size_t x, size_t y, uint64_t seed,
+                                  double density, cudaStream_t stream);
+void host_hash_bernoulli(uint8_t* cells, size_t n, uint64_t seed, double density);
 cudaError_t launch_unpack_cells(const uint32_t* words, uint8_t* cells, size_t x, size_t y,
                                 cudaStream_t stream);
 

@@ -136,6 +136,30 @@ __global__ void unpack_cells_kernel(const uint32_t* __restrict__ words, uint8_t*
     }
 }
 
+// Counter-based Bernoulli cells: cell i (raster order) of a grid with seed s
+// is alive iff (mix64(s + (i + 1) * 0x9E3779B97F4A7C15) >> 11) * 2^-53 <
+// density, mix64 the SplitMix64 finaliser. Each thread writes one word.
+__host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__global__ void hash_bernoulli_kernel(uint32_t* __restrict__ words, size_t nwords,
+                                      unsigned long long seed, unsigned long long threshold) {
+    for (size_t w = blockIdx.x * (size_t)blockDim.x + threadIdx.x; w < nwords;
+         w += (size_t)gridDim.x * blockDim.x) {
+        uint32_t v = 0;
+        const unsigned long long base = (unsigned long long)w * 32ull;
+#pragma unroll 8
+        for (int b = 0; b < 32; ++b) {
+            const unsigned long long h = mix64(seed + (base + b + 1ull) * 0x9E3779B97F4A7C15ull);
+            v |= (uint32_t)((h >> 11) < threshold) << b;
+        }
+        words[w] = v;
+    }
+}
+
 int grid_for(size_t n, int threads) {
     size_t blocks = (n + threads - 1) / threads;
     return (int)std::min<size_t>(std::max<size_t>(blocks, 1), 148 * 16);
@@ -149,6 +173,27 @@ cudaError_t launch_pack_cells(const uint8_t* cells, uint32_t* words, size_t x, s
     if (n == 0) return cudaSuccess;
     pack_cells_kernel<<<grid_for(n, 256), 256, 0, stream>>>(cells, words, n);
     return cudaPeekAtLastError();
+}
+
+unsigned long long bernoulli_threshold(double density) {
+    if (!(density > 0)) return 0ull;
+    if (density >= 1) return 1ull << 53;
+    return (unsigned long long)(density * 9007199254740992.0);   // density * 2^53
+}
+
+cudaError_t launch_hash_bernoulli(uint32_t* words, size_t x, size_t y, uint64_t seed,
+                                  double density, cudaStream_t stream) {
+    const size_t n = x / 32 * y;
+    if (n == 0) return cudaSuccess;
+    hash_bernoulli_kernel<<<grid_for(n, 256), 256, 0, stream>>>(words, n, seed,
+                                                                  bernoulli_threshold(density));
+    return cudaPeekAtLastError();
+}
+
+void host_hash_bernoulli(uint8_t* cells, size_t n, uint64_t seed, double density) {
+    const unsigned long long t = bernoulli_threshold(density);
+    for (size_t i = 0; i < n; ++i)
+        cells[i] = (mix64(seed + (i + 1ull) * 0x9E3779B97F4A7C15ull) >> 11) < t ? 1 : 0;
 }
 
 cudaError_t launch_unpack_cells(const uint32_t* words, uint8_t* cells, size_t x, size_t y,

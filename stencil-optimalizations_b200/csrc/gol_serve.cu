@@ -1,0 +1,524 @@
+// Serving: continuous batching of Game of Life simulations on one GPU.
+//
+// No counterpart in the reference (it runs one grid per invocation,
+// experiment_manager.hpp:365-394). Requests (grid + generation count) are
+// queued on the host; each round the server
+//   1. admits queued requests, in arrival order, whose two grid buffers fit
+//      in the free space of a device arena sized from free HBM (first fit,
+//      coalescing free list) and copies their packed input in;
+//   2. advances every admitted, unfinished request by up to `quantum`
+//      generations in ONE persistent launch of the batch kernel (the same
+//      dependency-driven work list as gol_batch_run, built for this round,
+//      each grid starting from whichever buffer holds its state);
+//   3. keeps grids resident between rounds; a request that reaches its
+//      generation count is finished once its round's event completes, and
+//      its slot returns to the arena when the caller fetches the result.
+// The state after a round is known in advance (every request advances a
+// fixed number of generations), so round r+1 is planned and queued while
+// round r still runs: up to kRoundsInFlight launches are queued back to
+// back and the GPU does not wait for the host between rounds. Requests
+// arriving meanwhile join the next round planned.
+#include <algorithm>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <new>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "gol_b200.h"
+#include "gol_internal.h"
+
+namespace {
+
+constexpr int kRoundsInFlight = 3;
+
+struct Request {
+    uint64_t id = 0;
+    uint64_t x = 0, y = 0;
+    int W = 0, Y = 0;
+    uint64_t gens = 0;          // requested
+    uint64_t planned = 0;       // generations covered by rounds queued so far
+    std::vector<uint32_t> words;
+    bool device_input = false;  // generated on the device at admission (hash Bernoulli)
+    uint64_t input_seed = 0;
+    double input_density = 0;
+    size_t offset = 0, stride = 0;
+    int parity = 0;             // buffer holding the state after the rounds queued so far
+    golb200::GridChoice plan{};
+    int state = 0;              // 0 queued, 1 admitted, 2 finished (after its last round), 3 fetched
+    int last_round_slot = -1;   // round buffer slot of its final round
+    uint64_t last_round_seq = 0;
+};
+
+struct RoundBuffers {
+    golb200::BatchGrid* d_grids = nullptr;
+    golb200::BatchItem* d_items = nullptr;
+    int* d_done = nullptr;
+    int* d_ticket = nullptr;
+    int* d_status = nullptr;
+    int* h_status = nullptr;                 // pinned copy, written by the round's stream
+    size_t cap_grids = 0, cap_items = 0, cap_done = 0;
+    golb200::BatchGrid* h_grids = nullptr;   // pinned staging
+    golb200::BatchItem* h_items = nullptr;
+    cudaEvent_t done_event = nullptr;
+    bool in_flight = false;
+    uint64_t seq = 0;
+    std::vector<uint64_t> finishing;        // requests whose last round this is
+};
+
+} // namespace
+
+struct gol_server {
+    int device = 0;
+    cudaStream_t stream = nullptr;         // uploads and rounds, in order
+    bool own_stream = false;
+    cudaStream_t copy_stream = nullptr;    // result copies, overlapping later rounds
+    int num_sms = 148;
+    uint32_t* arena = nullptr;
+    size_t arena_words = 0;
+    std::map<size_t, size_t> free_blocks;   // offset -> length (words)
+    uint64_t quantum = 128;
+    uint64_t next_id = 1;
+    std::unordered_map<uint64_t, Request> reqs;
+    std::deque<uint64_t> queue;             // waiting for memory
+    std::vector<uint64_t> running;          // admitted, generations left to plan
+    std::vector<uint64_t> finished;         // completed, not yet reported
+    RoundBuffers rounds[kRoundsInFlight];
+    int next_slot = 0;
+    uint64_t round_seq = 0;
+    uint64_t rounds_launched = 0, admitted = 0, cell_updates_done = 0;
+    int status = 0;
+    std::string err;
+
+    int fail(int code, const std::string& m) {
+        err = m;
+        return code;
+    }
+    int cuda_fail(cudaError_t e, const char* what) {
+        err = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+        return GOL_E_CUDA;
+    }
+};
+
+namespace {
+
+bool arena_alloc(gol_server* s, size_t words, size_t* off) {
+    for (auto it = s->free_blocks.begin(); it != s->free_blocks.end(); ++it) {
+        if (it->second >= words) {
+            *off = it->first;
+            const size_t rest = it->second - words;
+            const size_t at = it->first + words;
+            s->free_blocks.erase(it);
+            if (rest) s->free_blocks[at] = rest;
+            return true;
+        }
+    }
+    return false;
+}
+
+void arena_free(gol_server* s, size_t off, size_t words) {
+    auto it = s->free_blocks.emplace(off, words).first;
+    auto next = std::next(it);
+    if (next != s->free_blocks.end() && it->first + it->second == next->first) {
+        it->second += next->second;
+        s->free_blocks.erase(next);
+    }
+    if (it != s->free_blocks.begin()) {
+        auto prev = std::prev(it);
+        if (prev->first + prev->second == it->first) {
+            prev->second += it->second;
+            s->free_blocks.erase(it);
+        }
+    }
+}
+
+int ensure_round_capacity(gol_server* s, RoundBuffers& r, size_t grids, size_t items, size_t done) {
+    cudaError_t ce = cudaSuccess;
+    auto grow = [&](size_t need, size_t& cap, auto** dptr, auto** hptr) {
+        if (need <= cap || ce != cudaSuccess) return;
+        size_t n = std::max<size_t>(need, cap * 2);
+        if (*dptr) cudaFree(*dptr);
+        if (hptr && *hptr) cudaFreeHost(*hptr);
+        *dptr = nullptr;
+        ce = cudaMalloc(reinterpret_cast<void**>(dptr), n * sizeof(**dptr));
+        if (ce == cudaSuccess && hptr) ce = cudaMallocHost(reinterpret_cast<void**>(hptr), n * sizeof(**hptr));
+        cap = ce == cudaSuccess ? n : 0;
+    };
+    grow(std::max<size_t>(grids, 1), r.cap_grids, &r.d_grids, &r.h_grids);
+    grow(std::max<size_t>(items, 1), r.cap_items, &r.d_items, &r.h_items);
+    grow(std::max<size_t>(done, 1), r.cap_done, &r.d_done, static_cast<int**>(nullptr));
+    if (ce == cudaSuccess && !r.d_ticket) ce = cudaMalloc(&r.d_ticket, sizeof(int));
+    if (ce == cudaSuccess && !r.d_status) ce = cudaMalloc(&r.d_status, sizeof(int));
+    if (ce == cudaSuccess && !r.h_status) ce = cudaMallocHost(&r.h_status, sizeof(int));
+    if (ce == cudaSuccess && !r.done_event) ce = cudaEventCreateWithFlags(&r.done_event, cudaEventDisableTiming);
+    if (ce != cudaSuccess) return s->cuda_fail(ce, "round buffers");
+    return GOL_OK;
+}
+
+// Marks the requests of a completed round finished and checks its status.
+int retire_round(gol_server* s, RoundBuffers& r) {
+    const int st = *r.h_status;           // copied before the round's event was recorded
+    r.in_flight = false;
+    if (st != 0) {
+        s->status = st;
+        return s->fail(st, "a serving round gave up waiting on a dependency");
+    }
+    for (uint64_t id : r.finishing) {
+        auto it = s->reqs.find(id);
+        if (it != s->reqs.end() && it->second.state == 1) {
+            it->second.state = 2;
+            s->finished.push_back(id);
+        }
+    }
+    r.finishing.clear();
+    return GOL_OK;
+}
+
+// Retires every round whose event has completed (wait = block on the oldest).
+int harvest(gol_server* s, bool wait_oldest) {
+    for (;;) {
+        RoundBuffers* oldest = nullptr;
+        for (auto& r : s->rounds)
+            if (r.in_flight && (!oldest || r.seq < oldest->seq)) oldest = &r;
+        if (!oldest) return GOL_OK;
+        cudaError_t q = wait_oldest ? cudaEventSynchronize(oldest->done_event)
+                                    : cudaEventQuery(oldest->done_event);
+        if (q == cudaErrorNotReady) return GOL_OK;
+        if (q != cudaSuccess) return s->cuda_fail(q, "round event");
+        int rc = retire_round(s, *oldest);
+        if (rc) return rc;
+        wait_oldest = false;
+    }
+}
+
+} // namespace
+
+extern "C" {
+
+int gol_serve_create(gol_server** out, int32_t device, uint64_t arena_bytes, uint32_t quantum,
+                     void* stream) {
+    if (!out) return GOL_E_INVALID;
+    *out = nullptr;
+    gol_server* s = new (std::nothrow) gol_server();
+    if (!s) return GOL_E_NOMEM;
+    s->device = device;
+    s->quantum = quantum ? quantum : 128;
+    cudaError_t ce = cudaSetDevice(device);
+    if (ce == cudaSuccess) {
+        if (stream) {
+            s->stream = static_cast<cudaStream_t>(stream);
+        } else {
+            ce = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+            s->own_stream = ce == cudaSuccess;
+        }
+    }
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking);
+    if (ce == cudaSuccess && arena_bytes == 0) {
+        // Admission is bounded by the HBM free when the server starts:
+        // half of it goes to resident grids.
+        size_t fr = 0, tot = 0;
+        ce = cudaMemGetInfo(&fr, &tot);
+        arena_bytes = fr / 2;
+    }
+    if (ce == cudaSuccess) {
+        s->arena_words = arena_bytes / sizeof(uint32_t) / 64 * 64;
+        ce = cudaMalloc(&s->arena, std::max<size_t>(s->arena_words, 64) * sizeof(uint32_t));
+    }
+    if (ce != cudaSuccess) {
+        if (s->own_stream) cudaStreamDestroy(s->stream);
+        if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
+        delete s;
+        return ce == cudaErrorMemoryAllocation ? GOL_E_NOMEM : GOL_E_CUDA;
+    }
+    s->free_blocks[0] = s->arena_words;
+    s->num_sms = golb200::device_sm_count(device);
+    *out = s;
+    return GOL_OK;
+}
+
+int gol_serve_submit(gol_server* s, const uint8_t* cells, uint64_t x, uint64_t y,
+                     uint64_t generations, uint64_t* id) {
+    if (!s) return GOL_E_INVALID;
+    if (!cells || x == 0 || y == 0 || x % 32) return s->fail(GOL_E_INVALID, "x must be a positive multiple of 32");
+    if (y > (1u << 30) || generations > (1ull << 40)) return s->fail(GOL_E_INVALID, "request too large");
+    Request r;
+    r.id = s->next_id++;
+    r.x = x;
+    r.y = y;
+    r.W = (int)(x / 32);
+    r.Y = (int)y;
+    r.gens = generations;
+    r.stride = ((size_t)r.W * r.Y + 63) / 64 * 64;
+    if (2 * r.stride > s->arena_words) return s->fail(GOL_E_NOMEM, "request larger than the device arena");
+    if (!golb200::choose_batch_plan(r.W, r.Y, std::max<uint64_t>(generations, 1), 0, 0, 0, &r.plan))
+        return s->fail(GOL_E_UNSUPPORTED, "no plan for this request");
+    r.words.resize((size_t)r.W * r.Y);
+    golb200::host_pack_u8(cells, x, y, r.words.data());
+    if (id) *id = r.id;
+    s->queue.push_back(r.id);
+    s->reqs.emplace(r.id, std::move(r));
+    return GOL_OK;
+}
+
+// A request whose input is generated on the device when it is admitted:
+// cell i is alive iff (mix64(seed + (i+1) * 0x9E3779B97F4A7C15) >> 11) * 2^-53
+// < density (gol_load_hash_bernoulli gives the same cells on the host).
+int gol_serve_submit_random(gol_server* s, uint64_t x, uint64_t y, uint64_t generations,
+                            uint64_t seed, double density, uint64_t* id) {
+    if (!s) return GOL_E_INVALID;
+    if (x == 0 || y == 0 || x % 32) return s->fail(GOL_E_INVALID, "x must be a positive multiple of 32");
+    if (y > (1u << 30) || generations > (1ull << 40)) return s->fail(GOL_E_INVALID, "request too large");
+    Request r;
+    r.id = s->next_id++;
+    r.x = x;
+    r.y = y;
+    r.W = (int)(x / 32);
+    r.Y = (int)y;
+    r.gens = generations;
+    r.device_input = true;
+    r.input_seed = seed;
+    r.input_density = density;
+    r.stride = ((size_t)r.W * r.Y + 63) / 64 * 64;
+    if (2 * r.stride > s->arena_words) return s->fail(GOL_E_NOMEM, "request larger than the device arena");
+    if (!golb200::choose_batch_plan(r.W, r.Y, std::max<uint64_t>(generations, 1), 0, 0, 0, &r.plan))
+        return s->fail(GOL_E_UNSUPPORTED, "no plan for this request");
+    if (id) *id = r.id;
+    s->queue.push_back(r.id);
+    s->reqs.emplace(r.id, std::move(r));
+    return GOL_OK;
+}
+
+// One scheduling step: retire completed rounds, admit what fits, and queue
+// the next round if any admitted request has generations left. Returns
+// without waiting unless kRoundsInFlight rounds are already queued.
+int gol_serve_step(gol_server* s) {
+    if (!s) return GOL_E_INVALID;
+    if (s->status) return s->fail(s->status, "server stopped after a device-side timeout");
+    cudaError_t ce = cudaSetDevice(s->device);
+    if (ce != cudaSuccess) return s->cuda_fail(ce, "cudaSetDevice");
+    int rc = harvest(s, false);
+    if (rc) return rc;
+
+    // Admission: arrival order; a request that does not fit lets later,
+    // smaller ones through (its memory is reserved for it first next time).
+    for (auto it = s->queue.begin(); it != s->queue.end();) {
+        Request& r = s->reqs[*it];
+        size_t off = 0;
+        if (!arena_alloc(s, 2 * r.stride, &off)) {
+            ++it;
+            continue;
+        }
+        r.offset = off;
+        r.parity = 0;
+        r.state = 1;
+        if (r.device_input) {
+            ce = golb200::launch_hash_bernoulli(s->arena + off, r.x, r.y, r.input_seed,
+                                                r.input_density, s->stream);
+        } else {
+            ce = cudaMemcpyAsync(s->arena + off, r.words.data(), r.words.size() * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice, s->stream);
+        }
+        if (ce != cudaSuccess) return s->cuda_fail(ce, "request upload");
+        std::vector<uint32_t>().swap(r.words);   // a pageable source is staged before the call returns
+        if (r.gens == 0) {               // nothing to run: finished at once
+            r.state = 2;
+            s->finished.push_back(r.id);
+        } else {
+            s->running.push_back(r.id);
+        }
+        ++s->admitted;
+        it = s->queue.erase(it);
+    }
+    if (s->running.empty()) return GOL_OK;
+
+    RoundBuffers& rb = s->rounds[s->next_slot];
+    if (rb.in_flight) {                   // all round slots queued: wait for the oldest
+        rc = harvest(s, true);
+        if (rc) return rc;
+    }
+    // Plan this round: every running request advances min(quantum, left).
+    std::vector<golb200::BatchGrid> grids;
+    int done = 0, max_passes = 0;
+    std::vector<uint64_t> still;
+    for (uint64_t id : s->running) {
+        Request& r = s->reqs[id];
+        const uint64_t left = r.gens - r.planned;
+        const uint64_t g = std::min<uint64_t>(left, s->quantum);
+        golb200::GridChoice ch = r.plan;
+        ch.passes = (int)((g + ch.k - 1) / ch.k);
+        ch.last_k = g % ch.k ? (int)(g % ch.k) : ch.k;
+        golb200::BatchGrid bg{};
+        golb200::batch_grid_from_choice(ch, r.W, r.Y, &bg);
+        bg.buf[0] = s->arena + r.offset;
+        bg.buf[1] = s->arena + r.offset + r.stride;
+        bg.parity0 = r.parity;
+        bg.done_base = done;
+        done += bg.ngroups * bg.nslices;
+        max_passes = std::max(max_passes, bg.passes);
+        grids.push_back(bg);
+        r.planned += g;
+        r.parity = (r.parity + ch.passes) & 1;
+        s->cell_updates_done += r.x * r.y * g;
+        if (r.planned >= r.gens) {
+            rb.finishing.push_back(id);
+        } else {
+            still.push_back(id);
+        }
+    }
+    s->running.swap(still);
+    size_t nitems = 0;
+    for (int p = 0; p < max_passes; ++p)
+        for (const auto& g : grids)
+            if (p < g.passes) nitems += (size_t)g.ngroups * g.nslices;
+    if ((rc = ensure_round_capacity(s, rb, grids.size(), nitems, (size_t)done))) return rc;
+    size_t n = 0;
+    for (int p = 0; p < max_passes; ++p)
+        for (size_t gi = 0; gi < grids.size(); ++gi)
+            if (p < grids[gi].passes)
+                for (int j = 0; j < grids[gi].ngroups; ++j)
+                    for (int sl = 0; sl < grids[gi].nslices; ++sl)
+                        rb.h_items[n++] = {(int)gi, j, sl, p};
+    std::memcpy(rb.h_grids, grids.data(), grids.size() * sizeof(golb200::BatchGrid));
+    ce = cudaMemcpyAsync(rb.d_grids, rb.h_grids, grids.size() * sizeof(golb200::BatchGrid),
+                         cudaMemcpyHostToDevice, s->stream);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(rb.d_items, rb.h_items, nitems * sizeof(golb200::BatchItem),
+                             cudaMemcpyHostToDevice, s->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(rb.d_done, 0, (size_t)std::max(done, 1) * sizeof(int), s->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(rb.d_ticket, 0, sizeof(int), s->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(rb.d_status, 0, sizeof(int), s->stream);
+    if (ce == cudaSuccess)
+        ce = golb200::launch_batch_kernel(rb.d_grids, rb.d_items, (int)nitems, rb.d_ticket, rb.d_done,
+                                          rb.d_status, s->num_sms, s->stream);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(rb.h_status, rb.d_status, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+    if (ce == cudaSuccess) ce = cudaEventRecord(rb.done_event, s->stream);
+    if (ce != cudaSuccess) return s->cuda_fail(ce, "round launch");
+    rb.in_flight = true;
+    rb.seq = ++s->round_seq;
+    for (uint64_t id : rb.finishing) {
+        s->reqs[id].last_round_slot = s->next_slot;
+        s->reqs[id].last_round_seq = rb.seq;
+    }
+    ++s->rounds_launched;
+    s->next_slot = (s->next_slot + 1) % kRoundsInFlight;
+    return GOL_OK;
+}
+
+// Ids finished since the last call (their results are ready to fetch).
+int gol_serve_finished(gol_server* s, uint64_t* ids, uint32_t max_ids, uint32_t* count) {
+    if (!s || !count) return GOL_E_INVALID;
+    int rc = harvest(s, false);
+    if (rc) return rc;
+    const uint32_t n = (uint32_t)std::min<size_t>(s->finished.size(), max_ids);
+    for (uint32_t i = 0; i < n; ++i) ids[i] = s->finished[i];
+    s->finished.erase(s->finished.begin(), s->finished.begin() + n);
+    *count = n;
+    return GOL_OK;
+}
+
+// Copies a finished request's grid out and returns its slot to the arena.
+int gol_serve_fetch(gol_server* s, uint64_t id, uint8_t* cells) {
+    if (!s || !cells) return GOL_E_INVALID;
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return s->fail(GOL_E_INVALID, "unknown request");
+    Request& r = it->second;
+    if (r.state != 2) return s->fail(GOL_E_STATE, "request not finished");
+    // Its last round has completed and no later round touches its slot, so
+    // the copy runs on its own stream, beside the rounds still queued. A
+    // request with no generations never ran: wait for its upload instead.
+    cudaError_t ce = cudaSuccess;
+    if (r.gens == 0) ce = cudaStreamSynchronize(s->stream);
+    std::vector<uint32_t> words((size_t)r.W * r.Y);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(words.data(), s->arena + r.offset + (size_t)r.parity * r.stride,
+                             words.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->copy_stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->copy_stream);
+    if (ce != cudaSuccess) return s->cuda_fail(ce, "result copy");
+    golb200::host_unpack_u8(words.data(), r.x, r.y, cells);
+    arena_free(s, r.offset, 2 * r.stride);
+    s->reqs.erase(it);
+    return GOL_OK;
+}
+
+// Packed result (x/32 uint32 words per row) of a finished request; frees its slot.
+int gol_serve_fetch_words(gol_server* s, uint64_t id, void* words) {
+    if (!s || !words) return GOL_E_INVALID;
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return s->fail(GOL_E_INVALID, "unknown request");
+    Request& r = it->second;
+    if (r.state != 2) return s->fail(GOL_E_STATE, "request not finished");
+    cudaError_t ce = cudaSuccess;
+    if (r.gens == 0) ce = cudaStreamSynchronize(s->stream);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(words, s->arena + r.offset + (size_t)r.parity * r.stride,
+                             (size_t)r.W * r.Y * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->copy_stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->copy_stream);
+    if (ce != cudaSuccess) return s->cuda_fail(ce, "result copy");
+    arena_free(s, r.offset, 2 * r.stride);
+    s->reqs.erase(it);
+    return GOL_OK;
+}
+
+// Drops a finished request without copying it out.
+int gol_serve_release(gol_server* s, uint64_t id) {
+    if (!s) return GOL_E_INVALID;
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return s->fail(GOL_E_INVALID, "unknown request");
+    if (it->second.state != 2) return s->fail(GOL_E_STATE, "request not finished");
+    arena_free(s, it->second.offset, 2 * it->second.stride);
+    s->reqs.erase(it);
+    return GOL_OK;
+}
+
+// Queued (waiting for memory), running, and finished-but-unfetched counts.
+int gol_serve_stats(const gol_server* s, uint64_t* queued, uint64_t* running, uint64_t* rounds,
+                    uint64_t* cell_updates, uint64_t* arena_free_bytes) {
+    if (!s) return GOL_E_INVALID;
+    size_t fr = 0;
+    for (const auto& b : s->free_blocks) fr += b.second;
+    if (queued) *queued = s->queue.size();
+    if (running) *running = s->running.size();
+    if (rounds) *rounds = s->rounds_launched;
+    if (cell_updates) *cell_updates = s->cell_updates_done;
+    if (arena_free_bytes) *arena_free_bytes = fr * sizeof(uint32_t);
+    return GOL_OK;
+}
+
+// Waits for every queued round.
+int gol_serve_drain(gol_server* s) {
+    if (!s) return GOL_E_INVALID;
+    for (int i = 0; i < kRoundsInFlight; ++i) {
+        int rc = harvest(s, true);
+        if (rc) return rc;
+    }
+    return GOL_OK;
+}
+
+const char* gol_serve_last_error(const gol_server* s) { return s ? s->err.c_str() : "null server"; }
+
+void* gol_serve_stream(gol_server* s) { return s ? static_cast<void*>(s->stream) : nullptr; }
+
+void gol_serve_destroy(gol_server* s) {
+    if (!s) return;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (auto& r : s->rounds) {
+        if (r.d_grids) cudaFree(r.d_grids);
+        if (r.d_items) cudaFree(r.d_items);
+        if (r.d_done) cudaFree(r.d_done);
+        if (r.d_ticket) cudaFree(r.d_ticket);
+        if (r.d_status) cudaFree(r.d_status);
+        if (r.h_grids) cudaFreeHost(r.h_grids);
+        if (r.h_status) cudaFreeHost(r.h_status);
+        if (r.h_items) cudaFreeHost(r.h_items);
+        if (r.done_event) cudaEventDestroy(r.done_event);
+    }
+    if (s->arena) cudaFree(s->arena);
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+} // extern "C"

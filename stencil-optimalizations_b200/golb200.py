@@ -121,6 +121,24 @@ def lib():
     L.gol_batch_destroy.argtypes = [_vp]
     L.gol_batch_destroy.restype = None
     L.gol_rows_run_noalloc.argtypes = [_vp, _vp, _u64, _u64, _u64, _u32, _vp]
+    L.gol_load_hash_bernoulli.argtypes = [_vp, _u64, _u64, _u64, ctypes.c_double]
+    L.gol_serve_create.argtypes = [ctypes.POINTER(_vp), ctypes.c_int32, _u64, _u32, _vp]
+    L.gol_serve_submit.argtypes = [_vp, _vp, _u64, _u64, _u64, ctypes.POINTER(_u64)]
+    L.gol_serve_submit_random.argtypes = [_vp, _u64, _u64, _u64, _u64, ctypes.c_double,
+                                          ctypes.POINTER(_u64)]
+    L.gol_serve_step.argtypes = [_vp]
+    L.gol_serve_finished.argtypes = [_vp, _vp, _u32, ctypes.POINTER(_u32)]
+    L.gol_serve_fetch.argtypes = [_vp, _u64, _vp]
+    L.gol_serve_fetch_words.argtypes = [_vp, _u64, _vp]
+    L.gol_serve_release.argtypes = [_vp, _u64]
+    L.gol_serve_stats.argtypes = [_vp] + [ctypes.POINTER(_u64)] * 5
+    L.gol_serve_drain.argtypes = [_vp]
+    L.gol_serve_last_error.argtypes = [_vp]
+    L.gol_serve_last_error.restype = ctypes.c_char_p
+    L.gol_serve_stream.argtypes = [_vp]
+    L.gol_serve_stream.restype = _vp
+    L.gol_serve_destroy.argtypes = [_vp]
+    L.gol_serve_destroy.restype = None
     L.gol_probe_int_peak.argtypes = [ctypes.POINTER(ctypes.c_double), _vp]
     L.gol_abi_version.restype = ctypes.c_int
     L.gol_build_info.restype = ctypes.c_char_p
@@ -450,6 +468,101 @@ class GolBatch:
         if self._b:
             lib().gol_batch_destroy(self._b)
             self._b = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def load_hash_bernoulli(x: int, y: int, seed: int, density: float) -> np.ndarray:
+    """The cells gol_serve_submit_random generates on the device."""
+    out = np.empty((y, x), dtype=np.uint8)
+    rc = lib().gol_load_hash_bernoulli(_ptr(out), x, y, seed, density)
+    if rc != GOL_OK:
+        raise RuntimeError(f"gol_load_hash_bernoulli failed with status {rc}")
+    return out
+
+
+class GolServer:
+    """Continuous-batching server (gol_serve_*): requests stay resident on the
+    device and advance together, one persistent launch per round."""
+
+    def __init__(self, device: int = 0, arena_bytes: int = 0, quantum: int = 128,
+                 stream: int | None = None):
+        self._s = _vp()
+        rc = lib().gol_serve_create(ctypes.byref(self._s), device, arena_bytes, quantum, stream)
+        if rc != GOL_OK:
+            raise RuntimeError(f"gol_serve_create failed with status {rc}")
+        self.shapes: dict[int, tuple[int, int]] = {}
+        self._ids = np.zeros(4096, np.uint64)
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != GOL_OK:
+            raise RuntimeError(f"{what}: {lib().gol_serve_last_error(self._s).decode()} "
+                               f"(status {rc})")
+
+    def submit(self, cells: np.ndarray, generations: int) -> int:
+        g = np.ascontiguousarray(cells, dtype=np.uint8)
+        y, x = g.shape
+        rid = _u64()
+        self._check(lib().gol_serve_submit(self._s, _ptr(g), x, y, int(generations),
+                                           ctypes.byref(rid)), "serve_submit")
+        self.shapes[rid.value] = (y, x)
+        return rid.value
+
+    def submit_random(self, x: int, y: int, generations: int, seed: int, density: float) -> int:
+        rid = _u64()
+        self._check(lib().gol_serve_submit_random(self._s, x, y, int(generations), seed, density,
+                                                  ctypes.byref(rid)), "serve_submit_random")
+        self.shapes[rid.value] = (y, x)
+        return rid.value
+
+    def step(self) -> None:
+        self._check(lib().gol_serve_step(self._s), "serve_step")
+
+    def finished(self) -> list[int]:
+        n = _u32()
+        self._check(lib().gol_serve_finished(self._s, _ptr(self._ids), self._ids.size,
+                                             ctypes.byref(n)), "serve_finished")
+        return [int(v) for v in self._ids[:n.value]]
+
+    def fetch(self, rid: int) -> np.ndarray:
+        y, x = self.shapes.pop(rid)
+        out = np.empty((y, x), np.uint8)
+        self._check(lib().gol_serve_fetch(self._s, rid, _ptr(out)), "serve_fetch")
+        return out
+
+    def fetch_words(self, rid: int) -> np.ndarray:
+        y, x = self.shapes.pop(rid)
+        out = np.empty((y, x // 32), np.uint32)
+        self._check(lib().gol_serve_fetch_words(self._s, rid, _ptr(out)), "serve_fetch_words")
+        return out
+
+    def release(self, rid: int) -> None:
+        self.shapes.pop(rid, None)
+        self._check(lib().gol_serve_release(self._s, rid), "serve_release")
+
+    def stats(self) -> dict:
+        v = [_u64() for _ in range(5)]
+        self._check(lib().gol_serve_stats(self._s, *[ctypes.byref(a) for a in v]), "serve_stats")
+        return dict(zip(["queued", "running", "rounds", "cell_updates", "arena_free_bytes"],
+                        [a.value for a in v]))
+
+    def drain(self) -> None:
+        self._check(lib().gol_serve_drain(self._s), "serve_drain")
+
+    def close(self) -> None:
+        if self._s:
+            lib().gol_serve_destroy(self._s)
+            self._s = _vp()
 
     def __del__(self):
         try:
