@@ -65,6 +65,10 @@ def parse_args():
     ap.add_argument("--k", type=int, default=0, help="temporal depth (0 = sweep)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-check", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the sparse, batched and serving measurements")
+    ap.add_argument("--only", choices=["sparse", "batched", "serving"],
+                    help="measure just that configuration and print it")
     return ap.parse_args()
 
 
@@ -278,6 +282,98 @@ def ncu_traffic(k: int, wpl: int) -> float | None:
     return None if ent is None else float(ent["dram_bytes_per_launch"])
 
 
+# ---------------------------------------------------------------------------
+# the other configurations (reported beside the dense headline, N = 1)
+# ---------------------------------------------------------------------------
+
+def _events_ms(stream, fn, sync):
+    import torch
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    fn()
+    b.record(stream)
+    sync()
+    b.synchronize()
+    return a.elapsed_time(b)
+
+
+def bench_sparse(stream, device) -> dict:
+    """16384^2 all-dead grid, 1% of 64x64 slots Bernoulli(0.35), 20000
+    generations: change-tracking tiles vs the dense engine, same input."""
+    import golb200
+    size, gens, seed = SIZE, 20000, SEED
+    g = golb200.load_sparse_patches(size, size, seed, 64, 0.01, 0.35)
+    out = {"workload": f"{size}x{size} dead grid, 1% of 64x64 slots Bernoulli(0.35) seed {seed}, "
+                       f"{gens} generations", "unit": UNIT}
+    results = {}
+    for name, kw in (("local", dict(algorithm="local", temporal_steps=8)),
+                     ("dense", dict(temporal_steps=4))):
+        e = golb200.GolB200(grid_dimensions=(size, size), device=device, stream=stream.cuda_stream, **kw)
+        e.set_and_format_input_data(g)
+        e.initialize_data_structures()
+        ms = _events_ms(stream, lambda: e.run(gens), e.sync)
+        out[f"value_{name}"] = size * size * gens / (ms * 1e-3) / 1e9
+        if name == "local":
+            st = e.local_stats()
+            out["computed_tile_fraction"] = st["computed_tiles"] / max(1, st["passes"] * st["tiles_per_pass"])
+        e.finalize_data_structures()
+        results[name] = e.fetch_words(64)
+        e.close()
+    out["local_equals_dense"] = bool(np.array_equal(results["local"], results["dense"]))
+    return out
+
+
+def bench_batched(stream, device, n: int = 512, seed: int = SEED) -> dict:
+    """512 grids, sides log-uniform [256, 4096] (multiples of 64), density
+    U[0.2, 0.5], generations log-uniform [64, 4096]: one persistent launch
+    vs one launch per pass per grid on the same GPU."""
+    import concurrent.futures as cf
+
+    import golb200
+    work = golb200.workload_uneven(seed, n, 256, 4096, 64, (0.2, 0.5), (64, 4096))
+    b = golb200.GolBatch(device=device, stream=stream.cuda_stream)
+    with cf.ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as pool:
+        for i in range(0, n, 32):
+            chunk = work[i:i + 32]
+            grids = list(pool.map(lambda d: golb200.load_bernoulli(d["x"], d["y"], d["cell_seed"],
+                                                                   d["density"]), chunk))
+            for d, c in zip(chunk, grids):
+                b.add(c, d["gens"])
+    b.upload()
+    info = b.info()
+    b.run()
+    b.sync()                                        # warm-up (and graph capture)
+    batched = [_events_ms(stream, b.run, b.sync) for _ in range(3)]
+    sample = [b.fetch(i) for i in range(0, n, 64)]
+    b.run_plain(4)
+    b.sync()
+    plain = [_events_ms(stream, lambda: b.run_plain(4), b.sync) for _ in range(2)]
+    same = all(np.array_equal(b.fetch(i), s) for i, s in zip(range(0, n, 64), sample))
+    b.close()
+    cu = info["cell_updates"]
+    vb = cu / (min(batched) * 1e-3) / 1e9
+    vp = cu / (min(plain) * 1e-3) / 1e9
+    return {"workload": f"{n} grids, sides log-uniform [256, 4096] x64, density U[0.2, 0.5], "
+                        f"generations log-uniform [64, 4096], seed {seed}",
+            "cell_updates": cu, "work_items": info["items"], "unit": UNIT,
+            "value_batched": vb, "value_plain_per_grid": vp, "speedup": vb / vp,
+            "ms_batched": min(batched), "ms_plain": min(plain),
+            "batched_equals_plain_on_sample": same}
+
+
+def bench_serving(device) -> dict:
+    """Poisson stream, mean 2000 requests/s, sides log-uniform [128, 8192]
+    (multiples of 64), density U[0.1, 0.5], generations log-uniform
+    [16, 8192], inputs generated on the device, results copied back."""
+    import serve
+    r = serve.run_stream(rate=2000.0, seconds=2.0, seed=SEED, device=device)
+    r["workload"] = ("Poisson arrivals, mean 2000 req/s for 2 s, sides log-uniform [128, 8192] x64, "
+                     "density U[0.1, 0.5], generations log-uniform [16, 8192], seed 42")
+    r["unit_throughput"] = "cell-updates/s"
+    return r
+
+
 def run_ours(args, d: Dist) -> None:
     import torch
 
@@ -441,6 +537,12 @@ def run_ours(args, d: Dist) -> None:
     if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(cells)
 
+    sparse = batched = serving = None
+    if d.rank == 0 and d.world == 1 and not args.no_extras:
+        sparse = bench_sparse(stream, d.local_rank)
+        batched = bench_batched(stream, d.local_rank)
+        serving = bench_serving(d.local_rank)
+
     if d.rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world,
@@ -476,6 +578,9 @@ def run_ours(args, d: Dist) -> None:
                         "peak = live LOP3 probe (gol_probe_int_peak)",
             },
             "variant_8192_32bit": var,
+            "sparse_settling": sparse,
+            "batched_uneven": batched,
+            "serving": serving,
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": grid_bytes, "d2h_bytes_per_step": grid_bytes,
                     "phases_ms_median": {k: statistics.median(v) for k, v in phases.items()},
@@ -496,6 +601,14 @@ def main():
         run_reference_arm(args, d)      # rank 0 only; no process group needed
         return
     import torch
+    if args.only:
+        torch.cuda.set_device(d.local_rank)
+        s = torch.cuda.Stream()
+        fn = {"sparse": lambda: bench_sparse(s, d.local_rank),
+              "batched": lambda: bench_batched(s, d.local_rank),
+              "serving": lambda: bench_serving(d.local_rank)}[args.only]
+        print(json.dumps({args.only: fn()}), flush=True)
+        return
     if d.world > 1:
         torch.cuda.set_device(d.local_rank)
     d.init("nccl")

@@ -13,9 +13,10 @@
 //               cut into slices of 30 lanes plus a halo lane each side
 //               (errors from the unknown cells beyond the halo move one cell
 //               per generation and stay in the halo for k <= 32).
-//   order       items are numbered pass-major (all pass-0 items of every
-//               grid, then pass 1, ...); persistent one-warp CTAs take
-//               tickets from an atomic counter.
+//   order       items are numbered critical-path first: by descending
+//               remaining passes of their grid, so the longest grids start
+//               at once and short ones fill in; persistent one-warp CTAs
+//               take tickets from an atomic counter.
 //   dependency  (g, s, j, p) needs (g, s-1..s+1, j-1..j+1, p-1) finished:
 //               that is every word it reads, and it also ends every read of
 //               the buffer it overwrites. A per-group counter holds the passes done; the
@@ -191,11 +192,17 @@ __global__ void __launch_bounds__(32) batch_kernel(const BatchGrid* __restrict__
 //
 // Model: a work item costs (band + 3k) pipeline steps of k stages on one
 // warp, and a stage-step on a WPL-wide lane costs c[WPL] (relative warp
-// time, from calibration). A grid's cost is
+// time). A grid's work is
 //     passes * nslices * ngroups * (band + 3k) * k * c[WPL]
-// for passes = ceil(gens / k), ngroups = ceil(Y / (S * band)). The candidate
-// set is WPL in {1, 2, 4} (W % WPL == 0), k in 1..4, band in
-// {16, 24, 32, 48, 64} with band >= 2k; the cheapest wins.
+// for passes = ceil(gens / k), ngroups = ceil(Y / (S * band)), and its
+// dependency chain (one item per pass, in order) is
+//     passes * (band + 3k) * k * c[WPL].
+// A batch takes about max(total work / resident warps, longest chain), so a
+// first choice minimises work alone; grids whose chain would outlast the
+// batch's work-bound time are then re-planned to minimise work / resident
+// warps + chain (shorter bands: more, quicker items per pass). Candidates:
+// WPL in {1, 2, 4} (W % WPL == 0), k in 1..4, band in {16, 24, 32, 48, 64}
+// with band >= 2k.
 // ---------------------------------------------------------------------------
 
 struct BatchTuning {
@@ -205,7 +212,7 @@ struct BatchTuning {
 static BatchTuning g_tuning;
 
 bool choose_batch_plan(int W, int Y, uint64_t gens, int force_wpl, int force_k, int force_band,
-                       GridChoice* out) {
+                       GridChoice* out, double parallel, double crit_weight) {
     bool found = false;
     for (int wpl : {1, 2, 4}) {
         if (force_wpl && wpl != force_wpl) continue;
@@ -224,7 +231,10 @@ bool choose_batch_plan(int W, int Y, uint64_t gens, int force_wpl, int force_k, 
                 const uint64_t passes = (gens + k - 1) / k;
                 const double cost = (double)passes * nslices * ngroups * (band + 3 * k) * k *
                                     g_tuning.c[wpl];
-                if (!found || cost < out->cost) {
+                // one item per pass on the chain of dependent passes
+                const double crit = (double)passes * (band + 3 * k) * k * g_tuning.c[wpl];
+                const double score = cost / std::max(parallel, 1.0) + crit_weight * crit;
+                if (!found || score < out->score) {
                     found = true;
                     out->wpl = wpl;
                     out->k = k;
@@ -238,12 +248,43 @@ bool choose_batch_plan(int W, int Y, uint64_t gens, int force_wpl, int force_k, 
                     out->nslices = nslices;
                     out->halo = sliced ? wpl : 0;
                     out->cost = cost;
+                    out->crit = crit;
+                    out->score = score;
                 }
                 if (force_band) break;
             }
         }
     }
     return found;
+}
+
+size_t count_batch_items(const BatchGrid* grids, size_t ngrids) {
+    size_t n = 0;
+    for (size_t g = 0; g < ngrids; ++g)
+        n += (size_t)grids[g].passes * grids[g].ngroups * grids[g].nslices;
+    return n;
+}
+
+size_t order_batch_items(const BatchGrid* grids, size_t ngrids, BatchItem* out) {
+    int max_passes = 0;
+    for (size_t g = 0; g < ngrids; ++g) max_passes = std::max(max_passes, grids[g].passes);
+    size_t n = 0;
+    for (int rem = max_passes; rem >= 1; --rem)
+        for (size_t g = 0; g < ngrids; ++g) {
+            const BatchGrid& G = grids[g];
+            if (G.passes < rem) continue;
+            const int p = G.passes - rem;
+            for (int j = 0; j < G.ngroups; ++j)
+                for (int sl = 0; sl < G.nslices; ++sl) out[n++] = {(int)g, j, sl, p};
+        }
+    return n;
+}
+
+int batch_kernel_ctas_per_sm() {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, 32, 0) != cudaSuccess)
+        per_sm = 1;
+    return std::max(1, per_sm);
 }
 
 void batch_grid_from_choice(const GridChoice& ch, int W, int Y, BatchGrid* g) {
@@ -425,9 +466,23 @@ int gol_batch_upload(gol_batch* b) {
     std::vector<BatchGrid> hg;
     size_t words = 0;
     int groups = 0, max_passes = 0;
+    // Plans: least work first, then shorter chains for the grids whose
+    // chain would outlast the work-bound time of the whole batch.
+    const double parallel = (double)b->num_sms * golb200::batch_kernel_ctas_per_sm();
+    double total_work = 0;
     for (auto& e : b->grids) {
-        if (!golb200::choose_batch_plan(e.W, e.Y, e.gens, e.force_wpl, e.force_k, e.force_band, &e.choice))
+        if (!golb200::choose_batch_plan(e.W, e.Y, std::max<uint64_t>(e.gens, 1), e.force_wpl,
+                                        e.force_k, e.force_band, &e.choice))
             return b->fail(GOL_E_UNSUPPORTED, "no batched plan for a grid");
+        total_work += e.choice.cost;
+    }
+    const double work_time = total_work / parallel;
+    for (auto& e : b->grids) {
+        if (e.choice.crit > 0.5 * work_time && !(e.force_wpl && e.force_k && e.force_band))
+            golb200::choose_batch_plan(e.W, e.Y, std::max<uint64_t>(e.gens, 1), e.force_wpl, e.force_k,
+                                       e.force_band, &e.choice, parallel, 1.0);
+    }
+    for (auto& e : b->grids) {
         if (e.gens == 0) e.choice.passes = 0;
         // Every buffer starts on a 256-byte boundary: lanes move up to 16
         // bytes at once (uint4 / 16-byte cp.async), whatever the grid sizes.
@@ -442,12 +497,8 @@ int gol_batch_upload(gol_batch* b) {
         max_passes = std::max(max_passes, g.passes);
         hg.push_back(g);
     }
-    std::vector<BatchItem> items;
-    for (int p = 0; p < max_passes; ++p)
-        for (size_t gi = 0; gi < hg.size(); ++gi)
-            if (p < hg[gi].passes)
-                for (int j = 0; j < hg[gi].ngroups; ++j)
-                    for (int sl = 0; sl < hg[gi].nslices; ++sl) items.push_back({(int)gi, j, sl, p});
+    std::vector<BatchItem> items(golb200::count_batch_items(hg.data(), hg.size()));
+    golb200::order_batch_items(hg.data(), hg.size(), items.data());
     b->nitems = (int)items.size();
     b->ngroups_total = groups;
     b->arena_words = words;

@@ -84,12 +84,24 @@ constexpr int kBatchMaxK = 4;
 
 struct GridChoice {
     int wpl, k, band, seg_lanes, segs, ngroups, passes, last_k, slice, nslices, halo;
-    double cost;
+    double cost;    // total work
+    double crit;    // dependency chain
+    double score;   // what the autotuner minimised
 };
 
 // The batched autotuner: words per lane, depth and band height for one grid.
+// Minimises work / parallel + crit_weight * (the grid's dependency chain).
 bool choose_batch_plan(int W, int Y, uint64_t gens, int force_wpl, int force_k, int force_band,
-                       GridChoice* out);
+                       GridChoice* out, double parallel = 1.0, double crit_weight = 0.0);
+
+// Emits the work items of `grids` in critical-path-first order: descending
+// remaining passes (passes - pass), so long grids start first and every
+// dependency (same grid, previous pass) has a smaller ticket. Returns the count.
+size_t order_batch_items(const BatchGrid* grids, size_t ngrids, BatchItem* out);
+size_t count_batch_items(const BatchGrid* grids, size_t ngrids);
+
+// Resident one-warp CTAs per SM of the batch kernel.
+int batch_kernel_ctas_per_sm();
 
 // Fills a descriptor from a plan (buffers, progress base and parity set by the caller).
 void batch_grid_from_choice(const GridChoice& ch, int W, int Y, BatchGrid* g);

@@ -368,18 +368,10 @@ int gol_serve_step(gol_server* s) {
         }
     }
     s->running.swap(still);
-    size_t nitems = 0;
-    for (int p = 0; p < max_passes; ++p)
-        for (const auto& g : grids)
-            if (p < g.passes) nitems += (size_t)g.ngroups * g.nslices;
+    const size_t nitems = golb200::count_batch_items(grids.data(), grids.size());
     if ((rc = ensure_round_capacity(s, rb, grids.size(), nitems, (size_t)done))) return rc;
-    size_t n = 0;
-    for (int p = 0; p < max_passes; ++p)
-        for (size_t gi = 0; gi < grids.size(); ++gi)
-            if (p < grids[gi].passes)
-                for (int j = 0; j < grids[gi].ngroups; ++j)
-                    for (int sl = 0; sl < grids[gi].nslices; ++sl)
-                        rb.h_items[n++] = {(int)gi, j, sl, p};
+    golb200::order_batch_items(grids.data(), grids.size(), rb.h_items);
+    (void)max_passes;
     std::memcpy(rb.h_grids, grids.data(), grids.size() * sizeof(golb200::BatchGrid));
     ce = cudaMemcpyAsync(rb.d_grids, rb.h_grids, grids.size() * sizeof(golb200::BatchGrid),
                          cudaMemcpyHostToDevice, s->stream);

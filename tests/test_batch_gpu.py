@@ -8,7 +8,7 @@ import pytest
 import golb200
 import oracle
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.timeout(600)]
 
 
 def small_workload(seed, n, lo=64, hi=1024, gens=(1, 300)):

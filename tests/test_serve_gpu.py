@@ -8,7 +8,7 @@ import pytest
 import golb200
 import oracle
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.timeout(600)]
 
 
 def run_alone(cells, gens, quantum=64):
