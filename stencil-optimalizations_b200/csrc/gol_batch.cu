@@ -190,13 +190,17 @@ __global__ void __launch_bounds__(32) batch_kernel(const BatchGrid* __restrict__
 // ---------------------------------------------------------------------------
 // Autotuner: per grid, pick (words per lane, depth, band height).
 //
-// Model: a work item costs (band + 3k) pipeline steps of k stages on one
-// warp, and a stage-step on a WPL-wide lane costs c[WPL] (relative warp
-// time). A grid's work is
-//     passes * nslices * ngroups * (band + 3k) * k * c[WPL]
+// Model: a work item is (band + 3k) pipeline steps of k stages on one warp
+// plus, once per pass, each row's load and store (c_row stage-steps per
+// row) and a fixed start-up and dependency cost (c_item stage-steps); a
+// stage-step on a WPL-wide lane costs c[WPL] (relative warp time):
+//     item = ((band + 3k) * k + c_row * band) * c[WPL] + c_item.
+// The per-pass terms are what make deeper passes pay: on the dense kernel a
+// 1-generation pass costs ~1.4x a 4-generation pass per generation, which
+// c_row = 0.6 and c_item = 30 reproduce. A grid's work is
+//     passes * nslices * ngroups * item
 // for passes = ceil(gens / k), ngroups = ceil(Y / (S * band)), and its
-// dependency chain (one item per pass, in order) is
-//     passes * (band + 3k) * k * c[WPL].
+// dependency chain (one item per pass, in order) is passes * item.
 // A batch takes about max(total work / resident warps, longest chain), so a
 // first choice minimises work alone; grids whose chain would outlast the
 // batch's work-bound time are then re-planned to minimise work / resident
@@ -207,6 +211,8 @@ __global__ void __launch_bounds__(32) batch_kernel(const BatchGrid* __restrict__
 
 struct BatchTuning {
     double c[5] = {0, 1.0, 1.15, 0, 1.45};   // relative cost per stage-step by WPL
+    double c_row = 0.6;                       // per row per pass (load + store)
+    double c_item = 30.0;                     // per item (start-up, dependency wait, release)
 };
 
 static BatchTuning g_tuning;
@@ -229,10 +235,12 @@ bool choose_batch_plan(int W, int Y, uint64_t gens, int force_wpl, int force_k, 
                 const int S = sliced ? 1 : std::max(1, std::min(32 / L, (Y + band - 1) / band));
                 const int ngroups = (Y + S * band - 1) / (S * band);
                 const uint64_t passes = (gens + k - 1) / k;
-                const double cost = (double)passes * nslices * ngroups * (band + 3 * k) * k *
-                                    g_tuning.c[wpl];
+                const double item =
+                    ((double)(band + 3 * k) * k + g_tuning.c_row * band) * g_tuning.c[wpl] +
+                    g_tuning.c_item;
+                const double cost = (double)passes * nslices * ngroups * item;
                 // one item per pass on the chain of dependent passes
-                const double crit = (double)passes * (band + 3 * k) * k * g_tuning.c[wpl];
+                const double crit = (double)passes * item;
                 const double score = cost / std::max(parallel, 1.0) + crit_weight * crit;
                 if (!found || score < out->score) {
                     found = true;
@@ -478,7 +486,7 @@ int gol_batch_upload(gol_batch* b) {
     }
     const double work_time = total_work / parallel;
     for (auto& e : b->grids) {
-        if (e.choice.crit > 0.5 * work_time && !(e.force_wpl && e.force_k && e.force_band))
+        if (e.choice.crit > work_time && !(e.force_wpl && e.force_k && e.force_band))
             golb200::choose_batch_plan(e.W, e.Y, std::max<uint64_t>(e.gens, 1), e.force_wpl, e.force_k,
                                        e.force_band, &e.choice, parallel, 1.0);
     }
