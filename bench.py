@@ -109,6 +109,12 @@ class Dist:
             self.pg.destroy_process_group()
 
 
+def replica_throughput(world: int, units_per_rank: float, slowest_seconds: float) -> float:
+    """Whole-job rate of N independent replicas: every rank's units over the
+    slowest rank's time (weak scaling)."""
+    return world * units_per_rank / slowest_seconds
+
+
 # ---------------------------------------------------------------------------
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
@@ -455,7 +461,7 @@ def run_ours(args, d: Dist) -> None:
     torch.cuda.synchronize()
     clk = clocks.stop()
     total_ms = d.max(sum(step_ms))
-    value = d.world * cell_updates * args.steps / (total_ms * 1e-3) / 1e9
+    value = replica_throughput(d.world, cell_updates * args.steps, total_ms * 1e-3) / 1e9
     passes = gens // best_k + (1 if gens % best_k else 0)
 
     # -- dominant kernel: per-launch duration (one pass of k generations) ----
@@ -531,7 +537,7 @@ def run_ours(args, d: Dist) -> None:
             flush.zero_()
     eng.close()
     e2e_total = d.max(sum(e2e_times))
-    e2e_value = d.world * cell_updates * args.steps / e2e_total / 1e9
+    e2e_value = replica_throughput(d.world, cell_updates * args.steps, e2e_total) / 1e9
 
     cpu = None
     if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:

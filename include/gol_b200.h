@@ -253,6 +253,9 @@ int gol_batch_run_plain(gol_batch* b, uint32_t temporal_steps);
 int gol_batch_sync(gol_batch* b);
 int gol_batch_fetch(gol_batch* b, int32_t grid_id, uint8_t* cells);
 int gol_batch_info(const gol_batch* b, uint64_t* grids, uint64_t* items, uint64_t* cell_updates);
+/* Census of the last gol_batch_run: SM clock cycles its work items spent
+ * waiting on dependencies and computing, summed over items. */
+int gol_batch_census(gol_batch* b, uint64_t* wait_cycles, uint64_t* work_cycles);
 void* gol_batch_stream(gol_batch* b);
 const char* gol_batch_last_error(const gol_batch* b);
 void gol_batch_destroy(gol_batch* b);

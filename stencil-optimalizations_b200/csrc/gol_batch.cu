@@ -42,6 +42,13 @@
 #include "gol_internal.h"
 #include "gol_rows_temporal.cuh"
 
+#ifndef GOL_BATCH_REPLAN
+#define GOL_BATCH_REPLAN 4.0   // re-plan grids whose chain exceeds this many work-bound times
+#endif
+#ifndef GOL_BATCH_MIN_BLOCKS
+#define GOL_BATCH_MIN_BLOCKS 1   // resident one-warp CTAs per SM the registers are sized for
+#endif
+
 namespace golb200 {
 
 constexpr long long kSpinLimit = 1ll << 24;   // polls of >= 100 ns: a few-second guard
@@ -134,9 +141,9 @@ __device__ __forceinline__ void seg_dispatch(int k, const BatchGrid& G, int grou
     }
 }
 
-__global__ void __launch_bounds__(32) batch_kernel(const BatchGrid* __restrict__ grids,
-                                                   const BatchItem* __restrict__ items, int nitems,
-                                                   int* ticket, int* done, int* status) {
+__global__ void __launch_bounds__(32, GOL_BATCH_MIN_BLOCKS)
+batch_kernel(const BatchGrid* __restrict__ grids, const BatchItem* __restrict__ items, int nitems,
+             int* ticket, int* done, int* status, unsigned long long* census) {
     __shared__ __align__(16) uint32_t ring[kRowRing * 32 * 4];
     const int lane = threadIdx.x & 31;
     for (;;) {
@@ -147,6 +154,7 @@ __global__ void __launch_bounds__(32) batch_kernel(const BatchGrid* __restrict__
         const BatchItem it = items[t];
         const BatchGrid G = grids[it.grid];
         int* mine = done + G.done_base + it.group * G.nslices + it.slice;
+        const long long t_wait = clock64();
         if (it.pass > 0) {
             // Every lane acquires every counter it depends on, so each lane's
             // own copies below are ordered after the producers' releases.
@@ -171,6 +179,7 @@ __global__ void __launch_bounds__(32) batch_kernel(const BatchGrid* __restrict__
                 return;
             }
         }
+        const long long t_work = clock64();
         const int k = it.pass == G.passes - 1 ? G.last_k : G.k;
         const uint32_t* src = G.buf[(G.parity0 + it.pass) & 1];
         uint32_t* dst = G.buf[(G.parity0 + it.pass + 1) & 1];
@@ -181,7 +190,13 @@ __global__ void __launch_bounds__(32) batch_kernel(const BatchGrid* __restrict__
         }
         __threadfence();
         __syncwarp();
-        if (lane == 0) st_release(mine, it.pass + 1);
+        if (lane == 0) {
+            st_release(mine, it.pass + 1);
+            if (census) {   // SM cycles spent waiting on dependencies / computing
+                atomicAdd(census + 0, (unsigned long long)(t_work - t_wait));
+                atomicAdd(census + 1, (unsigned long long)(clock64() - t_work));
+            }
+        }
     }
 }
 
@@ -313,14 +328,15 @@ void batch_grid_from_choice(const GridChoice& ch, int W, int Y, BatchGrid* g) {
 
 cudaError_t launch_batch_kernel(const BatchGrid* d_grids, const BatchItem* d_items, int nitems,
                                 int* d_ticket, int* d_done, int* d_status, int num_sms,
-                                cudaStream_t stream) {
+                                cudaStream_t stream, unsigned long long* d_census) {
     if (nitems <= 0) return cudaSuccess;
     int per_sm = 0;
     cudaError_t ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, 32, 0);
     if (ce != cudaSuccess) return ce;
     per_sm = std::max(1, per_sm);
     const int ctas = std::min(nitems, num_sms * per_sm);   // every CTA resident at once
-    batch_kernel<<<ctas, 32, 0, stream>>>(d_grids, d_items, nitems, d_ticket, d_done, d_status);
+    batch_kernel<<<ctas, 32, 0, stream>>>(d_grids, d_items, nitems, d_ticket, d_done, d_status,
+                                          d_census);
     return cudaPeekAtLastError();
 }
 
@@ -358,6 +374,7 @@ struct gol_batch {
     int* d_done = nullptr;
     int* d_ticket = nullptr;
     int* d_status = nullptr;
+    unsigned long long* d_census = nullptr;   // wait / work SM cycles of the last run
     int nitems = 0, ngroups_total = 0;
     bool uploaded = false, ran = false;
     cudaGraphExec_t graph = nullptr;
@@ -380,7 +397,7 @@ void batch_free_device(gol_batch* b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
     for (void* p : {(void*)b->arena, (void*)b->d_grids, (void*)b->d_items, (void*)b->d_done,
-                    (void*)b->d_ticket, (void*)b->d_status})
+                    (void*)b->d_ticket, (void*)b->d_status, (void*)b->d_census})
         if (p) cudaFree(p);
     b->arena = nullptr;
     b->d_grids = nullptr;
@@ -388,6 +405,7 @@ void batch_free_device(gol_batch* b) {
     b->d_done = nullptr;
     b->d_ticket = nullptr;
     b->d_status = nullptr;
+    b->d_census = nullptr;
     b->uploaded = false;
 }
 
@@ -486,9 +504,30 @@ int gol_batch_upload(gol_batch* b) {
     }
     const double work_time = total_work / parallel;
     for (auto& e : b->grids) {
-        if (e.choice.crit > work_time && !(e.force_wpl && e.force_k && e.force_band))
+        if (e.choice.crit > GOL_BATCH_REPLAN * work_time &&
+            !(e.force_wpl && e.force_k && e.force_band))
             golb200::choose_batch_plan(e.W, e.Y, std::max<uint64_t>(e.gens, 1), e.force_wpl, e.force_k,
                                        e.force_band, &e.choice, parallel, 1.0);
+    }
+    // A first pass with fewer items than about two per resident warp leaves
+    // SMs idle on every pass: halve the tallest bands (not below 16 rows)
+    // until it has enough items.
+    for (int round = 0; round < 3; ++round) {
+        double first_pass = 0;
+        int tallest = 0;
+        for (const auto& e : b->grids) {
+            if (e.gens == 0) continue;
+            first_pass += (double)e.choice.ngroups * e.choice.nslices;
+            tallest = std::max(tallest, e.choice.band);
+        }
+        if (first_pass >= 2 * parallel || tallest <= 16) break;
+        for (auto& e : b->grids) {
+            if (e.gens == 0 || e.force_band || e.choice.band != tallest) continue;
+            golb200::GridChoice c2;
+            if (golb200::choose_batch_plan(e.W, e.Y, std::max<uint64_t>(e.gens, 1), e.force_wpl,
+                                           e.force_k, std::max(16, tallest / 2), &c2))
+                e.choice = c2;
+        }
     }
     for (auto& e : b->grids) {
         if (e.gens == 0) e.choice.passes = 0;
@@ -516,6 +555,7 @@ int gol_batch_upload(gol_batch* b) {
     if (ce == cudaSuccess) ce = cudaMalloc(&b->d_done, std::max(groups, 1) * sizeof(int));
     if (ce == cudaSuccess) ce = cudaMalloc(&b->d_ticket, sizeof(int));
     if (ce == cudaSuccess) ce = cudaMalloc(&b->d_status, sizeof(int));
+    if (ce == cudaSuccess) ce = cudaMalloc(&b->d_census, 2 * sizeof(unsigned long long));
     if (ce != cudaSuccess) {
         batch_free_device(b);
         return ce == cudaErrorMemoryAllocation ? b->fail(GOL_E_NOMEM, "device allocation failed")
@@ -572,9 +612,10 @@ int gol_batch_run(gol_batch* b) {
         if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_done, 0, std::max(b->ngroups_total, 1) * sizeof(int), cs);
         if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_ticket, 0, sizeof(int), cs);
         if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_status, 0, sizeof(int), cs);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_census, 0, 2 * sizeof(unsigned long long), cs);
         if (ce == cudaSuccess)
             ce = golb200::launch_batch_kernel(b->d_grids, b->d_items, b->nitems, b->d_ticket,
-                                              b->d_done, b->d_status, b->num_sms, cs);
+                                              b->d_done, b->d_status, b->num_sms, cs, b->d_census);
         cudaGraph_t g = nullptr;
         cudaError_t ce2 = cudaStreamEndCapture(cs, &g);
         if (ce == cudaSuccess) ce = ce2;
@@ -654,6 +695,19 @@ int gol_batch_info(const gol_batch* b, uint64_t* grids, uint64_t* items, uint64_
     if (grids) *grids = b->grids.size();
     if (items) *items = (uint64_t)b->nitems;
     if (cell_updates) *cell_updates = cu;
+    return GOL_OK;
+}
+
+// Cycles the last run's work items spent waiting on their dependencies and
+// computing, summed over items (SM clock cycles).
+int gol_batch_census(gol_batch* b, uint64_t* wait_cycles, uint64_t* work_cycles) {
+    if (!b || !b->d_census) return GOL_E_INVALID;
+    unsigned long long c[2] = {0, 0};
+    cudaError_t ce = cudaStreamSynchronize(b->stream);
+    if (ce == cudaSuccess) ce = cudaMemcpy(c, b->d_census, sizeof(c), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return b->cuda_fail(ce, "batch census");
+    if (wait_cycles) *wait_cycles = c[0];
+    if (work_cycles) *work_cycles = c[1];
     return GOL_OK;
 }
 

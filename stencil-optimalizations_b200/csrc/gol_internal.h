@@ -110,7 +110,7 @@ void batch_grid_from_choice(const GridChoice& ch, int W, int Y, BatchGrid* g);
 // order); done[] and *ticket, *status must be zero. All CTAs fit at once.
 cudaError_t launch_batch_kernel(const BatchGrid* d_grids, const BatchItem* d_items, int nitems,
                                 int* d_ticket, int* d_done, int* d_status, int num_sms,
-                                cudaStream_t stream);
+                                cudaStream_t stream, unsigned long long* d_census = nullptr);
 
 cudaError_t launch_pack_cells(const uint8_t* cells, uint32_t* words, size_t x, size_t y,
                               cudaStream_t stream);

@@ -114,6 +114,7 @@ def lib():
     L.gol_batch_sync.argtypes = [_vp]
     L.gol_batch_fetch.argtypes = [_vp, ctypes.c_int32, _vp]
     L.gol_batch_info.argtypes = [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u64)]
+    L.gol_batch_census.argtypes = [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]
     L.gol_batch_stream.argtypes = [_vp]
     L.gol_batch_stream.restype = _vp
     L.gol_batch_last_error.argtypes = [_vp]
@@ -460,6 +461,12 @@ class GolBatch:
         self._check(lib().gol_batch_info(self._b, ctypes.byref(g), ctypes.byref(i), ctypes.byref(c)),
                     "batch_info")
         return {"grids": g.value, "items": i.value, "cell_updates": c.value}
+
+    def census(self) -> dict:
+        """SM cycles the last run's items spent waiting / computing."""
+        w, c = _u64(), _u64()
+        self._check(lib().gol_batch_census(self._b, ctypes.byref(w), ctypes.byref(c)), "batch_census")
+        return {"wait_cycles": w.value, "work_cycles": c.value}
 
     def stream_ptr(self) -> int:
         return int(lib().gol_batch_stream(self._b) or 0)
