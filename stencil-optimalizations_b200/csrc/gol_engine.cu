@@ -116,7 +116,7 @@ int alloc_local(gol_engine* e) {
         for (auto& p : s.changed)
             if (ce == cudaSuccess) ce = cudaMalloc(&p, nt);
         if (ce == cudaSuccess) ce = cudaMalloc(&s.list, nt * sizeof(int));
-        if (ce == cudaSuccess) ce = cudaMalloc(&s.count, sizeof(int));
+        if (ce == cudaSuccess) ce = cudaMalloc(&s.count, 4 * sizeof(int));
         if (ce == cudaSuccess) ce = cudaMalloc(&s.census, kCensusCap * sizeof(uint32_t));
         if (ce == cudaSuccess) ce = cudaMalloc(&s.pass_no, sizeof(uint32_t));
         s.census_cap = kCensusCap;
@@ -129,6 +129,7 @@ int alloc_local(gol_engine* e) {
     ce = cudaMemsetAsync(s.changed[1], 1, nt, e->stream);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(s.changed[0], 0, nt, e->stream);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(s.pass_no, 0, sizeof(uint32_t), e->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(s.count, 0, 4 * sizeof(int), e->stream);
     if (ce != cudaSuccess) return e->cuda_fail(ce, "change-tracking reset");
     e->lparity = 0;
     return GOL_OK;

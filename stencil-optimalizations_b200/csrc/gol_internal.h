@@ -35,15 +35,17 @@ cudaError_t launch_rows_pass(const uint32_t* src, uint32_t* dst, int W, int Y, i
 
 // Change-tracking tiles (GOL_ALG_LOCAL): tile = x-slice x row band.
 struct LocalPlan {
-    RowsPlan rows;     // slice/band geometry of one tile, one warp per tile
+    RowsPlan rows;     // slice/band geometry of one tile
+    int seg_lanes = 0; // lanes per tile (its words plus a halo lane each side)
+    int segs = 0;      // tiles carried by one warp at once
     int tiles_x = 0, tiles_y = 0;
-    int ctas = 0;      // persistent CTAs of the tile kernel
+    int ctas = 0;      // persistent one-warp CTAs of the tile kernel
 };
 
 struct LocalState {
     uint8_t* changed[2] = {nullptr, nullptr};   // per tile, by pass parity
     int* list = nullptr;                        // active tiles of the current pass
-    int* count = nullptr;                       // its length
+    int* count = nullptr;                       // list lengths by pass parity, CTA ticket
     uint32_t* census = nullptr;                 // active tiles per pass
     uint32_t census_cap = 0;
     uint32_t* pass_no = nullptr;                // passes recorded so far

@@ -6,17 +6,19 @@
 // recomputed only if it or one of its 8 neighbour tiles changed in the
 // previous step; per-block state words record which warp tiles changed.
 //
-// Here one step is a pass of K generations and a tile is an x-slice (with
-// a one-lane halo) times a band of rows, so the skip rule needs tiles at
-// least K cells high and wide (a pass reads K cells around each cell). Per
-// pass:
-//   plan   one CTA reads the previous pass's per-tile `changed` bytes,
-//          compacts the tiles whose 3x3 neighbourhood changed into a list
-//          (block-wide scan, no atomics), clears this pass's bytes, and
-//          appends the list length to a census;
-//   tiles  persistent CTAs walk the list, run the K-stage pipeline on each
-//          tile (band_tile<.., TRACK>) and set changed[tile] when any of
-//          its cells differs after the pass.
+// Here one step is a pass of K generations and a tile is a narrow x-slice
+// (6 lanes of words; a halo lane each side absorbs the unknown cells beyond
+// it, whose errors move one cell per generation) times a band of rows, so
+// the skip rule needs tiles at least K cells high and wide (a pass reads K
+// cells around each cell). Per pass:
+//   plan   one thread per tile reads the previous pass's `changed` bytes
+//          of its 3x3 neighbourhood, active tiles are appended to a list
+//          (warp ballot + one atomic per warp), this pass's bytes are
+//          cleared, and the last CTA appends the list length to a census;
+//   tiles  persistent one-warp CTAs walk the list, several tiles per warp
+//          (one per 8-lane segment: the segmented-warp form of the K-stage
+//          pipeline), compare each tile's result with its input and set
+//          changed[tile] when any of its cells differs after the pass.
 // No copies for skipped tiles: a tile skipped at pass p did not change at
 // pass p-1 (it is in its own neighbourhood), so the buffer pass p writes —
 // the one pass p-1 read — already holds its current state.
@@ -29,7 +31,7 @@ namespace golb200 {
 
 namespace {
 
-constexpr int kPlanThreads = 1024;
+constexpr int kPlanThreads = 256;
 
 __device__ __forceinline__ bool tile_active(const uint8_t* prev, int tx, int ty, int tiles_x,
                                             int tiles_y) {
@@ -45,69 +47,144 @@ __device__ __forceinline__ bool tile_active(const uint8_t* prev, int tx, int ty,
     return false;
 }
 
+// One thread per tile. Active tiles are appended to `list` a warp at a time
+// (ballot, one atomic per warp: consecutive tiles stay together, so a warp
+// of the tile kernel gets neighbouring tiles). counts[parity] is this pass's
+// list length (zero on entry); counts[parity ^ 1] is zeroed for the next
+// pass; counts[2] is the CTA ticket the last CTA uses to record the census.
 __global__ void __launch_bounds__(kPlanThreads)
 plan_tiles_kernel(const uint8_t* __restrict__ prev, uint8_t* __restrict__ clear, int tiles_x,
-                  int tiles_y, int* __restrict__ list, int* __restrict__ count,
+                  int tiles_y, int* __restrict__ list, int* counts, int parity,
                   uint32_t* __restrict__ census, uint32_t census_cap, uint32_t* __restrict__ pass_no) {
-    __shared__ int warp_sums[kPlanThreads / 32];
     const int ntiles = tiles_x * tiles_y;
-    const int per = (ntiles + blockDim.x - 1) / blockDim.x;
-    const int t0 = min((int)threadIdx.x * per, ntiles), t1 = min(t0 + per, ntiles);
-    int mine = 0;
-    for (int t = t0; t < t1; ++t) mine += tile_active(prev, t % tiles_x, t / tiles_x, tiles_x, tiles_y);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    if (blockIdx.x == 0 && threadIdx.x == 0) counts[parity ^ 1] = 0;
+    const bool act = t < ntiles && tile_active(prev, t % tiles_x, t / tiles_x, tiles_x, tiles_y);
+    if (t < ntiles) clear[t] = 0;
+    const unsigned m = __ballot_sync(0xffffffffu, act);
+    int base = 0;
+    if (lane == 0 && m) base = atomicAdd(counts + parity, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (act) list[base + __popc(m & ((1u << lane) - 1u))] = t;
 
-    // Block-wide exclusive scan of `mine`.
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int incl = mine;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    if (lane == 31) warp_sums[warp] = incl;
+    __threadfence();
     __syncthreads();
-    if (warp == 0) {
-        const int nw = blockDim.x >> 5;
-        int w = lane < nw ? warp_sums[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int v = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += v;
+    if (threadIdx.x == 0) {
+        unsigned* ticket = reinterpret_cast<unsigned*>(counts + 2);
+        if (atomicAdd(ticket, 1u) == gridDim.x - 1) {   // every CTA has appended
+            __threadfence();
+            const int total = atomicAdd(counts + parity, 0);
+            const uint32_t p = *pass_no;
+            if (census && p < census_cap) census[p] = (uint32_t)total;
+            *pass_no = p + 1;
+            *ticket = 0u;
         }
-        if (lane < nw) warp_sums[lane] = w;   // inclusive over warps
     }
-    __syncthreads();
-    int pos = incl - mine + (warp > 0 ? warp_sums[warp - 1] : 0);
+}
 
-    for (int t = t0; t < t1; ++t) {
-        if (tile_active(prev, t % tiles_x, t / tiles_x, tiles_x, tiles_y)) list[pos++] = t;
-        clear[t] = 0;
-    }
-    if (threadIdx.x == blockDim.x - 1) {
-        const int total = pos;   // the last thread's end position is the total
-        *count = total;
-        const uint32_t p = *pass_no;
-        if (census && p < census_cap) census[p] = (uint32_t)total;
-        *pass_no = p + 1;
+struct TileList {
+    const int* list;        // active tile indices (band * tiles_x + slice)
+    const int* count;       // number of entries in `list`
+    uint8_t* changed;       // per tile, this pass
+    int tiles_x;
+};
+
+// One warp, up to `segs` tiles at once (segment s takes list entry
+// base + s). Each segment streams its tile's band through the K stages with
+// change tracking; a ballot over the segment's lanes gives changed[tile].
+template <int WPL, int K>
+__global__ void __launch_bounds__(32)
+seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
+    __shared__ __align__(16) uint32_t ring[kRowRing * 32 * WPL];
+    const int lane = threadIdx.x & 31;
+    const int L = seg_lanes;
+    const int seg = lane / L, q = lane - seg * L;
+    const int n = *t.count;
+    for (int first = blockIdx.x * segs; first < n; first += gridDim.x * segs) {
+        const int idx = first + seg;
+        const bool has = seg < segs && idx < n;
+        const int tile = has ? t.list[idx] : 0;
+        const int ty = tile / t.tiles_x, tx = tile - ty * t.tiles_x;
+        const int xs = tx * a.slice;
+        TemporalCtx c;
+        c.src = a.src;
+        c.dst = a.dst;
+        c.W = a.W;
+        c.Y = a.Y;
+        c.B = a.band;
+        c.y0 = ty * a.band;
+        c.y1 = min(c.y0 + a.band, a.Y);
+        c.lane = lane;
+        c.base = xs - a.halo + q * WPL;
+        c.lane_ok = has && c.y0 < a.Y && c.base >= 0 && c.base < a.W;
+        c.own = c.lane_ok && c.base >= xs && c.base < xs + a.slice;
+        c.first_lane = q == 0;
+        c.last_lane = q == L - 1;
+        c.src_l = max(lane - 1, 0);
+        c.src_r = min(lane + 1, 31);
+        c.erd = nullptr;
+        c.ewr = nullptr;
+        c.ring = ring + lane * WPL;
+        c.ring_saddr = (uint32_t)__cvta_generic_to_shared(c.ring);
+        c.ring_stride = 32 * WPL;
+        const uint32_t lane_mask = c.lane_ok ? 0xffffffffu : 0u;
+
+        TemporalRegs<WPL, K> s;
+#pragma unroll
+        for (int w = 0; w < WPL; ++w) {
+            s.ld[0][w] = s.ld[1][w] = s.ld[2][w] = 0u;
+#pragma unroll
+            for (int g = 0; g < K; ++g) {
+                s.h0[g][0][w] = s.h0[g][1][w] = s.h0[g][2][w] = 0u;
+                s.h1[g][0][w] = s.h1[g][1][w] = s.h1[g][2][w] = 0u;
+                s.o[g][0][w] = s.o[g][1][w] = s.o[g][2][w] = 0u;
+            }
+        }
+        for (int j = 0; j < kRowsInFlight; ++j) issue_row<WPL, K>(c, j, j);
+        cp_async_wait<kRowsInFlight - 1>();
+        lds_words<WPL>(c.ring, s.ld[0]);
+        s.rd_slot = 1;
+        s.diff = 0u;
+
+        // Steady state while every segment's rows stay inside the grid: the
+        // deepest band among the warp's tiles bounds the window.
+        const int y0_deep = __reduce_max_sync(0xffffffffu, c.lane_ok ? c.y0 : 0);
+        const int nsteps = c.B + 3 * K;
+        const int f0 = 3 * K;
+        const int f1 = min(c.B + 2 * K - 1, c.Y - y0_deep + K - 1);
+        const int fast_end = f1 > f0 ? f0 + (f1 - f0) / 3 * 3 : f0;
+        if (fast_end > f0) {
+            temporal_steps<WPL, K, false, false, true, true>(s, c, 0, f0, lane_mask);
+            temporal_steps<WPL, K, true, true, true, true>(s, c, f0, fast_end, lane_mask);
+            temporal_steps<WPL, K, false, false, true, true>(s, c, fast_end, nsteps, lane_mask);
+        } else {
+            temporal_steps<WPL, K, false, false, true, true>(s, c, 0, nsteps, lane_mask);
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        const unsigned any = __ballot_sync(0xffffffffu, s.diff != 0u);
+        if (has && q == 0) {
+            const unsigned segmask = (L == 32 ? 0xffffffffu : ((1u << L) - 1u)) << (seg * L);
+            t.changed[tile] = (any & segmask) ? 1 : 0;
+        }
     }
 }
 
 template <int WPL, int K>
-cudaError_t launch_tiles_one(const RowsLaunch& a, const TileList& t, int threads, int ctas,
+cudaError_t launch_tiles_one(const RowsLaunch& a, const TileList& t, const LocalPlan& lp,
                              cudaStream_t stream) {
-    const size_t smem = temporal_smem_bytes(K, threads, WPL);
-    rows_tiles_kernel<WPL, K><<<ctas, threads, smem, stream>>>(a, t);
+    seg_tiles_kernel<WPL, K><<<lp.ctas, 32, 0, stream>>>(a, t, lp.seg_lanes, lp.segs);
     return cudaPeekAtLastError();
 }
 
 template <int WPL, int K>
-cudaError_t dispatch_tiles(int k, const RowsLaunch& a, const TileList& t, int threads, int ctas,
+cudaError_t dispatch_tiles(int k, const RowsLaunch& a, const TileList& t, const LocalPlan& lp,
                            cudaStream_t stream) {
     if constexpr (K > kMaxKForWpl(WPL)) {
         return cudaErrorInvalidValue;
     } else {
-        if (k == K) return launch_tiles_one<WPL, K>(a, t, threads, ctas, stream);
-        return dispatch_tiles<WPL, K + 1>(k, a, t, threads, ctas, stream);
+        if (k == K) return launch_tiles_one<WPL, K>(a, t, lp, stream);
+        return dispatch_tiles<WPL, K + 1>(k, a, t, lp, stream);
     }
 }
 
@@ -124,17 +201,22 @@ bool plan_local_tiles(int W, int Y, int k, int tile_rows, int wpl, int num_sms, 
     p.band = band;
     p.nbands = (Y + band - 1) / band;
     p.threads = 32;
-    if (W / wpl <= 32) {
+    constexpr int kTileLanes = 8;                        // 6 lanes of words + a halo lane each side
+    if (W / wpl <= kTileLanes) {
         p.slice = W;
         p.halo = 0;
+        lp->seg_lanes = W / wpl;
     } else {
-        p.slice = 30 * wpl;                              // 30 lanes + a halo lane each side
+        p.slice = (kTileLanes - 2) * wpl;
         p.halo = wpl;
+        lp->seg_lanes = kTileLanes;
     }
+    lp->segs = 32 / lp->seg_lanes;
     p.nslices = (W + p.slice - 1) / p.slice;
     lp->tiles_x = p.nslices;
     lp->tiles_y = p.nbands;
-    lp->ctas = std::max(1, std::min(lp->tiles_x * lp->tiles_y, num_sms * 16));
+    const int warps = (lp->tiles_x * lp->tiles_y + lp->segs - 1) / lp->segs;
+    lp->ctas = std::max(1, std::min(warps, num_sms * 24));
     return true;
 }
 
@@ -142,17 +224,18 @@ cudaError_t launch_local_pass(const uint32_t* src, uint32_t* dst, int W, int Y, 
                               const LocalPlan& lp, const LocalState& st, int parity,
                               cudaStream_t stream) {
     const RowsPlan& p = lp.rows;
-    plan_tiles_kernel<<<1, kPlanThreads, 0, stream>>>(st.changed[parity ^ 1], st.changed[parity],
-                                                      lp.tiles_x, lp.tiles_y, st.list, st.count,
-                                                      st.census, st.census_cap, st.pass_no);
+    const int ntiles = lp.tiles_x * lp.tiles_y;
+    plan_tiles_kernel<<<(ntiles + kPlanThreads - 1) / kPlanThreads, kPlanThreads, 0, stream>>>(
+        st.changed[parity ^ 1], st.changed[parity], lp.tiles_x, lp.tiles_y, st.list, st.count,
+        parity, st.census, st.census_cap, st.pass_no);
     cudaError_t e = cudaPeekAtLastError();
     if (e != cudaSuccess) return e;
     RowsLaunch a{src, dst, W, Y, p.band, p.slice, p.halo};
-    TileList t{st.list, st.count, st.changed[parity], lp.tiles_x};
+    TileList t{st.list, st.count + parity, st.changed[parity], lp.tiles_x};
     switch (p.wpl) {
-        case 4: return dispatch_tiles<4, 1>(k, a, t, p.threads, lp.ctas, stream);
-        case 2: return dispatch_tiles<2, 1>(k, a, t, p.threads, lp.ctas, stream);
-        case 1: return dispatch_tiles<1, 1>(k, a, t, p.threads, lp.ctas, stream);
+        case 4: return dispatch_tiles<4, 1>(k, a, t, lp, stream);
+        case 2: return dispatch_tiles<2, 1>(k, a, t, lp, stream);
+        case 1: return dispatch_tiles<1, 1>(k, a, t, lp, stream);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -363,37 +363,6 @@ rows_temporal_kernel(RowsLaunch a) {
     band_tile<WPL, K, false>(a, blockIdx.x, blockIdx.y, smem);
 }
 
-// Change-tracking pass over a list of tiles (tile = x-slice x row band,
-// index band * tiles_x + slice). Persistent CTAs walk the list, which the
-// plan kernel built on the device; each writes changed[tile] = 1 iff any
-// cell of its tile differs after the pass.
-struct TileList {
-    const int* list;        // active tile indices
-    const int* count;       // number of entries in `list`
-    uint8_t* changed;       // per tile, this pass
-    int tiles_x;
-};
-
-template <int WPL, int K>
-__global__ void __launch_bounds__(kTemporalMaxThreads, GOL_TEMPORAL_MIN_BLOCKS)
-rows_tiles_kernel(RowsLaunch a, TileList t) {
-    extern __shared__ __align__(16) uint32_t smem[];
-    __shared__ int tile_changed;
-    const int n = *t.count;
-    for (int idx = blockIdx.x; idx < n; idx += gridDim.x) {
-        const int tile = t.list[idx];
-        if (threadIdx.x == 0) tile_changed = 0;
-        __syncthreads();
-        const uint32_t d = band_tile<WPL, K, true>(a, tile / t.tiles_x, tile % t.tiles_x, smem);
-        if (__any_sync(0xffffffffu, d != 0u) && (threadIdx.x & 31) == 0) tile_changed = 1;
-        __syncthreads();
-        if (threadIdx.x == 0) t.changed[tile] = (uint8_t)tile_changed;
-        __syncthreads();
-    }
-}
-
-
-
 // Shared memory a launch needs: the row ring, the edge table and one dummy
 // edge entry per warp.
 __host__ __device__ inline size_t temporal_smem_bytes(int K, int threads, int wpl) {
