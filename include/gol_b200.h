@@ -98,6 +98,21 @@ int gol_set_input_i32(gol_engine* e, const int32_t* cells, uint64_t x, uint64_t 
 int gol_set_input_words(gol_engine* e, const void* words, uint64_t x, uint64_t y,
                         uint32_t word_bits);
 
+/* Word layouts of the reference's GeneralBitGrid modes
+ * (src/algorithms/_shared/bitwise/bit_modes.hpp:10-177):
+ *   GOL_LAYOUT_ROWS    FullyPackedRows: cell (cx, cy) is bit cx % W of word
+ *                      cy * (x / W) + cx / W (the engine's own layout);
+ *   GOL_LAYOUT_COLUMNS BitColumns: bit cy % W of word (cy / W) * x + cx;
+ *   GOL_LAYOUT_TILES   BitTile: 4x4 cells per 16-bit word, 8x4 per 32-bit,
+ *                      8x8 per 64-bit; bit W-1 - ((cy % YB) * XB + cx % XB)
+ *                      of word (cy / YB) * (x / XB) + cx / XB.
+ * Word bits 16, 32 or 64; x and y multiples of the word's cell block. */
+enum gol_layout { GOL_LAYOUT_ROWS = 0, GOL_LAYOUT_COLUMNS = 1, GOL_LAYOUT_TILES = 2 };
+
+/* set_and_format_input_data from words in any layout (converted to rows on
+ * the host; x must also be a multiple of 32). */
+int gol_set_input_layout(gol_engine* e, const void* words, int layout, uint32_t word_bits);
+
 /* initialize_data_structures: allocates the device grids, copies input in. */
 int gol_init(gol_engine* e);
 
@@ -117,6 +132,9 @@ int gol_finalize(gol_engine* e);
 int gol_fetch_u8(gol_engine* e, uint8_t* cells);
 int gol_fetch_i32(gol_engine* e, int32_t* cells);
 int gol_fetch_words(gol_engine* e, void* words, uint32_t word_bits);
+
+/* fetch_result as words in any layout (see gol_set_input_layout). */
+int gol_fetch_layout(gol_engine* e, void* words, int layout, uint32_t word_bits);
 
 /* actually_performed_iterations of the last gol_run. */
 uint64_t gol_performed(const gol_engine* e);
@@ -143,6 +161,51 @@ int gol_load_random_ones_zeros(uint8_t* cells, uint64_t x, uint64_t y, uint64_t 
  * GOL_E_INVALID. Host only. */
 int gol_load_sparse_patches(uint8_t* cells, uint64_t x, uint64_t y, uint64_t seed, uint32_t patch,
                             double fraction, double density);
+
+/* The reference's other input loaders (src/infrastructure/data_loader.hpp:
+ * 77-152, registered in experiment_manager.hpp:396-410). Host only; cells
+ * are raster order (cells[cy*x + cx]), 0 dead / 1 alive.
+ *   zeros            : every cell dead (ZerosLoader).
+ *   always-changing  : a blinker (three live cells in a row) with its left
+ *                      cell at every (cx, cy) with cx % 4 == 0 and
+ *                      cy % 4 == 0, on a dead grid (AlwaysChangingSpaceLoader).
+ * A pattern cell that lands past the right edge continues on the next row
+ * (the reference's flat indexing); one past the end of the raster is
+ * dropped. */
+int gol_load_zeros(uint8_t* cells, uint64_t x, uint64_t y);
+int gol_load_always_changing(uint8_t* cells, uint64_t x, uint64_t y);
+
+/* Lexicon loader (LexiconLoader<2,T>, data_loader.hpp:77-99, and
+ * lexicon::Lexicon, gol-lexicon/lexicon.hpp:118-186). A gol_lexicon is a
+ * pattern dictionary read at run time from text in the format of the
+ * reference's gol-lexicon/patterns.cpp (entries {"name", {{_, X, ...}, ...}},
+ * `_` dead, `X` alive, one brace group per row; only the part between the
+ * LEXICON_START and LEXICON_END marker comments when both are present; the
+ * first entry of a repeated name wins). It starts with "blinker" only.
+ *   gol_lexicon_add_text / _add_file : add entries (later calls override
+ *       earlier names); returns the number of entries read, or GOL_E_INVALID
+ *       with gol_lexicon_last_error set.
+ *   gol_lexicon_insert : place the patterns of an expression such as
+ *       "glider[10,20]; block[3,4]" (whitespace and ';' are ignored; each
+ *       record is name[x,y] with (x, y) the pattern's top-left cell). Pattern
+ *       cells overwrite the grid, dead ones included; unknown names place
+ *       nothing. Returns the number of records placed, or GOL_E_INVALID for a
+ *       coordinate that is not a non-negative integer.
+ *   gol_lexicon_insert_repeating : the named pattern at every multiple of
+ *       (x_jump, y_jump) (Lexicon::insert_repeating, lexicon.hpp:137-145). */
+typedef struct gol_lexicon gol_lexicon;
+int gol_lexicon_create(gol_lexicon** out);
+int gol_lexicon_add_text(gol_lexicon* lx, const char* text);
+int gol_lexicon_add_file(gol_lexicon* lx, const char* path);
+int gol_lexicon_count(const gol_lexicon* lx);
+int gol_lexicon_pattern_size(const gol_lexicon* lx, const char* name, uint64_t* width,
+                             uint64_t* height);
+int gol_lexicon_insert(gol_lexicon* lx, const char* expression, uint8_t* cells, uint64_t x,
+                       uint64_t y);
+int gol_lexicon_insert_repeating(gol_lexicon* lx, const char* name, uint64_t x_jump,
+                                 uint64_t y_jump, uint8_t* cells, uint64_t x, uint64_t y);
+const char* gol_lexicon_last_error(const gol_lexicon* lx);
+void gol_lexicon_destroy(gol_lexicon* lx);
 
 /* Uneven multi-grid workloads (batched and serving configurations), drawn
  * from one std::mt19937_64(seed) stream with u = (rng() >> 11) * 2^-53, per
@@ -218,6 +281,21 @@ int gol_pack_cells_device(const uint8_t* d_cells, void* d_words, uint64_t x, uin
                           void* stream);
 int gol_unpack_cells_device(const void* d_words, uint8_t* d_cells, uint64_t x, uint64_t y,
                             void* stream);
+
+/* Host cells (uint8, nonzero = alive) <-> words in a layout
+ * (GeneralBitGrid fill_grid / to_grid, general_bit_grid.hpp:171-246). */
+int gol_pack_layout(const uint8_t* cells, uint64_t x, uint64_t y, int layout, uint32_t word_bits,
+                    void* words);
+int gol_unpack_layout(const void* words, uint64_t x, uint64_t y, int layout, uint32_t word_bits,
+                      uint8_t* cells);
+
+/* Device words in the column or tile layout <-> device rows (32-bit
+ * words), stream-ordered. x % 32 == 0, y a multiple of the layout's block
+ * height, both at most 2^30; pointers aligned to their word size (and 4). */
+int gol_layout_to_rows_device(const void* d_src, void* d_rows, uint64_t x, uint64_t y, int layout,
+                              uint32_t word_bits, void* stream);
+int gol_rows_to_layout_device(const void* d_rows, void* d_dst, uint64_t x, uint64_t y, int layout,
+                              uint32_t word_bits, void* stream);
 
 /* Measures the device's 32-bit LOP3 throughput (lane-ops/s) with a short
  * register-only kernel: the integer-pipe roofline of the bit-sliced passes.

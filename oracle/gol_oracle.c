@@ -28,6 +28,11 @@
  *                          general_bit_grid.hpp:171-246, bit_modes.hpp:127-148):
  *                          bit i of word (xw, y) is cell (xw*W + i, y), words
  *                          stored row-major at y*(X/W) + xw.
+ *   gor_pack_layout,       GeneralBitGrid<uintW_t, BitColumnsMode | BitTileMode>
+ *   gor_unpack_layout      fill_grid / to_grid (general_bit_grid.hpp:171-246,
+ *                          bit_modes.hpp:10-125, 165-177): words hold
+ *                          X_BITS x Y_BITS cell blocks, stored row-major at
+ *                          (y / Y_BITS) * (X / X_BITS) + x / X_BITS.
  *   gor_life_rows          GoLCpuBitwise<char, W, AdderOps>::run
  *                          (src/algorithms/cpu-bitwise-general/
  *                          gol_cpu_bitwise_general.hpp:32-120) with the
@@ -169,6 +174,90 @@ int gor_unpack_rows(int word_bits, const void* words, uint64_t x, uint64_t y, ui
                                            : (uint64_t)((const uint32_t*)words)[yy * wx + xw];
             for (int bit = 0; bit < word_bits; ++bit)
                 cells[yy * x + xw * (uint64_t)word_bits + (uint64_t)bit] = (uint8_t)((w >> bit) & 1u);
+        }
+    }
+    return 0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Column and tile layouts  (bit_modes.hpp:10-125)                          */
+/* ---------------------------------------------------------------------- */
+
+/* layout 1 = BitColumns<uintW>: X_BITS 1, Y_BITS W; the first mask is bit 0
+ *            and each next cell (down the column) moves it one bit up.
+ * layout 2 = BitTile<uintW>: 4x4 (16-bit), 8x4 (32-bit), 8x8 (64-bit); the
+ *            first mask is the top bit and each next cell (x fastest, then y)
+ *            moves it one bit down. */
+static int gor_layout_geom(int layout, int word_bits, uint64_t* xb, uint64_t* yb) {
+    if (word_bits != 16 && word_bits != 32 && word_bits != 64) return -2;
+    if (layout == 1) {
+        *xb = 1;
+        *yb = (uint64_t)word_bits;
+        return 0;
+    }
+    if (layout == 2) {
+        *xb = word_bits == 16 ? 4 : 8;
+        *yb = word_bits == 64 ? 8 : 4;
+        return 0;
+    }
+    return -2;
+}
+
+static uint64_t gor_get_word(const void* words, int word_bits, uint64_t i) {
+    if (word_bits == 64) return ((const uint64_t*)words)[i];
+    if (word_bits == 32) return ((const uint32_t*)words)[i];
+    return ((const uint16_t*)words)[i];
+}
+
+static void gor_set_word(void* words, int word_bits, uint64_t i, uint64_t w) {
+    if (word_bits == 64) ((uint64_t*)words)[i] = w;
+    else if (word_bits == 32) ((uint32_t*)words)[i] = (uint32_t)w;
+    else ((uint16_t*)words)[i] = (uint16_t)w;
+}
+
+/* Walks the cells of one word in the reference's order, yielding each
+ * cell's mask. */
+static uint64_t gor_first_mask(int layout, int word_bits) {
+    return layout == 1 ? 1u : (uint64_t)1 << (word_bits - 1);
+}
+
+static uint64_t gor_next_mask(int layout, uint64_t m) { return layout == 1 ? m << 1 : m >> 1; }
+
+int gor_pack_layout(int layout, int word_bits, const uint8_t* cells, uint64_t x, uint64_t y,
+                    void* words) {
+    uint64_t xb, yb;
+    if (gor_layout_geom(layout, word_bits, &xb, &yb)) return -2;
+    if (x % xb || y % yb) return -3;
+    const uint64_t wx = x / xb;
+    for (uint64_t cy = 0; cy < y; cy += yb) {
+        for (uint64_t cx = 0; cx < x; cx += xb) {
+            uint64_t w = 0, m = gor_first_mask(layout, word_bits);
+            for (uint64_t by = 0; by < yb; ++by)
+                for (uint64_t bx = 0; bx < xb; ++bx) {
+                    if (cells[(cy + by) * x + cx + bx]) w |= m;
+                    m = gor_next_mask(layout, m);
+                }
+            gor_set_word(words, word_bits, (cy / yb) * wx + cx / xb, w);
+        }
+    }
+    return 0;
+}
+
+int gor_unpack_layout(int layout, int word_bits, const void* words, uint64_t x, uint64_t y,
+                      uint8_t* cells) {
+    uint64_t xb, yb;
+    if (gor_layout_geom(layout, word_bits, &xb, &yb)) return -2;
+    if (x % xb || y % yb) return -3;
+    const uint64_t wx = x / xb;
+    for (uint64_t cy = 0; cy < y; cy += yb) {
+        for (uint64_t cx = 0; cx < x; cx += xb) {
+            const uint64_t w = gor_get_word(words, word_bits, (cy / yb) * wx + cx / xb);
+            uint64_t m = gor_first_mask(layout, word_bits);
+            for (uint64_t by = 0; by < yb; ++by)
+                for (uint64_t bx = 0; bx < xb; ++bx) {
+                    cells[(cy + by) * x + cx + bx] = (w & m) ? 1 : 0;
+                    m = gor_next_mask(layout, m);
+                }
         }
     }
     return 0;

@@ -25,6 +25,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libgoloracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libgolref.so")
+LEX_SO = os.path.join(HERE, "_ref", "libgollexref.so")
+
+LAYOUT_COLUMNS = 1
+LAYOUT_TILES = 2
 
 _u8p = ctypes.POINTER(ctypes.c_uint8)
 _vp = ctypes.c_void_p
@@ -33,6 +37,8 @@ _u64 = ctypes.c_uint64
 _oracle = None
 _ref = None
 _ref_tried = False
+_lex = None
+_lex_tried = False
 
 
 def build(with_ref: bool | None = None) -> None:
@@ -60,6 +66,8 @@ def liboracle():
         lib.gor_pack_rows.argtypes = [ctypes.c_int, _vp, _u64, _u64, _vp]
         lib.gor_unpack_rows.argtypes = [ctypes.c_int, _vp, _u64, _u64, _vp]
         lib.gor_life_rows.argtypes = [ctypes.c_int, _vp, _u64, _u64, _u64, _vp, ctypes.c_int]
+        lib.gor_pack_layout.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _u64, _u64, _vp]
+        lib.gor_unpack_layout.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _u64, _u64, _vp]
         lib.gor_fnv1a64.argtypes = [_vp, _u64]
         lib.gor_fnv1a64.restype = _u64
         lib.gor_max_threads.restype = ctypes.c_int
@@ -79,8 +87,28 @@ def libref():
             lib.ref_run_cpu_bitwise_adder.argtypes = [ctypes.c_int, _vp, _u64, _u64, _u64, _vp]
             lib.ref_pack_rows.argtypes = [ctypes.c_int, _vp, _u64, _u64, _vp]
             lib.ref_unpack_rows.argtypes = [ctypes.c_int, _vp, _u64, _u64, _vp]
+            lib.ref_pack_layout.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _u64, _u64, _vp]
+            lib.ref_unpack_layout.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _u64, _u64, _vp]
+            lib.ref_load_zeros.argtypes = [_u64, _u64, _vp]
             _ref = lib
     return _ref
+
+
+def liblexref():
+    """The reference's pattern loaders and compiled dictionary
+    (oracle/_ref/libgollexref.so, `make -C oracle lexicon`), or None."""
+    global _lex, _lex_tried
+    if not _lex_tried:
+        _lex_tried = True
+        if os.path.exists(LEX_SO):
+            lib = ctypes.CDLL(LEX_SO)
+            lib.ref_load_always_changing.argtypes = [_u64, _u64, _vp]
+            lib.ref_load_lexicon.argtypes = [ctypes.c_char_p, _u64, _u64, _vp]
+            lib.ref_lexicon_count.restype = ctypes.c_int64
+            lib.ref_lexicon_pattern.argtypes = [ctypes.c_int64, ctypes.c_char_p, _u64,
+                                                ctypes.POINTER(_u64), ctypes.POINTER(_u64), _vp]
+            _lex = lib
+    return _lex
 
 
 def ref_available() -> bool:
@@ -127,6 +155,131 @@ def unpack_rows(words: np.ndarray, x: int, word_bits: int = 64) -> np.ndarray:
     out = np.empty((y, x), dtype=np.uint8)
     _check(liboracle().gor_unpack_rows(word_bits, _ptr(words), x, y, _ptr(out)), "unpack_rows")
     return out
+
+
+_WORD_DTYPES = {16: np.uint16, 32: np.uint32, 64: np.uint64}
+
+
+def layout_geom(layout: int, word_bits: int) -> tuple:
+    """(X_BITS, Y_BITS) of BitColumns / BitTile (bit_modes.hpp:10-125)."""
+    if layout == LAYOUT_COLUMNS:
+        return 1, word_bits
+    if layout == LAYOUT_TILES:
+        return {16: (4, 4), 32: (8, 4), 64: (8, 8)}[word_bits]
+    raise ValueError(layout)
+
+
+def pack_layout(cells: np.ndarray, layout: int, word_bits: int) -> np.ndarray:
+    cells = np.ascontiguousarray(cells, dtype=np.uint8)
+    y, x = cells.shape
+    xb, yb = layout_geom(layout, word_bits)
+    out = np.empty((y // yb, x // xb), dtype=_WORD_DTYPES[word_bits])
+    _check(liboracle().gor_pack_layout(layout, word_bits, _ptr(cells), x, y, _ptr(out)),
+           "pack_layout")
+    return out
+
+
+def unpack_layout(words: np.ndarray, x: int, y: int, layout: int, word_bits: int) -> np.ndarray:
+    words = np.ascontiguousarray(words)
+    out = np.empty((y, x), dtype=np.uint8)
+    _check(liboracle().gor_unpack_layout(layout, word_bits, _ptr(words), x, y, _ptr(out)),
+           "unpack_layout")
+    return out
+
+
+# Pattern loaders, restated in Python for small grids
+# (src/infrastructure/data_loader.hpp:77-146, gol-lexicon/lexicon.hpp:11-186).
+
+def parse_pattern_dictionary(text: str) -> dict:
+    """Entries {"name", {{_, X, ...}, ...}} of a patterns.cpp-style text
+    (only between the LEXICON_START / LEXICON_END markers when both are
+    present); the first entry of a repeated name wins, as in a std::map
+    built from an initializer list."""
+    a, b = text.find("/* LEXICON_START */"), text.find("/* LEXICON_END */")
+    if a >= 0 and b > a:
+        text = text[a:b]
+    out: dict = {}
+    i = 0
+    while True:
+        q = text.find('{"', i)
+        if q < 0:
+            return out
+        e = text.index('"', q + 2)
+        name = text[q + 2:e]
+        depth, j, rows, row = 0, e + 1, [], None
+        while True:
+            c = text[j]
+            j += 1
+            if c == "{":
+                depth += 1
+                if depth == 2:
+                    row = []
+            elif c == "}":
+                if depth == 2:
+                    rows.append(row)
+                depth -= 1
+                if depth == 0:
+                    break
+            elif c in "X_" and depth == 2:
+                row.append(1 if c == "X" else 0)
+        out.setdefault(name, rows)
+        i = j
+
+
+def parse_pattern_expression(expr: str) -> list:
+    """[(name, x_str, y_str)] of "name[x,y]; ..." with whitespace and ';'
+    dropped first (PatterExpression::from, lexicon.hpp:97-116)."""
+    t = "".join(c for c in expr if not (c.isspace() or c == ";"))
+    recs, i = [], 0
+    while i < len(t):
+        j = i
+        while j < len(t) and t[j] != "[":
+            j += 1
+        name = t[i:j]
+        k = j + 1
+        while k < len(t) and t[k] not in ",]":
+            k += 1
+        xs = t[j + 1:k]
+        m = k + 1
+        while m < len(t) and t[m] not in ",]":
+            m += 1
+        ys = t[k + 1:m]
+        recs.append((name, xs, ys))
+        i = m + 1
+    return recs
+
+
+def place_pattern(cells: np.ndarray, rows: list, ox: int, oy: int) -> None:
+    """Lexicon::insert_pattern_at (lexicon.hpp:160-172) on a flat raster:
+    cell (px, py) goes to element (oy + py) * X + ox + px; past the end is
+    dropped."""
+    y, x = cells.shape
+    flat = cells.reshape(-1)
+    for py, row in enumerate(rows):
+        for px, v in enumerate(row):
+            i = (oy + py) * x + ox + px
+            if i < flat.size:
+                flat[i] = v
+
+
+def load_always_changing(x: int, y: int) -> np.ndarray:
+    """AlwaysChangingSpaceLoader: a blinker at every multiple of (4, 4)."""
+    g = np.zeros((y, x), dtype=np.uint8)
+    for ox in range(0, x, 4):
+        for oy in range(0, y, 4):
+            place_pattern(g, [[1, 1, 1]], ox, oy)
+    return g
+
+
+def load_lexicon(patterns: dict, expr: str, x: int, y: int) -> np.ndarray:
+    """LexiconLoader::load_data with the given dictionary; unknown names
+    place nothing."""
+    g = np.zeros((y, x), dtype=np.uint8)
+    for name, xs, ys in parse_pattern_expression(expr):
+        ox, oy = int(xs), int(ys)
+        if name in patterns:
+            place_pattern(g, patterns[name], ox, oy)
+    return g
 
 
 def life_rows(words: np.ndarray, x: int, iters: int, word_bits: int = 64,
@@ -204,4 +357,63 @@ def ref_unpack_rows(words: np.ndarray, x: int, word_bits: int = 64) -> np.ndarra
     y = words.shape[0]
     out = np.empty((y, x), dtype=np.uint8)
     _check(_need_ref().ref_unpack_rows(word_bits, _ptr(words), x, y, _ptr(out)), "ref_unpack_rows")
+    return out
+
+
+def ref_pack_layout(cells: np.ndarray, layout: int, word_bits: int) -> np.ndarray:
+    cells = np.ascontiguousarray(cells, dtype=np.uint8)
+    y, x = cells.shape
+    xb, yb = layout_geom(layout, word_bits)
+    out = np.empty((y // yb, x // xb), dtype=_WORD_DTYPES[word_bits])
+    _check(_need_ref().ref_pack_layout(layout, word_bits, _ptr(cells), x, y, _ptr(out)),
+           "ref_pack_layout")
+    return out
+
+
+def ref_unpack_layout(words: np.ndarray, x: int, y: int, layout: int, word_bits: int) -> np.ndarray:
+    words = np.ascontiguousarray(words)
+    out = np.empty((y, x), dtype=np.uint8)
+    _check(_need_ref().ref_unpack_layout(layout, word_bits, _ptr(words), x, y, _ptr(out)),
+           "ref_unpack_layout")
+    return out
+
+
+def ref_load_zeros(x: int, y: int) -> np.ndarray:
+    out = np.full((y, x), 7, dtype=np.uint8)
+    _check(_need_ref().ref_load_zeros(x, y, _ptr(out)), "ref_load_zeros")
+    return out
+
+
+def _need_lex():
+    lib = liblexref()
+    if lib is None:
+        raise RuntimeError("reference pattern loaders oracle/_ref/libgollexref.so not present")
+    return lib
+
+
+def ref_load_always_changing(x: int, y: int) -> np.ndarray:
+    out = np.empty((y, x), dtype=np.uint8)
+    _check(_need_lex().ref_load_always_changing(x, y, _ptr(out)), "ref_load_always_changing")
+    return out
+
+
+def ref_load_lexicon(expr: str, x: int, y: int) -> np.ndarray:
+    out = np.empty((y, x), dtype=np.uint8)
+    _check(_need_lex().ref_load_lexicon(expr.encode(), x, y, _ptr(out)), "ref_load_lexicon")
+    return out
+
+
+def ref_lexicon_patterns() -> dict:
+    """name -> uint8[h, w] (short rows padded dead) of the compiled dictionary."""
+    lib = _need_lex()
+    out = {}
+    name = ctypes.create_string_buffer(4096)
+    w, h = _u64(), _u64()
+    for i in range(lib.ref_lexicon_count()):
+        _check(lib.ref_lexicon_pattern(i, name, 4096, ctypes.byref(w), ctypes.byref(h), None),
+               "ref_lexicon_pattern")
+        cells = np.zeros((h.value, w.value), dtype=np.uint8)
+        _check(lib.ref_lexicon_pattern(i, name, 4096, ctypes.byref(w), ctypes.byref(h),
+                                       _ptr(cells)), "ref_lexicon_pattern")
+        out[name.value.decode()] = cells
     return out

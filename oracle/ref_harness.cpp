@@ -17,6 +17,11 @@
 //   ref_pack_rows / ref_unpack_rows : GeneralBitGrid<uintW_t, AdderMode>
 //                                fill_grid / to_grid
 //                                (src/algorithms/_shared/bitwise/general_bit_grid.hpp:171-246)
+//   ref_pack_layout / ref_unpack_layout : the same for BitColumnsMode and
+//                                BitTileMode (bit_modes.hpp:10-125, 165-177)
+//   ref_load_zeros             : ZerosLoader<2,char> (data_loader.hpp:128-146)
+// (the pattern loaders, which need the reference's compiled pattern
+// dictionary, are in ref_lexicon.cpp)
 //
 // The algorithm phases are called directly in the order the reference's
 // ExperimentManager::perform_alg uses (experiment_manager.hpp:365-394);
@@ -74,6 +79,42 @@ void run_phases(Alg& alg, const uint8_t* in, std::size_t x, std::size_t y, std::
 
 template <typename word_t>
 using RowBitGrid = algorithms::GeneralBitGrid<word_t, algorithms::AdderMode>;
+
+// layout 1 = BitColumnsMode, 2 = BitTileMode.
+template <typename word_t, typename mode>
+int pack_as(const uint8_t* cells, uint64_t x, uint64_t y, void* words) {
+    algorithms::GeneralBitGrid<word_t, mode> bg(grid_from(cells, x, y));
+    std::memcpy(words, bg.data(), bg.size() * sizeof(word_t));
+    return 0;
+}
+
+template <typename word_t, typename mode>
+int unpack_as(const void* words, uint64_t x, uint64_t y, uint8_t* cells) {
+    algorithms::GeneralBitGrid<word_t, mode> bg(x, y);
+    std::memcpy(bg.data(), words, bg.size() * sizeof(word_t));
+    grid_to(bg.template to_grid<char>(), cells);
+    return 0;
+}
+
+template <typename mode>
+int pack_bits(int word_bits, const uint8_t* cells, uint64_t x, uint64_t y, void* words) {
+    switch (word_bits) {
+        case 16: return pack_as<uint16_t, mode>(cells, x, y, words);
+        case 32: return pack_as<uint32_t, mode>(cells, x, y, words);
+        case 64: return pack_as<uint64_t, mode>(cells, x, y, words);
+        default: return -2;
+    }
+}
+
+template <typename mode>
+int unpack_bits(int word_bits, const void* words, uint64_t x, uint64_t y, uint8_t* cells) {
+    switch (word_bits) {
+        case 16: return unpack_as<uint16_t, mode>(words, x, y, cells);
+        case 32: return unpack_as<uint32_t, mode>(words, x, y, cells);
+        case 64: return unpack_as<uint64_t, mode>(words, x, y, cells);
+        default: return -2;
+    }
+}
 
 } // namespace
 
@@ -149,6 +190,38 @@ int ref_unpack_rows(int word_bits, const void* words, uint64_t x, uint64_t y, ui
         } else {
             return -2;
         }
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+int ref_pack_layout(int layout, int word_bits, const uint8_t* cells, uint64_t x, uint64_t y,
+                    void* words) {
+    try {
+        if (layout == 1) return pack_bits<algorithms::BitColumnsMode>(word_bits, cells, x, y, words);
+        if (layout == 2) return pack_bits<algorithms::BitTileMode>(word_bits, cells, x, y, words);
+        return -2;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+int ref_unpack_layout(int layout, int word_bits, const void* words, uint64_t x, uint64_t y,
+                      uint8_t* cells) {
+    try {
+        if (layout == 1) return unpack_bits<algorithms::BitColumnsMode>(word_bits, words, x, y, cells);
+        if (layout == 2) return unpack_bits<algorithms::BitTileMode>(word_bits, words, x, y, cells);
+        return -2;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+int ref_load_zeros(uint64_t x, uint64_t y, uint8_t* out) {
+    try {
+        infrastructure::ZerosLoader<2, char> loader;
+        grid_to(loader.load_data(make_params(x, y, 0, 0)), out);
         return 0;
     } catch (const std::exception&) {
         return -1;

@@ -351,6 +351,22 @@ int gol_set_input_words(gol_engine* e, const void* words, uint64_t x, uint64_t y
     return GOL_OK;
 }
 
+int gol_set_input_layout(gol_engine* e, const void* words, int layout, uint32_t word_bits) {
+    if (!e) return GOL_E_INVALID;
+    uint32_t xb, yb;
+    if (!golb200::layout_geom(layout, word_bits, &xb, &yb))
+        return e->fail(GOL_E_INVALID, "unknown layout or word_bits not 16, 32 or 64");
+    if (e->x % xb || e->y % yb) return e->fail(GOL_E_INVALID, "grid is not a whole number of layout words");
+    if (!words && e->x * e->y) return e->fail(GOL_E_INVALID, "null words");
+    if (e->initialized) return e->fail(GOL_E_STATE, "set_input while device data is live");
+    int rc = ensure_host(e);
+    if (rc) return rc;
+    golb200::host_layout_to_rows(words, e->x, e->y, layout, word_bits, xb, yb, e->h_words);
+    e->has_host_grid = true;
+    e->performed = 0;
+    return GOL_OK;
+}
+
 int gol_init(gol_engine* e) {
     if (!e) return GOL_E_INVALID;
     if (!e->has_host_grid) return e->fail(GOL_E_STATE, "initialize before set_input");
@@ -526,6 +542,18 @@ int gol_fetch_words(gol_engine* e, void* words, uint32_t word_bits) {
     if (!e->has_host_grid || e->initialized) return e->fail(GOL_E_STATE, "fetch before finalize");
     if (!words && e->h_bytes) return e->fail(GOL_E_INVALID, "null words");
     std::memcpy(words, e->h_words, e->h_bytes);
+    return GOL_OK;
+}
+
+int gol_fetch_layout(gol_engine* e, void* words, int layout, uint32_t word_bits) {
+    if (!e) return GOL_E_INVALID;
+    uint32_t xb, yb;
+    if (!golb200::layout_geom(layout, word_bits, &xb, &yb))
+        return e->fail(GOL_E_INVALID, "unknown layout or word_bits not 16, 32 or 64");
+    if (e->x % xb || e->y % yb) return e->fail(GOL_E_INVALID, "grid is not a whole number of layout words");
+    if (!e->has_host_grid || e->initialized) return e->fail(GOL_E_STATE, "fetch before finalize");
+    if (!words && e->h_bytes) return e->fail(GOL_E_INVALID, "null words");
+    golb200::host_rows_to_layout(e->h_words, e->x, e->y, layout, word_bits, xb, yb, words);
     return GOL_OK;
 }
 

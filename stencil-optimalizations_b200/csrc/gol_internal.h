@@ -42,6 +42,17 @@ struct LocalPlan {
     int ctas = 0;      // persistent one-warp CTAs of the tile kernel
 };
 
+// Word layouts (gol_layouts.cu): X_BITS x Y_BITS cells per word.
+bool layout_geom(int layout, uint32_t wb, uint32_t* xb, uint32_t* yb);
+void host_cells_to_layout(const uint8_t* cells, size_t x, size_t y, int layout, uint32_t wb,
+                          uint32_t xb, uint32_t yb, void* words);
+void host_layout_to_cells(const void* words, size_t x, size_t y, int layout, uint32_t wb,
+                          uint32_t xb, uint32_t yb, uint8_t* cells);
+void host_layout_to_rows(const void* words, size_t x, size_t y, int layout, uint32_t wb,
+                         uint32_t xb, uint32_t yb, uint32_t* rows);
+void host_rows_to_layout(const uint32_t* rows, size_t x, size_t y, int layout, uint32_t wb,
+                         uint32_t xb, uint32_t yb, void* words);
+
 struct LocalState {
     uint8_t* changed[2] = {nullptr, nullptr};   // per tile, by pass parity
     int* list = nullptr;                        // active tiles of the current pass

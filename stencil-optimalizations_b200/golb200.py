@@ -30,6 +30,22 @@ GOL_E_CUDA = -3
 GOL_E_NOMEM = -4
 GOL_E_UNSUPPORTED = -5
 
+LAYOUTS = {"rows": 0, "columns": 1, "tiles": 2}
+_WORD_DTYPES = {16: np.uint16, 32: np.uint32, 64: np.uint64}
+
+
+def layout_block(layout: str, word_bits: int) -> tuple:
+    """(cells per word in x, in y) of a layout (bit_modes.hpp:10-177)."""
+    if word_bits not in _WORD_DTYPES:
+        raise ValueError("word_bits must be 16, 32 or 64")
+    if layout == "rows":
+        return word_bits, 1
+    if layout == "columns":
+        return 1, word_bits
+    if layout == "tiles":
+        return {16: (4, 4), 32: (8, 4), 64: (8, 8)}[word_bits]
+    raise ValueError(f"unknown layout {layout!r}")
+
 ALGORITHMS = {"auto": 0, "rows": 1, "local": 2}
 
 
@@ -79,6 +95,12 @@ def lib():
     L.gol_fetch_u8.argtypes = [_vp, _vp]
     L.gol_fetch_i32.argtypes = [_vp, _vp]
     L.gol_fetch_words.argtypes = [_vp, _vp, _u32]
+    L.gol_set_input_layout.argtypes = [_vp, _vp, ctypes.c_int, _u32]
+    L.gol_fetch_layout.argtypes = [_vp, _vp, ctypes.c_int, _u32]
+    L.gol_pack_layout.argtypes = [_vp, _u64, _u64, ctypes.c_int, _u32, _vp]
+    L.gol_unpack_layout.argtypes = [_vp, _u64, _u64, ctypes.c_int, _u32, _vp]
+    L.gol_layout_to_rows_device.argtypes = [_vp, _vp, _u64, _u64, ctypes.c_int, _u32, _vp]
+    L.gol_rows_to_layout_device.argtypes = [_vp, _vp, _u64, _u64, ctypes.c_int, _u32, _vp]
     L.gol_performed.argtypes = [_vp]
     L.gol_performed.restype = _u64
     L.gol_destroy.argtypes = [_vp]
@@ -102,6 +124,20 @@ def lib():
     L.gol_workload_uneven.argtypes = [_u64, _u32, _u32, _u32, _u32, ctypes.c_double,
                                       ctypes.c_double, _u64, _u64, _vp, _vp, _vp, _vp, _vp]
     L.gol_load_bernoulli.argtypes = [_vp, _u64, _u64, _u64, ctypes.c_double]
+    L.gol_load_zeros.argtypes = [_vp, _u64, _u64]
+    L.gol_load_always_changing.argtypes = [_vp, _u64, _u64]
+    L.gol_lexicon_create.argtypes = [ctypes.POINTER(_vp)]
+    L.gol_lexicon_add_text.argtypes = [_vp, ctypes.c_char_p]
+    L.gol_lexicon_add_file.argtypes = [_vp, ctypes.c_char_p]
+    L.gol_lexicon_count.argtypes = [_vp]
+    L.gol_lexicon_pattern_size.argtypes = [_vp, ctypes.c_char_p, ctypes.POINTER(_u64),
+                                           ctypes.POINTER(_u64)]
+    L.gol_lexicon_insert.argtypes = [_vp, ctypes.c_char_p, _vp, _u64, _u64]
+    L.gol_lexicon_insert_repeating.argtypes = [_vp, ctypes.c_char_p, _u64, _u64, _vp, _u64, _u64]
+    L.gol_lexicon_last_error.argtypes = [_vp]
+    L.gol_lexicon_last_error.restype = ctypes.c_char_p
+    L.gol_lexicon_destroy.argtypes = [_vp]
+    L.gol_lexicon_destroy.restype = None
     L.gol_poisson_arrivals.argtypes = [_u64, _u32, ctypes.c_double, _vp]
     L.gol_batch_create.argtypes = [ctypes.POINTER(_vp), ctypes.c_int32, _vp]
     L.gol_batch_add.argtypes = [_vp, _vp, _u64, _u64, _u64, ctypes.POINTER(ctypes.c_int32)]
@@ -233,6 +269,15 @@ class GolB200:
         self._check(lib().gol_set_input_words(self._e, _ptr(w), self.x, self.y, word_bits),
                     "set_input_words")
 
+    def set_input_layout(self, words: np.ndarray, layout: str, word_bits: int) -> None:
+        """Input as words of the column / tile / rows layout."""
+        xb, yb = layout_block(layout, word_bits)
+        w = np.ascontiguousarray(words, dtype=_WORD_DTYPES[word_bits])
+        if w.size * xb * yb != self.x * self.y:
+            raise ValueError("words do not cover the grid")
+        self._check(lib().gol_set_input_layout(self._e, _ptr(w), LAYOUTS[layout], word_bits),
+                    "set_input_layout")
+
     def initialize_data_structures(self) -> None:
         self._check(lib().gol_init(self._e), "initialize")
 
@@ -258,6 +303,13 @@ class GolB200:
         dt = np.uint64 if word_bits == 64 else np.uint32
         out = np.empty((self.y, self.x // word_bits), dtype=dt)
         self._check(lib().gol_fetch_words(self._e, _ptr(out), word_bits), "fetch_words")
+        return out
+
+    def fetch_layout(self, layout: str, word_bits: int) -> np.ndarray:
+        xb, yb = layout_block(layout, word_bits)
+        out = np.empty((self.y // yb, self.x // xb), dtype=_WORD_DTYPES[word_bits])
+        self._check(lib().gol_fetch_layout(self._e, _ptr(out), LAYOUTS[layout], word_bits),
+                    "fetch_layout")
         return out
 
     def actually_performed_iterations(self) -> int:
@@ -337,6 +389,98 @@ def load_sparse_patches(x: int, y: int, seed: int, patch: int = 64, fraction: fl
     return out
 
 
+def load_zeros(x: int, y: int) -> np.ndarray:
+    """ZerosLoader (src/infrastructure/data_loader.hpp:128-146): every cell dead."""
+    out = np.empty((y, x), dtype=np.uint8)
+    rc = lib().gol_load_zeros(_ptr(out), x, y)
+    if rc < 0:
+        raise RuntimeError(f"gol_load_zeros failed with status {rc}")
+    return out
+
+
+def load_always_changing(x: int, y: int) -> np.ndarray:
+    """AlwaysChangingSpaceLoader (data_loader.hpp:102-125): a blinker every
+    4 cells in x and y on a dead grid."""
+    out = np.empty((y, x), dtype=np.uint8)
+    rc = lib().gol_load_always_changing(_ptr(out), x, y)
+    if rc < 0:
+        raise RuntimeError(f"gol_load_always_changing failed with status {rc}")
+    return out
+
+
+class Lexicon:
+    """Pattern dictionary and expression loader (LexiconLoader,
+    data_loader.hpp:77-99; lexicon::Lexicon, gol-lexicon/lexicon.hpp).
+
+    Entries come from text in the format of the reference's generated
+    dictionary (gol-lexicon/patterns.cpp); "blinker" is built in."""
+
+    def __init__(self, path: str | None = None, text: str | None = None):
+        h = _vp()
+        rc = lib().gol_lexicon_create(ctypes.byref(h))
+        if rc != GOL_OK:
+            raise RuntimeError(f"gol_lexicon_create failed with status {rc}")
+        self._h = h
+        if path is not None:
+            self.add_file(path)
+        if text is not None:
+            self.add_text(text)
+
+    def _check(self, rc: int, what: str) -> int:
+        if rc < 0:
+            msg = lib().gol_lexicon_last_error(self._h).decode()
+            raise ValueError(f"{what}: {msg} (status {rc})")
+        return rc
+
+    def add_text(self, text: str) -> int:
+        return self._check(lib().gol_lexicon_add_text(self._h, text.encode()), "add_text")
+
+    def add_file(self, path: str) -> int:
+        return self._check(lib().gol_lexicon_add_file(self._h, os.fsencode(path)), "add_file")
+
+    def __len__(self) -> int:
+        return lib().gol_lexicon_count(self._h)
+
+    def pattern_size(self, name: str) -> tuple:
+        w, h = _u64(), _u64()
+        self._check(lib().gol_lexicon_pattern_size(self._h, name.encode(), ctypes.byref(w),
+                                                   ctypes.byref(h)), f"pattern {name!r}")
+        return w.value, h.value
+
+    def insert(self, expression: str, cells: np.ndarray) -> int:
+        """Place the patterns of `expression` ("name[x,y]; ...") into the
+        (y, x) uint8 grid in place; returns the records placed."""
+        if cells.dtype != np.uint8 or not cells.flags.c_contiguous or cells.ndim != 2:
+            raise ValueError("cells must be a C-contiguous (y, x) uint8 array")
+        y, x = cells.shape
+        return self._check(lib().gol_lexicon_insert(self._h, expression.encode(), _ptr(cells),
+                                                    x, y), "insert")
+
+    def insert_repeating(self, name: str, x_jump: int, y_jump: int, cells: np.ndarray) -> None:
+        if cells.dtype != np.uint8 or not cells.flags.c_contiguous or cells.ndim != 2:
+            raise ValueError("cells must be a C-contiguous (y, x) uint8 array")
+        y, x = cells.shape
+        self._check(lib().gol_lexicon_insert_repeating(self._h, name.encode(), x_jump, y_jump,
+                                                       _ptr(cells), x, y), "insert_repeating")
+
+    def load(self, expression: str, x: int, y: int) -> np.ndarray:
+        """LexiconLoader::load_data: a dead (y, x) grid with the expression's patterns."""
+        out = np.zeros((y, x), dtype=np.uint8)
+        self.insert(expression, out)
+        return out
+
+    def close(self) -> None:
+        if self._h:
+            lib().gol_lexicon_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def probe_int_peak(stream: int = 0) -> float:
     """Measured 32-bit LOP3 lane-ops/s of the current device."""
     v = ctypes.c_double()
@@ -363,6 +507,42 @@ def unpack_cells_device(d_words: int, d_cells: int, x: int, y: int, stream: int 
     rc = lib().gol_unpack_cells_device(d_words, d_cells, x, y, stream)
     if rc != GOL_OK:
         raise RuntimeError(f"gol_unpack_cells_device failed with status {rc}")
+
+
+def pack_layout(cells: np.ndarray, layout: str, word_bits: int) -> np.ndarray:
+    """Host cells -> words of a layout (GeneralBitGrid::fill_grid)."""
+    cells = np.ascontiguousarray(cells, dtype=np.uint8)
+    y, x = cells.shape
+    xb, yb = layout_block(layout, word_bits)
+    out = np.empty((y // yb, x // xb), dtype=_WORD_DTYPES[word_bits])
+    rc = lib().gol_pack_layout(_ptr(cells), x, y, LAYOUTS[layout], word_bits, _ptr(out))
+    if rc != GOL_OK:
+        raise ValueError(f"gol_pack_layout failed with status {rc}")
+    return out
+
+
+def unpack_layout(words: np.ndarray, x: int, y: int, layout: str, word_bits: int) -> np.ndarray:
+    """Words of a layout -> host cells (GeneralBitGrid::to_grid)."""
+    w = np.ascontiguousarray(words, dtype=_WORD_DTYPES[word_bits])
+    out = np.empty((y, x), dtype=np.uint8)
+    rc = lib().gol_unpack_layout(_ptr(w), x, y, LAYOUTS[layout], word_bits, _ptr(out))
+    if rc != GOL_OK:
+        raise ValueError(f"gol_unpack_layout failed with status {rc}")
+    return out
+
+
+def layout_to_rows_device(d_src: int, d_rows: int, x: int, y: int, layout: str, word_bits: int,
+                          stream: int = 0) -> None:
+    rc = lib().gol_layout_to_rows_device(d_src, d_rows, x, y, LAYOUTS[layout], word_bits, stream)
+    if rc != GOL_OK:
+        raise RuntimeError(f"gol_layout_to_rows_device failed with status {rc}")
+
+
+def rows_to_layout_device(d_rows: int, d_dst: int, x: int, y: int, layout: str, word_bits: int,
+                          stream: int = 0) -> None:
+    rc = lib().gol_rows_to_layout_device(d_rows, d_dst, x, y, LAYOUTS[layout], word_bits, stream)
+    if rc != GOL_OK:
+        raise RuntimeError(f"gol_rows_to_layout_device failed with status {rc}")
 
 
 # ---------------------------------------------------------------------------
