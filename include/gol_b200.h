@@ -306,9 +306,13 @@ int gol_probe_int_peak(double* lane_ops_per_s, void* stream);
 
 /* Many independent grids, each with its own size and generation count,
  * advanced together by one persistent kernel launch (captured as a CUDA
- * graph). Per grid an autotuner picks words per lane, temporal depth and
- * band height; gol_batch_set_plan overrides it. No reference counterpart:
- * the reference runs one grid per invocation (experiment_manager.hpp:365-394). */
+ * graph). An autotuner picks one words-per-lane width and temporal depth for
+ * the whole batch (one pipeline body per launch) and a band height per grid;
+ * gol_batch_set_plan overrides a grid's plan (mixed widths then run the
+ * general kernel). gol_batch_plan reports the plan of the uploaded batch, or
+ * the grid's own best plan before gol_batch_upload. No reference
+ * counterpart: the reference runs one grid per invocation
+ * (experiment_manager.hpp:365-394). */
 typedef struct gol_batch gol_batch;
 
 int gol_batch_create(gol_batch** out, int32_t device, void* stream);
@@ -322,7 +326,8 @@ int gol_batch_plan(const gol_batch* b, int32_t grid_id, uint32_t* lane_words,
 /* Plans all grids and copies inputs and the work list to the device. */
 int gol_batch_upload(gol_batch* b);
 /* Runs every grid to its generation count in one persistent launch
- * (asynchronous; gol_batch_sync waits). Re-running restarts from the inputs. */
+ * (asynchronous; gol_batch_sync waits). Every run restarts from the inputs,
+ * restored from a device copy made at upload. */
 int gol_batch_run(gol_batch* b);
 /* Baseline: the same grids one after another through the single-grid pass
  * kernel, one launch per k-generation pass per grid. */

@@ -16,15 +16,19 @@
 //   order       items are numbered critical-path first: by descending
 //               remaining passes of their grid, so the longest grids start
 //               at once and short ones fill in; persistent one-warp CTAs
-//               take tickets from an atomic counter.
+//               take tickets from an atomic counter, claiming the next one
+//               while working on the current one.
 //   dependency  (g, s, j, p) needs (g, s-1..s+1, j-1..j+1, p-1) finished:
 //               that is every word it reads, and it also ends every read of
-//               the buffer it overwrites. A per-group counter holds the passes done; the
-//               waiting lane polls it with ld.acquire, bounded: after
-//               kSpinLimit polls the CTA records GOL_E_TIMEOUT and stops.
-//               Every dependency has a smaller ticket, held by a CTA that is
-//               resident and never waits on a larger one, so the wait always
-//               ends; the bound is only a guard.
+//               the buffer it overwrites. A per-group counter holds the
+//               passes done; one lane per dependency polls it with
+//               ld.acquire, bounded: after kSpinLimit polls the CTA records
+//               GOL_E_TIMEOUT and stops. Every dependency has a smaller
+//               ticket. The smallest unfinished ticket's dependencies are
+//               all finished, and its CTA (resident) holds no smaller
+//               unfinished item (a CTA claims tickets in increasing order),
+//               so it is running or about to run that item: the wait always
+//               ends, and the bound is only a guard.
 //   release     each lane fences its stores, the warp syncs, lane 0 stores
 //               the new pass count with st.release.
 //
@@ -141,52 +145,70 @@ __device__ __forceinline__ void seg_dispatch(int k, const BatchGrid& G, int grou
     }
 }
 
+// WPL_ONLY = 1, 2 or 4: every grid of the launch uses that many words per
+// lane, so the kernel holds one family of pipeline bodies (its registers
+// and instruction footprint are that family's); 0 dispatches on each grid's
+// own width. Warps of one SM that run different bodies compete for the
+// instruction cache, which halved throughput in measurements, so the
+// planner gives a batch one width and one depth.
+template <int WPL_ONLY>
 __global__ void __launch_bounds__(32, GOL_BATCH_MIN_BLOCKS)
 batch_kernel(const BatchGrid* __restrict__ grids, const BatchItem* __restrict__ items, int nitems,
              int* ticket, int* done, int* status, unsigned long long* census) {
-    __shared__ __align__(16) uint32_t ring[kRowRing * 32 * 4];
+    __shared__ __align__(16) uint32_t ring[kRowRing * 32 * (WPL_ONLY ? WPL_ONLY : 4)];
     const int lane = threadIdx.x & 31;
-    for (;;) {
-        int t = 0;
-        if (lane == 0) t = atomicAdd(ticket, 1);
-        t = __shfl_sync(0xffffffffu, t, 0);
-        if (t >= nitems) return;
+    int t = 0;
+    if (lane == 0) t = atomicAdd(ticket, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    while (t < nitems) {
         const BatchItem it = items[t];
         const BatchGrid G = grids[it.grid];
         int* mine = done + G.done_base + it.group * G.nslices + it.slice;
         const long long t_wait = clock64();
         if (it.pass > 0) {
-            // Every lane acquires every counter it depends on, so each lane's
-            // own copies below are ordered after the producers' releases.
-            bool ok = true;
+            // Lane d polls dependency d (3x3 neighbourhood of (group, slice))
+            // until it reached this pass; then every lane acquires every
+            // counter (each is already there), so each lane's own copies below
+            // are ordered after the producers' releases.
             const int jlo = max(it.group - 1, 0), jhi = min(it.group + 1, G.ngroups - 1);
             const int slo = max(it.slice - 1, 0), shi = min(it.slice + 1, G.nslices - 1);
-            for (int j = jlo; j <= jhi && ok; ++j) {
-                for (int sl = slo; sl <= shi && ok; ++sl) {
-                    const int* p = done + G.done_base + j * G.nslices + sl;
-                    long long spins = 0;
-                    while (ld_acquire(p) < it.pass) {
-                        if (++spins > kSpinLimit || *(volatile int*)status != 0) {
-                            ok = false;
-                            break;
-                        }
-                        __nanosleep(100);
+            const int nj = jhi - jlo + 1, ns = shi - slo + 1;
+            bool ok = true;
+            if (lane < nj * ns) {
+                const int* p = done + G.done_base + (jlo + lane / ns) * G.nslices + slo + lane % ns;
+                long long spins = 0;
+                while (ld_acquire(p) < it.pass) {
+                    if (++spins > kSpinLimit || *(volatile int*)status != 0) {
+                        ok = false;
+                        break;
                     }
+                    __nanosleep(64);
                 }
             }
             if (!__all_sync(0xffffffffu, ok)) {
                 if (lane == 0) atomicCAS(status, 0, GOL_E_TIMEOUT);
                 return;
             }
+            int seen = 0;
+            for (int d = 0; d < nj * ns; ++d)
+                seen |= ld_acquire(done + G.done_base + (jlo + d / ns) * G.nslices + slo + d % ns);
+            asm volatile("" ::"r"(seen));
         }
+        // Claim the next item now: the atomic's round trip overlaps the work.
+        int next = 0;
+        if (lane == 0) next = atomicAdd(ticket, 1);
         const long long t_work = clock64();
         const int k = it.pass == G.passes - 1 ? G.last_k : G.k;
         const uint32_t* src = G.buf[(G.parity0 + it.pass) & 1];
         uint32_t* dst = G.buf[(G.parity0 + it.pass + 1) & 1];
-        switch (G.wpl) {
-            case 4: seg_dispatch<4>(k, G, it.group, it.slice, src, dst, ring); break;
-            case 2: seg_dispatch<2>(k, G, it.group, it.slice, src, dst, ring); break;
-            default: seg_dispatch<1>(k, G, it.group, it.slice, src, dst, ring); break;
+        if constexpr (WPL_ONLY != 0) {
+            seg_dispatch<WPL_ONLY>(k, G, it.group, it.slice, src, dst, ring);
+        } else {
+            switch (G.wpl) {
+                case 4: seg_dispatch<4>(k, G, it.group, it.slice, src, dst, ring); break;
+                case 2: seg_dispatch<2>(k, G, it.group, it.slice, src, dst, ring); break;
+                default: seg_dispatch<1>(k, G, it.group, it.slice, src, dst, ring); break;
+            }
         }
         __threadfence();
         __syncwarp();
@@ -197,22 +219,25 @@ batch_kernel(const BatchGrid* __restrict__ grids, const BatchItem* __restrict__ 
                 atomicAdd(census + 1, (unsigned long long)(clock64() - t_work));
             }
         }
+        t = __shfl_sync(0xffffffffu, next, 0);
     }
 }
 
 } // namespace
 
 // ---------------------------------------------------------------------------
-// Autotuner: per grid, pick (words per lane, depth, band height).
+// Autotuner: one (words per lane, depth) for the whole batch, a band height
+// per grid.
 //
-// Model: a work item is (band + 3k) pipeline steps of k stages on one warp
-// plus, once per pass, each row's load and store (c_row stage-steps per
-// row) and a fixed start-up and dependency cost (c_item stage-steps); a
-// stage-step on a WPL-wide lane costs c[WPL] (relative warp time):
-//     item = ((band + 3k) * k + c_row * band) * c[WPL] + c_item.
+// Model, in units of one word through one stage on a 4-word lane: a work
+// item is (band + 3k) pipeline steps of k stages, each step moving WPL words
+// per lane at a per-word cost cw[WPL], plus each row's load and store once
+// per pass (c_row stage-steps per row) and a fixed start-up and dependency
+// cost (c_item):
+//     item = ((band + 3k) * k + c_row * band) * WPL * cw[WPL] + c_item.
 // The per-pass terms are what make deeper passes pay: on the dense kernel a
 // 1-generation pass costs ~1.4x a 4-generation pass per generation, which
-// c_row = 0.6 and c_item = 30 reproduce. A grid's work is
+// c_row = 0.6 and c_item reproduce. A grid's work is
 //     passes * nslices * ngroups * item
 // for passes = ceil(gens / k), ngroups = ceil(Y / (S * band)), and its
 // dependency chain (one item per pass, in order) is passes * item.
@@ -221,13 +246,14 @@ batch_kernel(const BatchGrid* __restrict__ grids, const BatchItem* __restrict__ 
 // batch's work-bound time are then re-planned to minimise work / resident
 // warps + chain (shorter bands: more, quicker items per pass). Candidates:
 // WPL in {1, 2, 4} (W % WPL == 0), k in 1..4, band in {16, 24, 32, 48, 64}
-// with band >= 2k.
+// with band >= 2k. gol_batch_upload runs this for every (WPL, k) the whole
+// batch can use and keeps the pair with the smallest estimated time.
 // ---------------------------------------------------------------------------
 
 struct BatchTuning {
-    double c[5] = {0, 1.0, 1.15, 0, 1.45};   // relative cost per stage-step by WPL
-    double c_row = 0.6;                       // per row per pass (load + store)
-    double c_item = 30.0;                     // per item (start-up, dependency wait, release)
+    double cw[5] = {0, 1.45, 1.15, 0, 1.0};   // relative cost per word-stage-step by WPL
+    double c_row = 0.6;                        // per row per pass (load + store)
+    double c_item = 120.0;                     // per item (start-up, dependency wait, release)
 };
 
 static BatchTuning g_tuning;
@@ -251,7 +277,7 @@ bool choose_batch_plan(int W, int Y, uint64_t gens, int force_wpl, int force_k, 
                 const int ngroups = (Y + S * band - 1) / (S * band);
                 const uint64_t passes = (gens + k - 1) / k;
                 const double item =
-                    ((double)(band + 3 * k) * k + g_tuning.c_row * band) * g_tuning.c[wpl] +
+                    ((double)(band + 3 * k) * k + g_tuning.c_row * band) * wpl * g_tuning.cw[wpl] +
                     g_tuning.c_item;
                 const double cost = (double)passes * nslices * ngroups * item;
                 // one item per pass on the chain of dependent passes
@@ -303,11 +329,31 @@ size_t order_batch_items(const BatchGrid* grids, size_t ngrids, BatchItem* out) 
     return n;
 }
 
-int batch_kernel_ctas_per_sm() {
+template <int W>
+static int ctas_per_sm_of() {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, 32, 0) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<W>, 32, 0) != cudaSuccess)
         per_sm = 1;
     return std::max(1, per_sm);
+}
+
+int batch_kernel_ctas_per_sm(int wpl_only) {
+    switch (wpl_only) {
+        case 4: return ctas_per_sm_of<4>();
+        case 2: return ctas_per_sm_of<2>();
+        case 1: return ctas_per_sm_of<1>();
+        default: return ctas_per_sm_of<0>();
+    }
+}
+
+int batch_uniform_wpl(const BatchGrid* grids, size_t ngrids) {
+    int w = 0;
+    for (size_t g = 0; g < ngrids; ++g) {
+        if (grids[g].passes == 0) continue;
+        if (w && grids[g].wpl != w) return 0;
+        w = grids[g].wpl;
+    }
+    return w;
 }
 
 void batch_grid_from_choice(const GridChoice& ch, int W, int Y, BatchGrid* g) {
@@ -328,15 +374,28 @@ void batch_grid_from_choice(const GridChoice& ch, int W, int Y, BatchGrid* g) {
 
 cudaError_t launch_batch_kernel(const BatchGrid* d_grids, const BatchItem* d_items, int nitems,
                                 int* d_ticket, int* d_done, int* d_status, int num_sms,
-                                cudaStream_t stream, unsigned long long* d_census) {
+                                cudaStream_t stream, unsigned long long* d_census, int wpl_only) {
     if (nitems <= 0) return cudaSuccess;
-    int per_sm = 0;
-    cudaError_t ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, 32, 0);
-    if (ce != cudaSuccess) return ce;
-    per_sm = std::max(1, per_sm);
-    const int ctas = std::min(nitems, num_sms * per_sm);   // every CTA resident at once
-    batch_kernel<<<ctas, 32, 0, stream>>>(d_grids, d_items, nitems, d_ticket, d_done, d_status,
-                                          d_census);
+    // every CTA resident at once (the dependency waits rely on it)
+    const int ctas = std::min(nitems, num_sms * batch_kernel_ctas_per_sm(wpl_only));
+    switch (wpl_only) {
+        case 4:
+            batch_kernel<4><<<ctas, 32, 0, stream>>>(d_grids, d_items, nitems, d_ticket, d_done,
+                                                     d_status, d_census);
+            break;
+        case 2:
+            batch_kernel<2><<<ctas, 32, 0, stream>>>(d_grids, d_items, nitems, d_ticket, d_done,
+                                                     d_status, d_census);
+            break;
+        case 1:
+            batch_kernel<1><<<ctas, 32, 0, stream>>>(d_grids, d_items, nitems, d_ticket, d_done,
+                                                     d_status, d_census);
+            break;
+        default:
+            batch_kernel<0><<<ctas, 32, 0, stream>>>(d_grids, d_items, nitems, d_ticket, d_done,
+                                                     d_status, d_census);
+            break;
+    }
     return cudaPeekAtLastError();
 }
 
@@ -362,13 +421,17 @@ struct gol_batch {
         golb200::GridChoice choice{};
         int force_wpl = 0, force_k = 0, force_band = 0;
         size_t offset = 0;                // word offset of buf[0] in the arena
-        size_t stride = 0;                // words from buf[0] to buf[1]
+        size_t stride = 0;                // words from buf[0] to buf[1] (the input region's size)
         int result_buf = 0;               // buffer holding the last run's result
     };
     std::vector<Entry> grids;
 
-    uint32_t* arena = nullptr;            // all grids' ping-pong buffers
+    // Arena: [every grid's buf[0] | every grid's buf[1] | a copy of the
+    // inputs], each region input_words long. A run starts by restoring the
+    // buf[0] region from the copy (one device-to-device copy).
+    uint32_t* arena = nullptr;
     size_t arena_words = 0;
+    size_t input_words = 0;
     BatchGrid* d_grids = nullptr;
     BatchItem* d_items = nullptr;
     int* d_done = nullptr;
@@ -376,6 +439,7 @@ struct gol_batch {
     int* d_status = nullptr;
     unsigned long long* d_census = nullptr;   // wait / work SM cycles of the last run
     int nitems = 0, ngroups_total = 0;
+    int wpl_only = 0;                     // lane width shared by every grid (0: mixed)
     bool uploaded = false, ran = false;
     cudaGraphExec_t graph = nullptr;
     double last_ms = 0;
@@ -473,8 +537,9 @@ int gol_batch_plan(const gol_batch* b, int32_t grid_id, uint32_t* lane_words,
                    uint32_t* temporal_steps, uint32_t* band_rows, uint32_t* segments) {
     if (!b || grid_id < 0 || grid_id >= (int)b->grids.size()) return GOL_E_INVALID;
     const auto& e = b->grids[grid_id];
-    golb200::GridChoice ch;
-    if (!golb200::choose_batch_plan(e.W, e.Y, e.gens, e.force_wpl, e.force_k, e.force_band, &ch))
+    golb200::GridChoice ch = e.choice;   // the uploaded batch's plan
+    if (!b->uploaded &&
+        !golb200::choose_batch_plan(e.W, e.Y, e.gens, e.force_wpl, e.force_k, e.force_band, &ch))
         return GOL_E_UNSUPPORTED;
     if (lane_words) *lane_words = ch.wpl;
     if (temporal_steps) *temporal_steps = ch.k;
@@ -492,23 +557,50 @@ int gol_batch_upload(gol_batch* b) {
     std::vector<BatchGrid> hg;
     size_t words = 0;
     int groups = 0, max_passes = 0;
-    // Plans: least work first, then shorter chains for the grids whose
-    // chain would outlast the work-bound time of the whole batch.
-    const double parallel = (double)b->num_sms * golb200::batch_kernel_ctas_per_sm();
-    double total_work = 0;
-    for (auto& e : b->grids) {
-        if (!golb200::choose_batch_plan(e.W, e.Y, std::max<uint64_t>(e.gens, 1), e.force_wpl,
-                                        e.force_k, e.force_band, &e.choice))
-            return b->fail(GOL_E_UNSUPPORTED, "no batched plan for a grid");
-        total_work += e.choice.cost;
+    // Plans: for every (words per lane, depth) all grids can use, each grid
+    // takes its least-work band, then grids whose chain would outlast the
+    // work-bound time of the whole batch take shorter chains; the pair with
+    // the smallest max(work / resident warps, longest chain) wins. Grids with
+    // a plan forced by gol_batch_set_plan keep it.
+    const double parallel = (double)b->num_sms * golb200::batch_kernel_ctas_per_sm(0);
+    double best_est = -1;
+    std::vector<golb200::GridChoice> best;
+    for (int wpl : {4, 2, 1}) {
+        for (int k = golb200::kBatchMaxK; k >= 1; --k) {
+            std::vector<golb200::GridChoice> ch(b->grids.size());
+            double total_work = 0;
+            bool ok = true;
+            for (size_t i = 0; i < b->grids.size() && ok; ++i) {
+                const auto& e = b->grids[i];
+                ok = golb200::choose_batch_plan(e.W, e.Y, std::max<uint64_t>(e.gens, 1),
+                                                e.force_wpl ? e.force_wpl : wpl,
+                                                e.force_k ? e.force_k : k, e.force_band, &ch[i]);
+                total_work += ok && e.gens ? ch[i].cost : 0;
+            }
+            if (!ok) continue;
+            const double work_time = total_work / parallel;
+            double chain = 0;
+            for (size_t i = 0; i < b->grids.size(); ++i) {
+                const auto& e = b->grids[i];
+                if (ch[i].crit > GOL_BATCH_REPLAN * work_time && !e.force_band)
+                    golb200::choose_batch_plan(e.W, e.Y, std::max<uint64_t>(e.gens, 1),
+                                               e.force_wpl ? e.force_wpl : wpl,
+                                               e.force_k ? e.force_k : k, e.force_band, &ch[i],
+                                               parallel, 1.0);
+                if (e.gens) chain = std::max(chain, ch[i].crit);
+            }
+            double total2 = 0;
+            for (size_t i = 0; i < b->grids.size(); ++i)
+                if (b->grids[i].gens) total2 += ch[i].cost;
+            const double est = std::max(total2 / parallel, chain);
+            if (best_est < 0 || est < best_est) {
+                best_est = est;
+                best = std::move(ch);
+            }
+        }
     }
-    const double work_time = total_work / parallel;
-    for (auto& e : b->grids) {
-        if (e.choice.crit > GOL_BATCH_REPLAN * work_time &&
-            !(e.force_wpl && e.force_k && e.force_band))
-            golb200::choose_batch_plan(e.W, e.Y, std::max<uint64_t>(e.gens, 1), e.force_wpl, e.force_k,
-                                       e.force_band, &e.choice, parallel, 1.0);
-    }
+    if (best_est < 0) return b->fail(GOL_E_UNSUPPORTED, "no batched plan for a grid");
+    for (size_t i = 0; i < b->grids.size(); ++i) b->grids[i].choice = best[i];
     // A first pass with fewer items than about two per resident warp leaves
     // SMs idle on every pass: halve the tallest bands (not below 16 rows)
     // until it has enough items.
@@ -524,8 +616,8 @@ int gol_batch_upload(gol_batch* b) {
         for (auto& e : b->grids) {
             if (e.gens == 0 || e.force_band || e.choice.band != tallest) continue;
             golb200::GridChoice c2;
-            if (golb200::choose_batch_plan(e.W, e.Y, std::max<uint64_t>(e.gens, 1), e.force_wpl,
-                                           e.force_k, std::max(16, tallest / 2), &c2))
+            if (golb200::choose_batch_plan(e.W, e.Y, std::max<uint64_t>(e.gens, 1), e.choice.wpl,
+                                           e.choice.k, std::max(16, tallest / 2), &c2))
                 e.choice = c2;
         }
     }
@@ -533,9 +625,8 @@ int gol_batch_upload(gol_batch* b) {
         if (e.gens == 0) e.choice.passes = 0;
         // Every buffer starts on a 256-byte boundary: lanes move up to 16
         // bytes at once (uint4 / 16-byte cp.async), whatever the grid sizes.
-        e.stride = ((size_t)e.W * e.Y + 63) / 64 * 64;
         e.offset = words;
-        words += 2 * e.stride;
+        words += ((size_t)e.W * e.Y + 63) / 64 * 64;
         BatchGrid g{};
         golb200::batch_grid_from_choice(e.choice, e.W, e.Y, &g);
         g.parity0 = 0;
@@ -548,8 +639,11 @@ int gol_batch_upload(gol_batch* b) {
     golb200::order_batch_items(hg.data(), hg.size(), items.data());
     b->nitems = (int)items.size();
     b->ngroups_total = groups;
-    b->arena_words = words;
-    ce = cudaMalloc(&b->arena, std::max<size_t>(words, 1) * sizeof(uint32_t));
+    b->wpl_only = golb200::batch_uniform_wpl(hg.data(), hg.size());
+    b->input_words = words;
+    b->arena_words = 3 * words;
+    for (auto& e : b->grids) e.stride = words;
+    ce = cudaMalloc(&b->arena, std::max<size_t>(b->arena_words, 1) * sizeof(uint32_t));
     if (ce == cudaSuccess) ce = cudaMalloc(&b->d_grids, std::max<size_t>(hg.size(), 1) * sizeof(BatchGrid));
     if (ce == cudaSuccess) ce = cudaMalloc(&b->d_items, std::max<size_t>(items.size(), 1) * sizeof(BatchItem));
     if (ce == cudaSuccess) ce = cudaMalloc(&b->d_done, std::max(groups, 1) * sizeof(int));
@@ -569,6 +663,9 @@ int gol_batch_upload(gol_batch* b) {
                              cudaMemcpyHostToDevice, b->stream);
         if (ce != cudaSuccess) break;
     }
+    if (ce == cudaSuccess && words)
+        ce = cudaMemcpyAsync(b->arena + 2 * words, b->arena, words * sizeof(uint32_t),
+                             cudaMemcpyDeviceToDevice, b->stream);
     if (ce == cudaSuccess)
         ce = cudaMemcpyAsync(b->d_grids, hg.data(), hg.size() * sizeof(BatchGrid),
                              cudaMemcpyHostToDevice, b->stream);
@@ -585,37 +682,40 @@ int gol_batch_upload(gol_batch* b) {
     return GOL_OK;
 }
 
-// Resets inputs on the device (buf[0] = uploaded input) without re-planning.
-static int batch_reset_inputs(gol_batch* b) {
-    for (auto& e : b->grids) {
-        cudaError_t ce = cudaMemcpyAsync(b->arena + e.offset, e.words.data(),
-                                         e.words.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
-                                         b->stream);
-        if (ce != cudaSuccess) return b->cuda_fail(ce, "batch input copy");
-    }
-    return GOL_OK;
+// Restores every grid's buf[0] from the device copy of the inputs.
+static cudaError_t batch_restore_inputs(gol_batch* b, cudaStream_t s) {
+    if (!b->input_words) return cudaSuccess;
+    return cudaMemcpyAsync(b->arena, b->arena + 2 * b->input_words,
+                           b->input_words * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
 }
 
-// All grids, all generations: one persistent launch (captured once as a
-// CUDA graph together with the counter resets). Asynchronous; gol_batch_sync
-// waits and reports a timeout recorded by the kernel.
+static int batch_reset_inputs(gol_batch* b) {
+    cudaError_t ce = batch_restore_inputs(b, b->stream);
+    return ce == cudaSuccess ? GOL_OK : b->cuda_fail(ce, "batch input restore");
+}
+
+// All grids, all generations: one persistent launch, captured once as a
+// CUDA graph together with the input restore (device-to-device) and the
+// counter resets. Asynchronous; gol_batch_sync waits and reports a timeout
+// recorded by the kernel.
 int gol_batch_run(gol_batch* b) {
     if (!b) return GOL_E_INVALID;
     int rc;
     if (!b->uploaded && (rc = gol_batch_upload(b))) return rc;
-    if (b->ran && (rc = batch_reset_inputs(b))) return rc;
     if (!b->graph) {
         cudaStream_t cs = nullptr;
         cudaError_t ce = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
         if (ce != cudaSuccess) return b->cuda_fail(ce, "capture stream");
         ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (ce == cudaSuccess) ce = batch_restore_inputs(b, cs);
         if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_done, 0, std::max(b->ngroups_total, 1) * sizeof(int), cs);
         if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_ticket, 0, sizeof(int), cs);
         if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_status, 0, sizeof(int), cs);
         if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_census, 0, 2 * sizeof(unsigned long long), cs);
         if (ce == cudaSuccess)
             ce = golb200::launch_batch_kernel(b->d_grids, b->d_items, b->nitems, b->d_ticket,
-                                              b->d_done, b->d_status, b->num_sms, cs, b->d_census);
+                                              b->d_done, b->d_status, b->num_sms, cs, b->d_census,
+                                              b->wpl_only);
         cudaGraph_t g = nullptr;
         cudaError_t ce2 = cudaStreamEndCapture(cs, &g);
         if (ce == cudaSuccess) ce = ce2;

@@ -113,17 +113,23 @@ bool choose_batch_plan(int W, int Y, uint64_t gens, int force_wpl, int force_k, 
 size_t order_batch_items(const BatchGrid* grids, size_t ngrids, BatchItem* out);
 size_t count_batch_items(const BatchGrid* grids, size_t ngrids);
 
-// Resident one-warp CTAs per SM of the batch kernel.
-int batch_kernel_ctas_per_sm();
+// Resident one-warp CTAs per SM of the batch kernel built for one lane
+// width (1, 2, 4) or for any (0).
+int batch_kernel_ctas_per_sm(int wpl_only = 0);
+
+// The lane width every grid with work shares, or 0 when they differ.
+int batch_uniform_wpl(const BatchGrid* grids, size_t ngrids);
 
 // Fills a descriptor from a plan (buffers, progress base and parity set by the caller).
 void batch_grid_from_choice(const GridChoice& ch, int W, int Y, BatchGrid* g);
 
 // Launches the persistent batch kernel over `nitems` items (pass-major
 // order); done[] and *ticket, *status must be zero. All CTAs fit at once.
+// wpl_only: the lane width all grids share (batch_uniform_wpl), or 0.
 cudaError_t launch_batch_kernel(const BatchGrid* d_grids, const BatchItem* d_items, int nitems,
                                 int* d_ticket, int* d_done, int* d_status, int num_sms,
-                                cudaStream_t stream, unsigned long long* d_census = nullptr);
+                                cudaStream_t stream, unsigned long long* d_census = nullptr,
+                                int wpl_only = 0);
 
 cudaError_t launch_pack_cells(const uint8_t* cells, uint32_t* words, size_t x, size_t y,
                               cudaStream_t stream);

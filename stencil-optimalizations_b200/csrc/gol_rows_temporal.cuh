@@ -86,7 +86,10 @@ __device__ __forceinline__ void store_words(uint32_t* p, const uint32_t (&v)[WPL
 // and later reads back only its own words, so a per-thread
 // cp.async.wait_group (a hardware wait, no spin) orders the two. Rows and
 // lanes outside the grid are zero-filled by the copy itself (src-size 0).
-constexpr int kRowRing = 6;
+#ifndef GOL_ROW_RING
+#define GOL_ROW_RING 6
+#endif
+constexpr int kRowRing = GOL_ROW_RING;
 constexpr int kRowsInFlight = kRowRing - 1;
 
 template <int WPL>

@@ -238,6 +238,14 @@ int gol_serve_create(gol_server** out, int32_t device, uint64_t arena_bytes, uin
     return GOL_OK;
 }
 
+// Every request runs 2 words per lane (1 for an odd word count) at depth
+// 4 with its own band height, so a round's launch holds one pipeline family
+// (mixed families on one SM compete for the instruction cache).
+static bool plan_request(Request& r, uint64_t generations) {
+    return golb200::choose_batch_plan(r.W, r.Y, std::max<uint64_t>(generations, 1), r.W % 2 ? 1 : 2,
+                                      golb200::kBatchMaxK, 0, &r.plan);
+}
+
 int gol_serve_submit(gol_server* s, const uint8_t* cells, uint64_t x, uint64_t y,
                      uint64_t generations, uint64_t* id) {
     if (!s) return GOL_E_INVALID;
@@ -252,8 +260,7 @@ int gol_serve_submit(gol_server* s, const uint8_t* cells, uint64_t x, uint64_t y
     r.gens = generations;
     r.stride = ((size_t)r.W * r.Y + 63) / 64 * 64;
     if (2 * r.stride > s->arena_words) return s->fail(GOL_E_NOMEM, "request larger than the device arena");
-    if (!golb200::choose_batch_plan(r.W, r.Y, std::max<uint64_t>(generations, 1), 0, 0, 0, &r.plan))
-        return s->fail(GOL_E_UNSUPPORTED, "no plan for this request");
+    if (!plan_request(r, generations)) return s->fail(GOL_E_UNSUPPORTED, "no plan for this request");
     r.words.resize((size_t)r.W * r.Y);
     golb200::host_pack_u8(cells, x, y, r.words.data());
     if (id) *id = r.id;
@@ -282,8 +289,7 @@ int gol_serve_submit_random(gol_server* s, uint64_t x, uint64_t y, uint64_t gene
     r.input_density = density;
     r.stride = ((size_t)r.W * r.Y + 63) / 64 * 64;
     if (2 * r.stride > s->arena_words) return s->fail(GOL_E_NOMEM, "request larger than the device arena");
-    if (!golb200::choose_batch_plan(r.W, r.Y, std::max<uint64_t>(generations, 1), 0, 0, 0, &r.plan))
-        return s->fail(GOL_E_UNSUPPORTED, "no plan for this request");
+    if (!plan_request(r, generations)) return s->fail(GOL_E_UNSUPPORTED, "no plan for this request");
     if (id) *id = r.id;
     s->queue.push_back(r.id);
     s->reqs.emplace(r.id, std::move(r));
@@ -383,7 +389,8 @@ int gol_serve_step(gol_server* s) {
     if (ce == cudaSuccess) ce = cudaMemsetAsync(rb.d_status, 0, sizeof(int), s->stream);
     if (ce == cudaSuccess)
         ce = golb200::launch_batch_kernel(rb.d_grids, rb.d_items, (int)nitems, rb.d_ticket, rb.d_done,
-                                          rb.d_status, s->num_sms, s->stream);
+                                          rb.d_status, s->num_sms, s->stream, nullptr,
+                                          golb200::batch_uniform_wpl(grids.data(), grids.size()));
     if (ce == cudaSuccess)
         ce = cudaMemcpyAsync(rb.h_status, rb.d_status, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
     if (ce == cudaSuccess) ce = cudaEventRecord(rb.done_event, s->stream);
