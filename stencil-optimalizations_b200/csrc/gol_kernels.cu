@@ -10,11 +10,24 @@ namespace golb200 {
 
 namespace {
 
+// Launched as a programmatic dependent of the previous kernel in the
+// stream: its CTAs may be scheduled while that kernel drains and wait in
+// griddepcontrol.wait (full completion and memory flush of the previous
+// grid) before touching global memory, which hides the launch gap between
+// consecutive passes.
 template <int WPL, int K>
 cudaError_t launch_one(const RowsLaunch& a, const RowsPlan& p, cudaStream_t stream) {
-    const size_t smem = temporal_smem_bytes(K, p.threads, WPL);
-    rows_temporal_kernel<WPL, K><<<dim3(p.nbands, p.nslices), p.threads, smem, stream>>>(a);
-    return cudaPeekAtLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(p.nbands, p.nslices);
+    cfg.blockDim = dim3(p.threads);
+    cfg.dynamicSmemBytes = temporal_smem_bytes(K, p.threads, WPL);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, rows_temporal_kernel<WPL, K>, a);
 }
 
 template <int WPL, int K>

@@ -359,10 +359,20 @@ __device__ __forceinline__ uint32_t band_tile(const RowsLaunch& a, int band, int
     return s.diff;
 }
 
+// Programmatic dependent launch: let the next pass's CTAs be scheduled
+// now (they wait below for this grid to finish), then wait for the
+// previous pass to complete before the first global access. Both are
+// no-ops for an ordinary launch.
+__device__ __forceinline__ void pdl_trigger_and_wait() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 template <int WPL, int K>
 __global__ void __launch_bounds__(kTemporalMaxThreads, GOL_TEMPORAL_MIN_BLOCKS)
 rows_temporal_kernel(RowsLaunch a) {
     extern __shared__ __align__(16) uint32_t smem[];
+    pdl_trigger_and_wait();
     band_tile<WPL, K, false>(a, blockIdx.x, blockIdx.y, smem);
 }
 
