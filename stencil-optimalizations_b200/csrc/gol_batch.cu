@@ -80,6 +80,7 @@ __device__ __forceinline__ void seg_group(const BatchGrid& G, int group, int sli
     c.src = src;
     c.dst = dst;
     c.W = G.W;
+    c.pitch = G.pitch;
     c.Y = G.Y;
     c.B = G.band;
     c.y0 = (group * G.segs + seg) * G.band;
@@ -97,7 +98,7 @@ __device__ __forceinline__ void seg_group(const BatchGrid& G, int group, int sli
     c.ring = ring + lane * WPL;
     c.ring_saddr = (uint32_t)__cvta_generic_to_shared(c.ring);
     c.ring_stride = 32 * WPL;
-    const uint32_t lane_mask = c.lane_ok ? 0xffffffffu : 0u;
+    set_word_masks<WPL>(c);
 
     TemporalRegs<WPL, K> s;
 #pragma unroll
@@ -125,11 +126,11 @@ __device__ __forceinline__ void seg_group(const BatchGrid& G, int group, int sli
     const int f1 = min(G.band + 2 * K - 1, G.Y - y0_last + K - 1);
     const int fast_end = f1 > f0 ? f0 + (f1 - f0) / 3 * 3 : f0;
     if (fast_end > f0) {
-        temporal_steps<WPL, K, false, false, false, true>(s, c, 0, f0, lane_mask);
-        temporal_steps<WPL, K, true, true, false, true>(s, c, f0, fast_end, lane_mask);
-        temporal_steps<WPL, K, false, false, false, true>(s, c, fast_end, nsteps, lane_mask);
+        temporal_steps<WPL, K, false, false, false, true>(s, c, 0, f0);
+        temporal_steps<WPL, K, true, true, false, true>(s, c, f0, fast_end);
+        temporal_steps<WPL, K, false, false, false, true>(s, c, fast_end, nsteps);
     } else {
-        temporal_steps<WPL, K, false, false, false, true>(s, c, 0, nsteps, lane_mask);
+        temporal_steps<WPL, K, false, false, false, true>(s, c, 0, nsteps);
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
@@ -199,8 +200,11 @@ batch_kernel(const BatchGrid* __restrict__ grids, const BatchItem* __restrict__ 
         if (lane == 0) next = atomicAdd(ticket, 1);
         const long long t_work = clock64();
         const int k = it.pass == G.passes - 1 ? G.last_k : G.k;
-        const uint32_t* src = G.buf[(G.parity0 + it.pass) & 1];
-        uint32_t* dst = G.buf[(G.parity0 + it.pass + 1) & 1];
+        // Selects, not an index: a dynamically indexed descriptor would be
+        // kept in local memory for the whole item.
+        const bool odd = (G.parity0 + it.pass) & 1;
+        const uint32_t* src = odd ? G.buf[1] : G.buf[0];
+        uint32_t* dst = odd ? G.buf[0] : G.buf[1];
         if constexpr (WPL_ONLY != 0) {
             seg_dispatch<WPL_ONLY>(k, G, it.group, it.slice, src, dst, ring);
         } else {
@@ -245,13 +249,18 @@ batch_kernel(const BatchGrid* __restrict__ grids, const BatchItem* __restrict__ 
 // first choice minimises work alone; grids whose chain would outlast the
 // batch's work-bound time are then re-planned to minimise work / resident
 // warps + chain (shorter bands: more, quicker items per pass). Candidates:
-// WPL in {1, 2, 4} (W % WPL == 0), k in 1..4, band in {16, 24, 32, 48, 64}
+// WPL in {1, 2, 4} (rows padded to whole lanes), k in 1..4, band in
+// {16, 24, 32, 48} (taller bands measured slower: fewer items per pass
+// leave warps waiting on the previous pass)
 // with band >= 2k. gol_batch_upload runs this for every (WPL, k) the whole
 // batch can use and keeps the pair with the smallest estimated time.
 // ---------------------------------------------------------------------------
 
 struct BatchTuning {
-    double cw[5] = {0, 1.45, 1.15, 0, 1.0};   // relative cost per word-stage-step by WPL
+    // relative cost per word-stage-step by WPL, measured on uniform batches
+    // with every lane busy (per-variant kernels: 21, 15 and 9 resident warps
+    // per SM for 1, 2 and 4 words per lane)
+    double cw[5] = {0, 1.13, 0.81, 0, 1.0};
     double c_row = 0.6;                        // per row per pass (load + store)
     double c_item = 120.0;                     // per item (start-up, dependency wait, release)
 };
@@ -263,14 +272,16 @@ bool choose_batch_plan(int W, int Y, uint64_t gens, int force_wpl, int force_k, 
     bool found = false;
     for (int wpl : {1, 2, 4}) {
         if (force_wpl && wpl != force_wpl) continue;
-        if (W % wpl) continue;
-        const bool sliced = W / wpl > 32;
-        const int L = sliced ? 32 : W / wpl;
+        // A row of W words takes ceil(W / wpl) lanes; rows are padded to a
+        // whole number of lanes (the padding words stay zero).
+        const int lanes = (W + wpl - 1) / wpl;
+        const bool sliced = lanes > 32;
+        const int L = sliced ? 32 : lanes;
         const int slice = sliced ? 30 * wpl : W;
         const int nslices = (W + slice - 1) / slice;
         for (int k = 1; k <= kBatchMaxK; ++k) {
             if (force_k && k != force_k) continue;
-            for (int band : {16, 24, 32, 48, 64}) {
+            for (int band : {16, 24, 32, 48}) {
                 if (force_band) band = force_band;
                 if (band < 2 * k && !force_band) continue;
                 const int S = sliced ? 1 : std::max(1, std::min(32 / L, (Y + band - 1) / band));
@@ -359,6 +370,7 @@ int batch_uniform_wpl(const BatchGrid* grids, size_t ngrids) {
 void batch_grid_from_choice(const GridChoice& ch, int W, int Y, BatchGrid* g) {
     g->W = W;
     g->Y = Y;
+    g->pitch = (W + ch.wpl - 1) / ch.wpl * ch.wpl;
     g->wpl = ch.wpl;
     g->k = ch.k;
     g->last_k = ch.last_k;
@@ -421,6 +433,7 @@ struct gol_batch {
         golb200::GridChoice choice{};
         int force_wpl = 0, force_k = 0, force_band = 0;
         size_t offset = 0;                // word offset of buf[0] in the arena
+        int pitch = 0;                    // words per row on the device (W padded to wpl)
         size_t stride = 0;                // words from buf[0] to buf[1] (the input region's size)
         int result_buf = 0;               // buffer holding the last run's result
     };
@@ -562,10 +575,14 @@ int gol_batch_upload(gol_batch* b) {
     // work-bound time of the whole batch take shorter chains; the pair with
     // the smallest max(work / resident warps, longest chain) wins. Grids with
     // a plan forced by gol_batch_set_plan keep it.
-    const double parallel = (double)b->num_sms * golb200::batch_kernel_ctas_per_sm(0);
-    double best_est = -1;
+    // Units: a work item's cost is warp time at the variant's occupancy
+    // (per-word costs are calibrated on whole batches), so a batch needs
+    // about max(total / num_sms, longest chain * warps per SM) SM time.
+    double best_est = -1, parallel = 1;
     std::vector<golb200::GridChoice> best;
     for (int wpl : {4, 2, 1}) {
+        const double wps = golb200::batch_kernel_ctas_per_sm(wpl);
+        const double par = (double)b->num_sms * wps;
         for (int k = golb200::kBatchMaxK; k >= 1; --k) {
             std::vector<golb200::GridChoice> ch(b->grids.size());
             double total_work = 0;
@@ -578,7 +595,7 @@ int gol_batch_upload(gol_batch* b) {
                 total_work += ok && e.gens ? ch[i].cost : 0;
             }
             if (!ok) continue;
-            const double work_time = total_work / parallel;
+            const double work_time = total_work / par;
             double chain = 0;
             for (size_t i = 0; i < b->grids.size(); ++i) {
                 const auto& e = b->grids[i];
@@ -586,15 +603,16 @@ int gol_batch_upload(gol_batch* b) {
                     golb200::choose_batch_plan(e.W, e.Y, std::max<uint64_t>(e.gens, 1),
                                                e.force_wpl ? e.force_wpl : wpl,
                                                e.force_k ? e.force_k : k, e.force_band, &ch[i],
-                                               parallel, 1.0);
+                                               par, 1.0);
                 if (e.gens) chain = std::max(chain, ch[i].crit);
             }
             double total2 = 0;
             for (size_t i = 0; i < b->grids.size(); ++i)
                 if (b->grids[i].gens) total2 += ch[i].cost;
-            const double est = std::max(total2 / parallel, chain);
+            const double est = wps * std::max(total2 / par, chain);
             if (best_est < 0 || est < best_est) {
                 best_est = est;
+                parallel = par;
                 best = std::move(ch);
             }
         }
@@ -625,10 +643,11 @@ int gol_batch_upload(gol_batch* b) {
         if (e.gens == 0) e.choice.passes = 0;
         // Every buffer starts on a 256-byte boundary: lanes move up to 16
         // bytes at once (uint4 / 16-byte cp.async), whatever the grid sizes.
-        e.offset = words;
-        words += ((size_t)e.W * e.Y + 63) / 64 * 64;
         BatchGrid g{};
         golb200::batch_grid_from_choice(e.choice, e.W, e.Y, &g);
+        e.pitch = g.pitch;
+        e.offset = words;
+        words += ((size_t)g.pitch * e.Y + 63) / 64 * 64;
         g.parity0 = 0;
         g.done_base = groups;
         groups += g.ngroups * g.nslices;
@@ -655,13 +674,16 @@ int gol_batch_upload(gol_batch* b) {
         return ce == cudaErrorMemoryAllocation ? b->fail(GOL_E_NOMEM, "device allocation failed")
                                                : b->cuda_fail(ce, "cudaMalloc");
     }
-    for (size_t gi = 0; gi < hg.size(); ++gi) {
+    // Padding words past W must read as dead: the arena starts zeroed.
+    ce = cudaMemsetAsync(b->arena, 0, std::max<size_t>(b->arena_words, 1) * sizeof(uint32_t), b->stream);
+    for (size_t gi = 0; gi < hg.size() && ce == cudaSuccess; ++gi) {
         auto& e = b->grids[gi];
         hg[gi].buf[0] = b->arena + e.offset;
         hg[gi].buf[1] = b->arena + e.offset + e.stride;
-        ce = cudaMemcpyAsync(hg[gi].buf[0], e.words.data(), e.words.size() * sizeof(uint32_t),
-                             cudaMemcpyHostToDevice, b->stream);
-        if (ce != cudaSuccess) break;
+        if (e.W == 0 || e.Y == 0) continue;
+        ce = cudaMemcpy2DAsync(hg[gi].buf[0], (size_t)e.pitch * sizeof(uint32_t), e.words.data(),
+                               (size_t)e.W * sizeof(uint32_t), (size_t)e.W * sizeof(uint32_t), e.Y,
+                               cudaMemcpyHostToDevice, b->stream);
     }
     if (ce == cudaSuccess && words)
         ce = cudaMemcpyAsync(b->arena + 2 * words, b->arena, words * sizeof(uint32_t),
@@ -762,7 +784,8 @@ int gol_batch_run_plain(gol_batch* b, uint32_t temporal_steps) {
             golb200::RowsPlan p;
             if (!golb200::plan_rows(e.W, e.Y, k, 0, 0, b->num_sms, &p))
                 return b->fail(GOL_E_UNSUPPORTED, "no plan");
-            cudaError_t ce = golb200::launch_rows_pass(buf[cur], buf[cur ^ 1], e.W, e.Y, k, p, b->stream);
+            cudaError_t ce = golb200::launch_rows_pass(buf[cur], buf[cur ^ 1], e.W, e.Y, k, p,
+                                                       b->stream, e.pitch);
             if (ce != cudaSuccess) return b->cuda_fail(ce, "plain launch");
             cur ^= 1;
             left -= k;
@@ -779,9 +802,12 @@ int gol_batch_fetch(gol_batch* b, int32_t grid_id, uint8_t* cells) {
     auto& e = b->grids[grid_id];
     const int which = e.result_buf;
     std::vector<uint32_t> words((size_t)e.W * e.Y);
-    cudaError_t ce = cudaMemcpyAsync(words.data(), b->arena + e.offset + (size_t)which * e.stride,
-                                     words.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                                     b->stream);
+    cudaError_t ce = cudaSuccess;
+    if (!words.empty())
+        ce = cudaMemcpy2DAsync(words.data(), (size_t)e.W * sizeof(uint32_t),
+                               b->arena + e.offset + (size_t)which * e.stride,
+                               (size_t)e.pitch * sizeof(uint32_t), (size_t)e.W * sizeof(uint32_t),
+                               e.Y, cudaMemcpyDeviceToHost, b->stream);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(b->stream);
     if (ce != cudaSuccess) return b->cuda_fail(ce, "batch fetch");
     golb200::host_unpack_u8(words.data(), e.x, e.y, cells);

@@ -29,9 +29,10 @@ struct RowsPlan {
 // it. Returns false for k outside 1..16 or a wpl that W or k rules out.
 bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPlan* plan);
 
-// One pass of k generations (1 <= k <= kMaxKForWpl(plan.wpl)).
+// One pass of k generations (1 <= k <= kMaxKForWpl(plan.wpl)). pitch: words
+// from one row to the next (0 = W).
 cudaError_t launch_rows_pass(const uint32_t* src, uint32_t* dst, int W, int Y, int k,
-                             const RowsPlan& plan, cudaStream_t stream);
+                             const RowsPlan& plan, cudaStream_t stream, int pitch = 0);
 
 // Change-tracking tiles (GOL_ALG_LOCAL): tile = x-slice x row band.
 struct LocalPlan {
@@ -74,6 +75,7 @@ cudaError_t launch_local_pass(const uint32_t* src, uint32_t* dst, int W, int Y, 
 struct BatchGrid {
     uint32_t* buf[2];      // ping-pong device grids (W words per row)
     int W, Y;              // words per row, rows
+    int pitch;             // words from one row to the next: W rounded up to wpl
     int wpl;               // words per lane
     int k;                 // depth of full passes
     int last_k;            // depth of the final pass

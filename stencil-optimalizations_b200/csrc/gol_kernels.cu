@@ -93,9 +93,9 @@ bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPla
 }
 
 cudaError_t launch_rows_pass(const uint32_t* src, uint32_t* dst, int W, int Y, int k,
-                             const RowsPlan& p, cudaStream_t stream) {
+                             const RowsPlan& p, cudaStream_t stream, int pitch) {
     if (Y <= 0 || W <= 0) return cudaSuccess;
-    RowsLaunch a{src, dst, W, Y, p.band, p.slice, p.halo};
+    RowsLaunch a{src, dst, W, Y, p.band, p.slice, p.halo, pitch ? pitch : W};
     switch (p.wpl) {
         case 4: return dispatch_k<4, 1>(k, a, p, stream);
         case 2: return dispatch_k<2, 1>(k, a, p, stream);

@@ -111,6 +111,7 @@ seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
         c.src = a.src;
         c.dst = a.dst;
         c.W = a.W;
+        c.pitch = a.pitch;
         c.Y = a.Y;
         c.B = a.band;
         c.y0 = ty * a.band;
@@ -128,7 +129,7 @@ seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
         c.ring = ring + lane * WPL;
         c.ring_saddr = (uint32_t)__cvta_generic_to_shared(c.ring);
         c.ring_stride = 32 * WPL;
-        const uint32_t lane_mask = c.lane_ok ? 0xffffffffu : 0u;
+        set_word_masks<WPL>(c);
 
         TemporalRegs<WPL, K> s;
 #pragma unroll
@@ -155,11 +156,11 @@ seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
         const int f1 = min(c.B + 2 * K - 1, c.Y - y0_deep + K - 1);
         const int fast_end = f1 > f0 ? f0 + (f1 - f0) / 3 * 3 : f0;
         if (fast_end > f0) {
-            temporal_steps<WPL, K, false, false, true, true>(s, c, 0, f0, lane_mask);
-            temporal_steps<WPL, K, true, true, true, true>(s, c, f0, fast_end, lane_mask);
-            temporal_steps<WPL, K, false, false, true, true>(s, c, fast_end, nsteps, lane_mask);
+            temporal_steps<WPL, K, false, false, true, true>(s, c, 0, f0);
+            temporal_steps<WPL, K, true, true, true, true>(s, c, f0, fast_end);
+            temporal_steps<WPL, K, false, false, true, true>(s, c, fast_end, nsteps);
         } else {
-            temporal_steps<WPL, K, false, false, true, true>(s, c, 0, nsteps, lane_mask);
+            temporal_steps<WPL, K, false, false, true, true>(s, c, 0, nsteps);
         }
         asm volatile("cp.async.wait_all;\n" ::: "memory");
         const unsigned any = __ballot_sync(0xffffffffu, s.diff != 0u);
@@ -230,7 +231,7 @@ cudaError_t launch_local_pass(const uint32_t* src, uint32_t* dst, int W, int Y, 
         parity, st.census, st.census_cap, st.pass_no);
     cudaError_t e = cudaPeekAtLastError();
     if (e != cudaSuccess) return e;
-    RowsLaunch a{src, dst, W, Y, p.band, p.slice, p.halo};
+    RowsLaunch a{src, dst, W, Y, p.band, p.slice, p.halo, W};
     TileList t{st.list, st.count + parity, st.changed[parity], lp.tiles_x};
     switch (p.wpl) {
         case 4: return dispatch_tiles<4, 1>(k, a, t, lp, stream);

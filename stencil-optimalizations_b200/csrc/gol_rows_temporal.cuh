@@ -55,6 +55,7 @@ struct RowsLaunch {
     int band;              // output rows per CTA (blockIdx.x)
     int slice;             // words per x-slice (blockIdx.y); W when unsliced
     int halo;              // words of x-halo each side of a slice (0 or WPL)
+    int pitch;             // words from one row to the next (>= W)
 };
 
 template <int WPL>
@@ -155,11 +156,22 @@ struct TemporalCtx {
     uint32_t ring_saddr;   // same, as a shared-window address for cp.async
     int ring_stride;       // words per ring slot (blockDim.x * WPL)
     int W, Y, y0, y1, B;
+    int pitch;      // words from one row to the next: W, or W rounded up to WPL
+                    // (then the words past W are zero and stay zero)
     int lane, base;
-    bool lane_ok;   // this lane's words lie inside the grid
+    bool lane_ok;   // this lane's first word lies inside the grid
     bool own;       // ... and inside this CTA's slice (not halo): stored
     int src_l, src_r;   // segmented warps: lanes holding the words left / right
+    uint32_t wmask[4];  // per word of the lane: all ones inside the grid, else 0
 };
+
+// Word masks of a lane whose words start at `base` in a W-word row.
+template <int WPL>
+__device__ __forceinline__ void set_word_masks(TemporalCtx& c) {
+#pragma unroll
+    for (int w = 0; w < 4; ++w)
+        c.wmask[w] = (w < WPL && c.lane_ok && c.base + w < c.W) ? 0xffffffffu : 0u;
+}
 
 // Copies the row stage 0 consumes at step j (grid row y0 - K + j) into ring
 // slot `slot`, zero-filled outside the grid; commits it as one group.
@@ -167,7 +179,7 @@ template <int WPL, int K>
 __device__ __forceinline__ void issue_row(const TemporalCtx& c, int j, int slot) {
     const int r = c.y0 - K + j;
     const bool v = c.lane_ok && (unsigned)r < (unsigned)c.Y;
-    const uint32_t* g = v ? c.src + (size_t)r * c.W + c.base : c.src;
+    const uint32_t* g = v ? c.src + (size_t)r * c.pitch + c.base : c.src;
     cp_async_words<WPL>(c.ring_saddr + (uint32_t)(slot * c.ring_stride) * 4u, g, v);
     cp_async_commit();
 }
@@ -175,14 +187,14 @@ __device__ __forceinline__ void issue_row(const TemporalCtx& c, int j, int slot)
 // Step body. FAST = steady state: every stage active, every row inside the
 // grid, so no activity tests or row masks (the whole step is one basic
 // block and the K stages' independent chains interleave). LMASK forces the
-// out-of-grid lanes of a partial CTA to stay dead. SEG = segmented warp: the
+// out-of-grid words of a partial CTA (whole lanes, or the tail of the last
+// lane of a padded row) to stay dead. SEG = segmented warp: the
 // CTA is one warp cut into segments that each span a whole (narrow) grid
 // row for their own band; neighbours come from explicit shuffle source
 // lanes, segment ends see dead cells, and no shared-memory edge table or
 // barrier is needed (y0/y1 are then per lane, B the common band height).
 template <int WPL, int K, int PH, bool FAST, bool LMASK, bool TRACK, bool SEG = false>
-__device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const TemporalCtx& c, int i,
-                                              uint32_t lane_mask) {
+__device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const TemporalCtx& c, int i) {
     constexpr int NEW3 = PH % 3;          // ring-of-3 slot written at this step
     constexpr int PREV3 = (PH + 2) % 3;   // ... written one step ago
     constexpr int OLD3 = (PH + 1) % 3;    // ... written two steps ago
@@ -226,22 +238,21 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
             }
             // Output row r of gen g (garbage during warm-up, never consumed).
             const int row = c.y0 - K + i - 2 * g;
-            uint32_t keep = lane_mask;
-            if (!FAST) keep = (c.lane_ok && (unsigned)row < (unsigned)c.Y) ? 0xffffffffu : 0u;
+            const bool row_ok = FAST || (unsigned)row < (unsigned)c.Y;
             uint32_t res[WPL];
 #pragma unroll
             for (int w = 0; w < WPL; ++w) {
                 res[w] = next_word(s.h0[g - 1][OLD3][w], s.h1[g - 1][OLD3][w],
                                    s.h0[g - 1][PREV3][w], s.h1[g - 1][PREV3][w],
                                    s.h0[g - 1][NEW3][w], s.h1[g - 1][NEW3][w], C[w]);
-                if (!FAST || LMASK) res[w] &= keep;
+                if (!FAST || LMASK) res[w] &= row_ok ? c.wmask[w] : 0u;
             }
             if (g == K) {
                 if ((FAST || (row >= c.y0 && row < c.y1)) && c.own) {
-                    store_words<WPL>(c.dst + (size_t)row * c.W + c.base, res);
+                    store_words<WPL>(c.dst + (size_t)row * c.pitch + c.base, res);
                     if (TRACK) {   // compare with the same row before the pass
                         uint32_t old[WPL];
-                        load_words<WPL>(c.src + (size_t)row * c.W + c.base, old);
+                        load_words<WPL>(c.src + (size_t)row * c.pitch + c.base, old);
 #pragma unroll
                         for (int w = 0; w < WPL; ++w) s.diff |= res[w] ^ old[w];
                     }
@@ -270,11 +281,11 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
 
 template <int WPL, int K, bool FAST, bool LMASK, bool TRACK, bool SEG = false>
 __device__ __forceinline__ void temporal_steps(TemporalRegs<WPL, K>& s, const TemporalCtx& c,
-                                               int i0, int i1, uint32_t lane_mask) {
+                                               int i0, int i1) {
     for (int i = i0; i < i1; i += 3) {
-        temporal_step<WPL, K, 0, FAST, LMASK, TRACK, SEG>(s, c, i + 0, lane_mask);
-        temporal_step<WPL, K, 1, FAST, LMASK, TRACK, SEG>(s, c, i + 1, lane_mask);
-        temporal_step<WPL, K, 2, FAST, LMASK, TRACK, SEG>(s, c, i + 2, lane_mask);
+        temporal_step<WPL, K, 0, FAST, LMASK, TRACK, SEG>(s, c, i + 0);
+        temporal_step<WPL, K, 1, FAST, LMASK, TRACK, SEG>(s, c, i + 1);
+        temporal_step<WPL, K, 2, FAST, LMASK, TRACK, SEG>(s, c, i + 2);
     }
 }
 
@@ -293,6 +304,7 @@ __device__ __forceinline__ uint32_t band_tile(const RowsLaunch& a, int band, int
     c.src = a.src;
     c.dst = a.dst;
     c.W = a.W;
+    c.pitch = a.pitch;
     c.Y = a.Y;
     c.y0 = band * a.band;
     c.y1 = min(c.y0 + a.band, a.Y);
@@ -312,7 +324,7 @@ __device__ __forceinline__ uint32_t band_tile(const RowsLaunch& a, int band, int
     c.lane_ok = c.base >= 0 && c.base < a.W;
     c.own = c.lane_ok && c.base >= xs && c.base < xs + a.slice;
     const bool all_lanes_ok = x0 >= 0 && x0 + (int)blockDim.x * WPL <= a.W;
-    const uint32_t lane_mask = c.lane_ok ? 0xffffffffu : 0u;
+    set_word_masks<WPL>(c);
 
     for (int t = threadIdx.x; t < EW * ESTRIDE; t += blockDim.x) edges[t] = 0u;
 
@@ -346,14 +358,14 @@ __device__ __forceinline__ uint32_t band_tile(const RowsLaunch& a, int band, int
     const int f1 = min(c.B + 2 * K - 1, c.Y - c.y0 + K - 1);
     const int fast_end = f1 > f0 ? f0 + (f1 - f0) / 3 * 3 : f0;
     if (fast_end > f0) {
-        temporal_steps<WPL, K, false, false, TRACK>(s, c, 0, f0, lane_mask);
+        temporal_steps<WPL, K, false, false, TRACK>(s, c, 0, f0);
         if (all_lanes_ok)
-            temporal_steps<WPL, K, true, false, TRACK>(s, c, f0, fast_end, lane_mask);
+            temporal_steps<WPL, K, true, false, TRACK>(s, c, f0, fast_end);
         else
-            temporal_steps<WPL, K, true, true, TRACK>(s, c, f0, fast_end, lane_mask);
-        temporal_steps<WPL, K, false, false, TRACK>(s, c, fast_end, nsteps, lane_mask);
+            temporal_steps<WPL, K, true, true, TRACK>(s, c, f0, fast_end);
+        temporal_steps<WPL, K, false, false, TRACK>(s, c, fast_end, nsteps);
     } else {
-        temporal_steps<WPL, K, false, false, TRACK>(s, c, 0, nsteps, lane_mask);
+        temporal_steps<WPL, K, false, false, TRACK>(s, c, 0, nsteps);
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");   // no copy outlives the tile
     return s.diff;

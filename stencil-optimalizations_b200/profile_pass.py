@@ -1,12 +1,19 @@
-"""Runs a few k-generation passes of the row-band kernel on one grid, for
+"""Runs one of the engine's kernels on a small, fixed workload, for
 profiling (ncu) and quick timing.
 
     python stencil-optimalizations_b200/profile_pass.py --size 16384 --k 5 --passes 8
+    python stencil-optimalizations_b200/profile_pass.py --mode local --size 4096 --gens 400
+    python stencil-optimalizations_b200/profile_pass.py --mode batch --grids 32
 
-The grid is the dense benchmark input (Bernoulli(0.5), seed 42, from the
-reference's RandomOnesZerosDataLoader). Each pass reads one device buffer
-and writes the other through gol_rows_pass; the script prints the mean
-per-launch time measured with CUDA events.
+dense (default): k-generation passes of the row-band kernel on the dense
+benchmark input (Bernoulli(0.5), seed 42, from the reference's
+RandomOnesZerosDataLoader); each pass reads one device buffer and writes the
+other through gol_rows_pass; prints the mean per-launch time (CUDA events).
+local: the change-tracking engine on the sparse input (1 % of 64x64 slots
+Bernoulli(0.35), seed 42), --gens generations; prints the run time and the
+fraction of tiles computed.
+batch: the first --grids grids of the uneven batched workload (seed 42), one
+persistent launch after a warm-up launch; prints the launch time.
 """
 from __future__ import annotations
 
@@ -28,7 +35,14 @@ def main() -> None:
     ap.add_argument("--passes", type=int, default=8)
     ap.add_argument("--band", type=int, default=0)
     ap.add_argument("--wpl", type=int, default=0)
+    ap.add_argument("--mode", choices=["dense", "local", "batch"], default="dense")
+    ap.add_argument("--gens", type=int, default=400)
+    ap.add_argument("--grids", type=int, default=32)
     a = ap.parse_args()
+    if a.mode == "local":
+        return run_local(a)
+    if a.mode == "batch":
+        return run_batch(a)
 
     import torch
     x, y = a.size, a.height or a.size
@@ -53,6 +67,49 @@ def main() -> None:
     print(f"{x}x{y} k={a.k} wpl={a.wpl or 'auto'} band={a.band or 'auto'}: "
           f"{mean * 1e3:.1f} us per pass, "
           f"{x * y * a.k / (mean * 1e-3) / 1e12:.2f} Tcell-updates/s")
+
+
+def run_local(a) -> None:
+    import time
+    x, y = a.size, a.height or a.size
+    g = golb200.load_sparse_patches(x, y, seed=42)
+    with golb200.GolB200(grid_dimensions=(x, y), temporal_steps=a.k if a.k <= 16 else 8,
+                         algorithm="local") as alg:
+        alg.set_and_format_input_data(g)
+        alg.initialize_data_structures()
+        t0 = time.perf_counter()
+        alg.run(a.gens)
+        alg.sync()
+        dt = time.perf_counter() - t0
+        st = alg.local_stats()
+        alg.finalize_data_structures()
+    frac = st["computed_tiles"] / max(1, st["passes"] * st["tiles_per_pass"])
+    print(f"local {x}x{y}, {a.gens} generations, k={a.k}: {dt * 1e3:.2f} ms (wall), "
+          f"{frac:.3f} of tile-passes computed")
+
+
+def run_batch(a) -> None:
+    import torch
+    work = golb200.workload_uneven(42, 512, 256, 4096, 64, (0.2, 0.5), (64, 4096))[:a.grids]
+    s = torch.cuda.Stream()
+    b = golb200.GolBatch(stream=s.cuda_stream)
+    cu = 0
+    for d in work:
+        b.add(golb200.load_bernoulli(d["x"], d["y"], d["cell_seed"], d["density"]), d["gens"])
+        cu += d["x"] * d["y"] * d["gens"]
+    b.upload()
+    b.run()
+    b.sync()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    b.run()
+    e1.record(s)
+    b.sync()
+    ms = e0.elapsed_time(e1)
+    print(f"batch of {len(work)} grids, {b.info()['items']} items: {ms:.2f} ms, "
+          f"{cu / (ms * 1e-3) / 1e12:.2f} Tcell-updates/s")
+    b.close()
 
 
 if __name__ == "__main__":

@@ -33,9 +33,7 @@ def test_batch_forced_plans(wpl, k, band):
     work = small_workload(2 + wpl * 10 + k, 12, lo=128, hi=768, gens=(1, 97))
     with golb200.GolBatch() as b:
         ids = []
-        for c, n in work:
-            if c.shape[1] // 32 % wpl:
-                continue
+        for c, n in work:                # rows padded to whole lanes where W % wpl != 0
             gid = b.add(c, n)
             b.set_plan(gid, wpl, k, band)
             ids.append((gid, c, n))
@@ -58,6 +56,32 @@ def test_batch_wide_sliced_and_tiny_grids():
         b.sync()
         for gid, (c, n) in zip(ids, work):
             assert np.array_equal(b.fetch(gid), oracle.life_cells(c, n)), (c.shape, n)
+
+
+@pytest.mark.parametrize("wpl", [4, 2])
+def test_batch_padded_rows(wpl):
+    """Word counts that are not a multiple of the lane width: rows are padded
+    on the device and the padding stays dead (narrow, single-lane-tail and
+    x-sliced widths)."""
+    shapes = [(96, 50, 33), (160, 17, 20), (32 * 7, 64, 41), (32 * 130, 30, 12),
+              (32 * 131, 21, 9), (32 * 66, 40, 25), (32 * 127, 33, 17), (32 * 250, 12, 7)]
+    work = [(oracle.random_ones_zeros(x, y, x + y), n) for x, y, n in shapes]
+    with golb200.GolBatch() as b:
+        ids = []
+        for c, n in work:
+            gid = b.add(c, n)
+            b.set_plan(gid, wpl, 4, 16)
+            ids.append(gid)
+        b.run()
+        b.sync()
+        got = [b.fetch(g) for g in ids]
+        b.run_plain(4)
+        b.sync()
+        plain = [b.fetch(g) for g in ids]
+    for (c, n), g, p in zip(work, got, plain):
+        ref = oracle.life_cells(c, n)
+        assert np.array_equal(g, ref), (c.shape, n)
+        assert np.array_equal(p, ref), (c.shape, n)
 
 
 def test_batch_matches_plain_and_reruns():
