@@ -336,6 +336,11 @@ int gol_batch_run_plain(gol_batch* b, uint32_t temporal_steps);
 int gol_batch_sync(gol_batch* b);
 int gol_batch_fetch(gol_batch* b, int32_t grid_id, uint8_t* cells);
 int gol_batch_info(const gol_batch* b, uint64_t* grids, uint64_t* items, uint64_t* cell_updates);
+/* Exercises the persistent kernel's dependency-wait guard without a fault:
+ * launches a work list whose only item waits on a pass that never runs;
+ * the wait gives up after spin_limit polls (1 .. 2^24, each >= 64 ns) and
+ * *status = GOL_E_TIMEOUT is expected; the context stays usable. */
+int gol_batch_probe_timeout(int32_t device, uint64_t spin_limit, int32_t* status);
 /* Census of the last gol_batch_run: SM clock cycles its work items spent
  * waiting on dependencies and computing, summed over items. */
 int gol_batch_census(gol_batch* b, uint64_t* wait_cycles, uint64_t* work_cycles);

@@ -55,7 +55,7 @@
 
 namespace golb200 {
 
-constexpr long long kSpinLimit = 1ll << 24;   // polls of >= 100 ns: a few-second guard
+constexpr long long kSpinLimit = 1ll << 24;   // polls of >= 64 ns: a few-second guard
 
 namespace {
 
@@ -126,11 +126,11 @@ __device__ __forceinline__ void seg_group(const BatchGrid& G, int group, int sli
     const int f1 = min(G.band + 2 * K - 1, G.Y - y0_last + K - 1);
     const int fast_end = f1 > f0 ? f0 + (f1 - f0) / 3 * 3 : f0;
     if (fast_end > f0) {
-        temporal_steps<WPL, K, false, false, false, true>(s, c, 0, f0);
-        temporal_steps<WPL, K, true, true, false, true>(s, c, f0, fast_end);
-        temporal_steps<WPL, K, false, false, false, true>(s, c, fast_end, nsteps);
+        temporal_steps<WPL, K, false, false, false, true, true>(s, c, 0, f0);
+        temporal_steps<WPL, K, true, true, false, true, true>(s, c, f0, fast_end);
+        temporal_steps<WPL, K, false, false, false, true, true>(s, c, fast_end, nsteps);
     } else {
-        temporal_steps<WPL, K, false, false, false, true>(s, c, 0, nsteps);
+        temporal_steps<WPL, K, false, false, false, true, true>(s, c, 0, nsteps);
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
@@ -155,7 +155,7 @@ __device__ __forceinline__ void seg_dispatch(int k, const BatchGrid& G, int grou
 template <int WPL_ONLY>
 __global__ void __launch_bounds__(32, GOL_BATCH_MIN_BLOCKS)
 batch_kernel(const BatchGrid* __restrict__ grids, const BatchItem* __restrict__ items, int nitems,
-             int* ticket, int* done, int* status, unsigned long long* census) {
+             int* ticket, int* done, int* status, unsigned long long* census, long long spin_limit) {
     __shared__ __align__(16) uint32_t ring[kRowRing * 32 * (WPL_ONLY ? WPL_ONLY : 4)];
     const int lane = threadIdx.x & 31;
     int t = 0;
@@ -179,7 +179,7 @@ batch_kernel(const BatchGrid* __restrict__ grids, const BatchItem* __restrict__ 
                 const int* p = done + G.done_base + (jlo + lane / ns) * G.nslices + slo + lane % ns;
                 long long spins = 0;
                 while (ld_acquire(p) < it.pass) {
-                    if (++spins > kSpinLimit || *(volatile int*)status != 0) {
+                    if (++spins > spin_limit || *(volatile int*)status != 0) {
                         ok = false;
                         break;
                     }
@@ -386,26 +386,28 @@ void batch_grid_from_choice(const GridChoice& ch, int W, int Y, BatchGrid* g) {
 
 cudaError_t launch_batch_kernel(const BatchGrid* d_grids, const BatchItem* d_items, int nitems,
                                 int* d_ticket, int* d_done, int* d_status, int num_sms,
-                                cudaStream_t stream, unsigned long long* d_census, int wpl_only) {
+                                cudaStream_t stream, unsigned long long* d_census, int wpl_only,
+                                long long spin_limit) {
+    if (spin_limit <= 0) spin_limit = kSpinLimit;
     if (nitems <= 0) return cudaSuccess;
     // every CTA resident at once (the dependency waits rely on it)
     const int ctas = std::min(nitems, num_sms * batch_kernel_ctas_per_sm(wpl_only));
     switch (wpl_only) {
         case 4:
             batch_kernel<4><<<ctas, 32, 0, stream>>>(d_grids, d_items, nitems, d_ticket, d_done,
-                                                     d_status, d_census);
+                                                     d_status, d_census, spin_limit);
             break;
         case 2:
             batch_kernel<2><<<ctas, 32, 0, stream>>>(d_grids, d_items, nitems, d_ticket, d_done,
-                                                     d_status, d_census);
+                                                     d_status, d_census, spin_limit);
             break;
         case 1:
             batch_kernel<1><<<ctas, 32, 0, stream>>>(d_grids, d_items, nitems, d_ticket, d_done,
-                                                     d_status, d_census);
+                                                     d_status, d_census, spin_limit);
             break;
         default:
             batch_kernel<0><<<ctas, 32, 0, stream>>>(d_grids, d_items, nitems, d_ticket, d_done,
-                                                     d_status, d_census);
+                                                     d_status, d_census, spin_limit);
             break;
     }
     return cudaPeekAtLastError();
@@ -821,6 +823,52 @@ int gol_batch_info(const gol_batch* b, uint64_t* grids, uint64_t* items, uint64_
     if (grids) *grids = b->grids.size();
     if (items) *items = (uint64_t)b->nitems;
     if (cell_updates) *cell_updates = cu;
+    return GOL_OK;
+}
+
+// Exercises the dependency-wait guard without a fault: a work list whose
+// only item (pass 1 of a one-word grid) depends on pass 0, which is not in
+// the list, so its wait must give up after spin_limit polls, record
+// GOL_E_TIMEOUT in the status word and end the launch normally.
+int gol_batch_probe_timeout(int32_t device, uint64_t spin_limit, int32_t* status_out) {
+    if (!status_out || spin_limit == 0 || spin_limit > (1ull << 24)) return GOL_E_INVALID;
+    *status_out = 0;
+    if (cudaSetDevice(device) != cudaSuccess) return GOL_E_CUDA;
+    golb200::GridChoice ch;
+    if (!golb200::choose_batch_plan(1, 32, 2, 1, 1, 16, &ch)) return GOL_E_UNSUPPORTED;
+    BatchGrid g{};
+    golb200::batch_grid_from_choice(ch, 1, 32, &g);
+    const BatchItem item{0, 0, 0, 1};
+    const int ncount = g.ngroups * g.nslices;
+    uint32_t* bufs = nullptr;
+    BatchGrid* d_grid = nullptr;
+    BatchItem* d_item = nullptr;
+    int* d_ints = nullptr;   // done[ncount], ticket, status
+    cudaStream_t s = nullptr;
+    cudaError_t ce = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaMalloc(&bufs, 2 * 32 * sizeof(uint32_t));
+    if (ce == cudaSuccess) ce = cudaMalloc(&d_grid, sizeof(BatchGrid));
+    if (ce == cudaSuccess) ce = cudaMalloc(&d_item, sizeof(BatchItem));
+    if (ce == cudaSuccess) ce = cudaMalloc(&d_ints, (ncount + 2) * sizeof(int));
+    if (ce == cudaSuccess) {
+        g.buf[0] = bufs;
+        g.buf[1] = bufs + 32;
+        ce = cudaMemsetAsync(bufs, 0, 2 * 32 * sizeof(uint32_t), s);
+    }
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(d_ints, 0, (ncount + 2) * sizeof(int), s);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(d_grid, &g, sizeof(g), cudaMemcpyHostToDevice, s);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(d_item, &item, sizeof(item), cudaMemcpyHostToDevice, s);
+    if (ce == cudaSuccess)
+        ce = golb200::launch_batch_kernel(d_grid, d_item, 1, d_ints + ncount, d_ints, d_ints + ncount + 1,
+                                          1, s, nullptr, g.wpl, (long long)spin_limit);
+    int st = 0;
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(&st, d_ints + ncount + 1, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    for (void* p : {(void*)bufs, (void*)d_grid, (void*)d_item, (void*)d_ints})
+        if (p) cudaFree(p);
+    if (s) cudaStreamDestroy(s);
+    if (ce != cudaSuccess) return GOL_E_CUDA;
+    *status_out = st;
     return GOL_OK;
 }
 

@@ -128,10 +128,11 @@ void batch_grid_from_choice(const GridChoice& ch, int W, int Y, BatchGrid* g);
 // Launches the persistent batch kernel over `nitems` items (pass-major
 // order); done[] and *ticket, *status must be zero. All CTAs fit at once.
 // wpl_only: the lane width all grids share (batch_uniform_wpl), or 0.
+// spin_limit: polls before a dependency wait gives up (0 = the default guard).
 cudaError_t launch_batch_kernel(const BatchGrid* d_grids, const BatchItem* d_items, int nitems,
                                 int* d_ticket, int* d_done, int* d_status, int num_sms,
                                 cudaStream_t stream, unsigned long long* d_census = nullptr,
-                                int wpl_only = 0);
+                                int wpl_only = 0, long long spin_limit = 0);
 
 cudaError_t launch_pack_cells(const uint8_t* cells, uint32_t* words, size_t x, size_t y,
                               cudaStream_t stream);

@@ -193,7 +193,10 @@ __device__ __forceinline__ void issue_row(const TemporalCtx& c, int j, int slot)
 // row for their own band; neighbours come from explicit shuffle source
 // lanes, segment ends see dead cells, and no shared-memory edge table or
 // barrier is needed (y0/y1 are then per lane, B the common band height).
-template <int WPL, int K, int PH, bool FAST, bool LMASK, bool TRACK, bool SEG = false>
+// PART = rows padded to whole lanes: the last lane of a row may hold words
+// past W, masked word by word (otherwise a lane is all in or all out).
+template <int WPL, int K, int PH, bool FAST, bool LMASK, bool TRACK, bool SEG = false,
+          bool PART = false>
 __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const TemporalCtx& c, int i) {
     constexpr int NEW3 = PH % 3;          // ring-of-3 slot written at this step
     constexpr int PREV3 = (PH + 2) % 3;   // ... written one step ago
@@ -239,13 +242,14 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
             // Output row r of gen g (garbage during warm-up, never consumed).
             const int row = c.y0 - K + i - 2 * g;
             const bool row_ok = FAST || (unsigned)row < (unsigned)c.Y;
+            const uint32_t keep = row_ok ? c.wmask[0] : 0u;   // whole-lane mask
             uint32_t res[WPL];
 #pragma unroll
             for (int w = 0; w < WPL; ++w) {
                 res[w] = next_word(s.h0[g - 1][OLD3][w], s.h1[g - 1][OLD3][w],
                                    s.h0[g - 1][PREV3][w], s.h1[g - 1][PREV3][w],
                                    s.h0[g - 1][NEW3][w], s.h1[g - 1][NEW3][w], C[w]);
-                if (!FAST || LMASK) res[w] &= row_ok ? c.wmask[w] : 0u;
+                if (!FAST || LMASK) res[w] &= PART ? (row_ok ? c.wmask[w] : 0u) : keep;
             }
             if (g == K) {
                 if ((FAST || (row >= c.y0 && row < c.y1)) && c.own) {
@@ -279,13 +283,13 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
     if (!SEG) __syncthreads();
 }
 
-template <int WPL, int K, bool FAST, bool LMASK, bool TRACK, bool SEG = false>
+template <int WPL, int K, bool FAST, bool LMASK, bool TRACK, bool SEG = false, bool PART = false>
 __device__ __forceinline__ void temporal_steps(TemporalRegs<WPL, K>& s, const TemporalCtx& c,
                                                int i0, int i1) {
     for (int i = i0; i < i1; i += 3) {
-        temporal_step<WPL, K, 0, FAST, LMASK, TRACK, SEG>(s, c, i + 0);
-        temporal_step<WPL, K, 1, FAST, LMASK, TRACK, SEG>(s, c, i + 1);
-        temporal_step<WPL, K, 2, FAST, LMASK, TRACK, SEG>(s, c, i + 2);
+        temporal_step<WPL, K, 0, FAST, LMASK, TRACK, SEG, PART>(s, c, i + 0);
+        temporal_step<WPL, K, 1, FAST, LMASK, TRACK, SEG, PART>(s, c, i + 1);
+        temporal_step<WPL, K, 2, FAST, LMASK, TRACK, SEG, PART>(s, c, i + 2);
     }
 }
 

@@ -29,6 +29,7 @@ GOL_E_STATE = -2
 GOL_E_CUDA = -3
 GOL_E_NOMEM = -4
 GOL_E_UNSUPPORTED = -5
+GOL_E_TIMEOUT = -6
 
 LAYOUTS = {"rows": 0, "columns": 1, "tiles": 2}
 _WORD_DTYPES = {16: np.uint16, 32: np.uint32, 64: np.uint64}
@@ -125,6 +126,7 @@ def lib():
                                       ctypes.c_double, _u64, _u64, _vp, _vp, _vp, _vp, _vp]
     L.gol_load_bernoulli.argtypes = [_vp, _u64, _u64, _u64, ctypes.c_double]
     L.gol_load_zeros.argtypes = [_vp, _u64, _u64]
+    L.gol_batch_probe_timeout.argtypes = [ctypes.c_int32, _u64, ctypes.POINTER(ctypes.c_int32)]
     L.gol_load_always_changing.argtypes = [_vp, _u64, _u64]
     L.gol_lexicon_create.argtypes = [ctypes.POINTER(_vp)]
     L.gol_lexicon_add_text.argtypes = [_vp, ctypes.c_char_p]
@@ -479,6 +481,16 @@ class Lexicon:
             self.close()
         except Exception:
             pass
+
+
+def probe_batch_timeout(spin_limit: int = 1 << 14, device: int = 0) -> int:
+    """Runs the batch kernel on a work list whose only item waits forever on
+    its dependency; returns the status word (GOL_E_TIMEOUT expected)."""
+    st = ctypes.c_int32()
+    rc = lib().gol_batch_probe_timeout(device, spin_limit, ctypes.byref(st))
+    if rc != GOL_OK:
+        raise RuntimeError(f"gol_batch_probe_timeout failed with status {rc}")
+    return st.value
 
 
 def probe_int_peak(stream: int = 0) -> float:

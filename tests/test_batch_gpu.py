@@ -107,3 +107,18 @@ def test_autotuner_uses_segments_for_narrow_grids():
         assert p["segments"] > 1 and p["lane_words"] * (256 // 32 // p["lane_words"]) == 8
         gid2 = b.add(np.zeros((64, 8192), np.uint8), 10)
         assert b.plan(gid2)["segments"] == 1
+
+
+def test_dependency_wait_gives_up_with_a_status():
+    """The bounded dependency wait ends with GOL_E_TIMEOUT (no trap, no hang)
+    when a dependency never completes, and the context stays usable."""
+    import time
+    t0 = time.perf_counter()
+    assert golb200.probe_batch_timeout(1 << 12) == golb200.GOL_E_TIMEOUT
+    assert time.perf_counter() - t0 < 30
+    c = oracle.random_ones_zeros(256, 64, 1)
+    with golb200.GolBatch() as b:
+        gid = b.add(c, 17)
+        b.run()
+        b.sync()
+        assert np.array_equal(b.fetch(gid), oracle.life_cells(c, 17))
