@@ -93,8 +93,7 @@ __device__ __forceinline__ void seg_group(const BatchGrid& G, int group, int sli
     c.last_lane = q == L - 1;
     c.src_l = max(lane - 1, 0);
     c.src_r = min(lane + 1, 31);
-    c.erd = nullptr;
-    c.ewr = nullptr;
+    c.eb = nullptr;
     c.ring = ring + lane * WPL;
     c.ring_saddr = (uint32_t)__cvta_generic_to_shared(c.ring);
     c.ring_stride = 32 * WPL;

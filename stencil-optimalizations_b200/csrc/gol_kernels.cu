@@ -17,6 +17,12 @@ namespace {
 // consecutive passes.
 template <int WPL, int K>
 cudaError_t launch_one(const RowsLaunch& a, const RowsPlan& p, cudaStream_t stream) {
+    // Deep passes need more than the default 48 KB of dynamic shared memory
+    // (the edge table grows with K): opt in once per instantiation.
+    static const cudaError_t attr_ok = cudaFuncSetAttribute(
+        rows_temporal_kernel<WPL, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int)temporal_smem_bytes(K, kTemporalMaxThreads, WPL));
+    if (attr_ok != cudaSuccess) return attr_ok;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(p.nbands, p.nslices);
     cfg.blockDim = dim3(p.threads);

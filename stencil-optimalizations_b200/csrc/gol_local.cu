@@ -124,8 +124,7 @@ seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
         c.last_lane = q == L - 1;
         c.src_l = max(lane - 1, 0);
         c.src_r = min(lane + 1, 31);
-        c.erd = nullptr;
-        c.ewr = nullptr;
+        c.eb = nullptr;
         c.ring = ring + lane * WPL;
         c.ring_saddr = (uint32_t)__cvta_generic_to_shared(c.ring);
         c.ring_stride = 32 * WPL;

@@ -138,19 +138,23 @@ struct TemporalRegs {
     uint32_t o[K][3][WPL];        // stage g's output rows, slot = step % 3
 };
 
-// Edge table layout: [EW padded warps][K producer stages][3 step slots]
-// [2 sides], then one dummy entry per warp. Every lane's read/write base is
-// loop-invariant and each stage/slot offset is a compile-time immediate.
-// Padded warps 0 and EW-1 stay zero: the dead cells beyond the CTA's
-// outermost words. Lanes 1..30 write their (unused) edge words to their
-// warp's dummy entry, so publishing needs no branch.
-__host__ __device__ constexpr int edge_off(int g, int slot) { return (g * 3 + slot) * 2; }
+// Edge table: every lane publishes the first and the last word of each row
+// it produces (stage g's output, or stage 0's loaded row) and reads its
+// neighbours' from the previous step, one barrier per step in between.
+// Layout: [2 sides: first words, last words][K producer stages][3 step
+// slots][kEdgeStride lanes, lane t at t + 1]; entries 0 and threads + 1 stay
+// zero (the dead cells beyond the CTA's outermost words). Each lane's base
+// is loop-invariant and every stage/slot offset is a compile-time immediate;
+// neighbouring lanes touch neighbouring words (no bank conflicts).
+constexpr int kEdgeStride = kTemporalMaxThreads + 2;
+__host__ __device__ constexpr int edge_off(int g, int slot) { return (g * 3 + slot) * kEdgeStride; }
+template <int K>
+__host__ __device__ constexpr int edge_last_side() { return K * 3 * kEdgeStride; }
 
 struct TemporalCtx {
     const uint32_t* src;
     uint32_t* dst;
-    const uint32_t* erd;   // lane 0: left warp's side-1 entry; lane 31: right warp's side-0
-    uint32_t* ewr;         // lane 0 / 31: this warp's entry, side 0 / 1; others: dummy word
+    uint32_t* eb;          // edge table + this lane's index (entry of lane t is t + 1)
     bool first_lane, last_lane;
     const uint32_t* ring;  // this lane's words in ring slot 0 (shared memory)
     uint32_t ring_saddr;   // same, as a shared-window address for cp.async
@@ -226,12 +230,9 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
                 rw = __shfl_sync(0xffffffffu, P[0], c.src_r);
                 lw = c.first_lane ? 0u : lw;
                 rw = c.last_lane ? 0u : rw;
-            } else {
-                lw = __shfl_up_sync(0xffffffffu, P[WPL - 1], 1);
-                rw = __shfl_down_sync(0xffffffffu, P[0], 1);
-                const uint32_t ev = c.erd[edge_off(g - 1, PREV3)];
-                lw = c.first_lane ? ev : lw;
-                rw = c.last_lane ? ev : rw;
+            } else {   // published by the neighbour lanes last step
+                lw = c.eb[edge_last_side<K>() + edge_off(g - 1, PREV3)];
+                rw = c.eb[2 + edge_off(g - 1, PREV3)];
             }
 #pragma unroll
             for (int w = 0; w < WPL; ++w) {
@@ -264,7 +265,10 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
             } else {
 #pragma unroll
                 for (int w = 0; w < WPL; ++w) s.o[g - 1][NEW3][w] = res[w];
-                if (!SEG) c.ewr[edge_off(g, NEW3)] = c.last_lane ? res[WPL - 1] : res[0];
+                if (!SEG) {
+                    c.eb[1 + edge_off(g, NEW3)] = res[0];
+                    c.eb[1 + edge_last_side<K>() + edge_off(g, NEW3)] = res[WPL - 1];
+                }
             }
         }
     }
@@ -272,7 +276,10 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
     // Stage 0 (every step, so each step commits exactly one copy group):
     // publish this step's row, issue the row kRowsInFlight steps ahead, and
     // read the next step's row out of the ring.
-    if (!SEG) c.ewr[edge_off(0, NEW3)] = c.last_lane ? s.ld[NEW3][WPL - 1] : s.ld[NEW3][0];
+    if (!SEG) {
+        c.eb[1 + edge_off(0, NEW3)] = s.ld[NEW3][0];
+        c.eb[1 + edge_last_side<K>() + edge_off(0, NEW3)] = s.ld[NEW3][WPL - 1];
+    }
     // rd_slot holds step i+1's row; step i+kRowsInFlight's row goes kRowsInFlight-1
     // slots further on, into the slot read two steps ago.
     const int wr_slot = s.rd_slot + (kRowsInFlight - 1) - (s.rd_slot >= kRowRing - (kRowsInFlight - 1) ? kRowRing : 0);
@@ -301,7 +308,6 @@ __device__ __forceinline__ void temporal_steps(TemporalRegs<WPL, K>& s, const Te
 template <int WPL, int K, bool TRACK>
 __device__ __forceinline__ uint32_t band_tile(const RowsLaunch& a, int band, int slice_idx,
                                               uint32_t* smem) {
-    constexpr int ESTRIDE = K * 6;            // words per padded-warp entry
     uint32_t* ring = smem;                    // kRowRing slots of blockDim.x * WPL words
     uint32_t* edges = smem + kRowRing * blockDim.x * WPL;
     TemporalCtx c;
@@ -314,14 +320,9 @@ __device__ __forceinline__ uint32_t band_tile(const RowsLaunch& a, int band, int
     c.y1 = min(c.y0 + a.band, a.Y);
     c.B = c.y1 - c.y0;
     c.lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const int EW = (blockDim.x >> 5) + 2;
     c.first_lane = c.lane == 0;
     c.last_lane = c.lane == 31;
-    c.erd = edges + (c.first_lane ? warp * ESTRIDE + 1 : (warp + 2) * ESTRIDE);
-    c.ewr = (c.first_lane || c.last_lane)
-                ? edges + (warp + 1) * ESTRIDE + (c.last_lane ? 1 : 0)
-                : edges + (EW + warp) * ESTRIDE;
+    c.eb = edges + threadIdx.x;
     const int xs = slice_idx * a.slice;
     const int x0 = xs - a.halo;
     c.base = x0 + (int)threadIdx.x * WPL;
@@ -330,7 +331,7 @@ __device__ __forceinline__ uint32_t band_tile(const RowsLaunch& a, int band, int
     const bool all_lanes_ok = x0 >= 0 && x0 + (int)blockDim.x * WPL <= a.W;
     set_word_masks<WPL>(c);
 
-    for (int t = threadIdx.x; t < EW * ESTRIDE; t += blockDim.x) edges[t] = 0u;
+    for (int t = threadIdx.x; t < 2 * edge_last_side<K>(); t += blockDim.x) edges[t] = 0u;
 
     TemporalRegs<WPL, K> s;
 #pragma unroll
@@ -392,11 +393,9 @@ rows_temporal_kernel(RowsLaunch a) {
     band_tile<WPL, K, false>(a, blockIdx.x, blockIdx.y, smem);
 }
 
-// Shared memory a launch needs: the row ring, the edge table and one dummy
-// edge entry per warp.
+// Shared memory a launch needs: the row ring and the edge table.
 __host__ __device__ inline size_t temporal_smem_bytes(int K, int threads, int wpl) {
-    return ((size_t)kRowRing * threads * wpl + (size_t)(2 * (threads >> 5) + 2) * K * 6) *
-           sizeof(uint32_t);
+    return ((size_t)kRowRing * threads * wpl + (size_t)2 * K * 3 * kEdgeStride) * sizeof(uint32_t);
 }
 
 } // namespace golb200
