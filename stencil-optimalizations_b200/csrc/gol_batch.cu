@@ -71,7 +71,8 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 
 template <int WPL, int K>
 __device__ __forceinline__ void seg_group(const BatchGrid& G, int group, int slice_idx,
-                                          const uint32_t* src, uint32_t* dst, uint32_t* ring) {
+                                          const uint32_t* src, uint32_t* dst, uint32_t* ring,
+                                          uint32_t* etab) {
     const int lane = threadIdx.x & 31;
     const int L = G.seg_lanes;
     const int seg = lane / L, q = lane - seg * L;
@@ -89,11 +90,13 @@ __device__ __forceinline__ void seg_group(const BatchGrid& G, int group, int sli
     c.base = xs - G.halo + q * WPL;
     c.lane_ok = seg < G.segs && c.y0 < G.Y && c.base >= 0 && c.base < G.W;
     c.own = c.lane_ok && c.base >= xs && c.base < xs + G.slice;
-    c.first_lane = q == 0;
-    c.last_lane = q == L - 1;
+    c.eb = etab + lane;
+    c.el = q == 0 ? etab : etab + lane;                          // segment ends: zero entries
+    c.er = q == L - 1 ? etab + kSegEdgeStride - 1 : etab + lane + 2;
     c.src_l = max(lane - 1, 0);
     c.src_r = min(lane + 1, 31);
-    c.eb = nullptr;
+    c.seg_first = q == 0;
+    c.seg_last = q == L - 1;
     c.ring = ring + lane * WPL;
     c.ring_saddr = (uint32_t)__cvta_generic_to_shared(c.ring);
     c.ring_stride = 32 * WPL;
@@ -136,12 +139,13 @@ __device__ __forceinline__ void seg_group(const BatchGrid& G, int group, int sli
 
 template <int WPL>
 __device__ __forceinline__ void seg_dispatch(int k, const BatchGrid& G, int group, int slice,
-                                             const uint32_t* src, uint32_t* dst, uint32_t* ring) {
+                                             const uint32_t* src, uint32_t* dst, uint32_t* ring,
+                                             uint32_t* etab) {
     switch (k) {
-        case 1: seg_group<WPL, 1>(G, group, slice, src, dst, ring); break;
-        case 2: seg_group<WPL, 2>(G, group, slice, src, dst, ring); break;
-        case 3: seg_group<WPL, 3>(G, group, slice, src, dst, ring); break;
-        default: seg_group<WPL, 4>(G, group, slice, src, dst, ring); break;
+        case 1: seg_group<WPL, 1>(G, group, slice, src, dst, ring, etab); break;
+        case 2: seg_group<WPL, 2>(G, group, slice, src, dst, ring, etab); break;
+        case 3: seg_group<WPL, 3>(G, group, slice, src, dst, ring, etab); break;
+        default: seg_group<WPL, 4>(G, group, slice, src, dst, ring, etab); break;
     }
 }
 
@@ -156,7 +160,11 @@ __global__ void __launch_bounds__(32, GOL_BATCH_MIN_BLOCKS)
 batch_kernel(const BatchGrid* __restrict__ grids, const BatchItem* __restrict__ items, int nitems,
              int* ticket, int* done, int* status, unsigned long long* census, long long spin_limit) {
     __shared__ __align__(16) uint32_t ring[kRowRing * 32 * (WPL_ONLY ? WPL_ONLY : 4)];
+    constexpr int kEdgeWords = WPL_ONLY == 1 ? 1 : seg_edge_words(kBatchMaxK);   // 1: shuffles
+    __shared__ uint32_t etab[kEdgeWords];
     const int lane = threadIdx.x & 31;
+    for (int t = lane; t < kEdgeWords; t += 32) etab[t] = 0u;
+    __syncwarp();
     int t = 0;
     if (lane == 0) t = atomicAdd(ticket, 1);
     t = __shfl_sync(0xffffffffu, t, 0);
@@ -205,12 +213,12 @@ batch_kernel(const BatchGrid* __restrict__ grids, const BatchItem* __restrict__ 
         const uint32_t* src = odd ? G.buf[1] : G.buf[0];
         uint32_t* dst = odd ? G.buf[0] : G.buf[1];
         if constexpr (WPL_ONLY != 0) {
-            seg_dispatch<WPL_ONLY>(k, G, it.group, it.slice, src, dst, ring);
+            seg_dispatch<WPL_ONLY>(k, G, it.group, it.slice, src, dst, ring, etab);
         } else {
             switch (G.wpl) {
-                case 4: seg_dispatch<4>(k, G, it.group, it.slice, src, dst, ring); break;
-                case 2: seg_dispatch<2>(k, G, it.group, it.slice, src, dst, ring); break;
-                default: seg_dispatch<1>(k, G, it.group, it.slice, src, dst, ring); break;
+                case 4: seg_dispatch<4>(k, G, it.group, it.slice, src, dst, ring, etab); break;
+                case 2: seg_dispatch<2>(k, G, it.group, it.slice, src, dst, ring, etab); break;
+                default: seg_dispatch<1>(k, G, it.group, it.slice, src, dst, ring, etab); break;
             }
         }
         __threadfence();

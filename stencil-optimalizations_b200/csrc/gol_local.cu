@@ -97,9 +97,13 @@ template <int WPL, int K>
 __global__ void __launch_bounds__(32)
 seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
     __shared__ __align__(16) uint32_t ring[kRowRing * 32 * WPL];
+    constexpr int kEdgeWords = WPL == 1 ? 1 : seg_edge_words(K);   // one word per lane: shuffles
+    __shared__ uint32_t etab[kEdgeWords];
     const int lane = threadIdx.x & 31;
     const int L = seg_lanes;
     const int seg = lane / L, q = lane - seg * L;
+    for (int t = lane; t < kEdgeWords; t += 32) etab[t] = 0u;
+    __syncwarp();
     const int n = *t.count;
     for (int first = blockIdx.x * segs; first < n; first += gridDim.x * segs) {
         const int idx = first + seg;
@@ -120,11 +124,13 @@ seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
         c.base = xs - a.halo + q * WPL;
         c.lane_ok = has && c.y0 < a.Y && c.base >= 0 && c.base < a.W;
         c.own = c.lane_ok && c.base >= xs && c.base < xs + a.slice;
-        c.first_lane = q == 0;
-        c.last_lane = q == L - 1;
+        c.eb = etab + lane;
+        c.el = q == 0 ? etab : etab + lane;                      // segment ends: zero entries
+        c.er = q == L - 1 ? etab + kSegEdgeStride - 1 : etab + lane + 2;
         c.src_l = max(lane - 1, 0);
         c.src_r = min(lane + 1, 31);
-        c.eb = nullptr;
+        c.seg_first = q == 0;
+        c.seg_last = q == L - 1;
         c.ring = ring + lane * WPL;
         c.ring_saddr = (uint32_t)__cvta_generic_to_shared(c.ring);
         c.ring_stride = 32 * WPL;

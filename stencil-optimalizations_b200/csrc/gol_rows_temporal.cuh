@@ -142,20 +142,30 @@ struct TemporalRegs {
 // it produces (stage g's output, or stage 0's loaded row) and reads its
 // neighbours' from the previous step, one barrier per step in between.
 // Layout: [2 sides: first words, last words][K producer stages][3 step
-// slots][kEdgeStride lanes, lane t at t + 1]; entries 0 and threads + 1 stay
-// zero (the dead cells beyond the CTA's outermost words). Each lane's base
-// is loop-invariant and every stage/slot offset is a compile-time immediate;
-// neighbouring lanes touch neighbouring words (no bank conflicts).
+// slots][ES entries, lane t at t + 1]; entries 0 and ES - 1 are never
+// written and stay zero: the dead cells beyond the CTA's (or a segment's)
+// outermost words. Each lane reads through two loop-invariant pointers (its
+// left and right neighbour's entry, or a zero entry at a segment end) and
+// every stage/slot offset is a compile-time immediate; neighbouring lanes
+// touch neighbouring words (no bank conflicts). ES = kEdgeStride for
+// CTA-wide tables, kSegEdgeStride for one-warp (segmented) ones.
 constexpr int kEdgeStride = kTemporalMaxThreads + 2;
-__host__ __device__ constexpr int edge_off(int g, int slot) { return (g * 3 + slot) * kEdgeStride; }
-template <int K>
-__host__ __device__ constexpr int edge_last_side() { return K * 3 * kEdgeStride; }
+constexpr int kSegEdgeStride = 32 + 2;
+template <int ES>
+__host__ __device__ constexpr int edge_off(int g, int slot) { return (g * 3 + slot) * ES; }
+template <int K, int ES>
+__host__ __device__ constexpr int edge_last_side() { return K * 3 * ES; }
+// Words of a segmented warp's edge table for depth K.
+__host__ __device__ constexpr int seg_edge_words(int K) { return 2 * K * 3 * kSegEdgeStride; }
 
 struct TemporalCtx {
     const uint32_t* src;
     uint32_t* dst;
     uint32_t* eb;          // edge table + this lane's index (entry of lane t is t + 1)
-    bool first_lane, last_lane;
+    const uint32_t* el;    // entry of the left neighbour (eb), or a zero entry
+    const uint32_t* er;    // entry of the right neighbour (eb + 2), or a zero entry
+    // segmented warps of one word per lane exchange edges by shuffle instead
+    bool seg_first, seg_last;   // segment ends (their outer neighbour is dead)
     const uint32_t* ring;  // this lane's words in ring slot 0 (shared memory)
     uint32_t ring_saddr;   // same, as a shared-window address for cp.async
     int ring_stride;       // words per ring slot (blockDim.x * WPL)
@@ -192,16 +202,20 @@ __device__ __forceinline__ void issue_row(const TemporalCtx& c, int j, int slot)
 // grid, so no activity tests or row masks (the whole step is one basic
 // block and the K stages' independent chains interleave). LMASK forces the
 // out-of-grid words of a partial CTA (whole lanes, or the tail of the last
-// lane of a padded row) to stay dead. SEG = segmented warp: the
-// CTA is one warp cut into segments that each span a whole (narrow) grid
-// row for their own band; neighbours come from explicit shuffle source
-// lanes, segment ends see dead cells, and no shared-memory edge table or
-// barrier is needed (y0/y1 are then per lane, B the common band height).
+// lane of a padded row) to stay dead. SEG = segmented warp: the CTA is
+// one warp cut into segments that each span a whole (narrow) grid row for
+// their own band; segment ends read zero entries (dead cells), the edge
+// table is the warp's own and a step ends with a warp barrier (y0/y1 are
+// then per lane, B the common band height). With one word per lane the
+// four shared-memory accesses per stage would outweigh the word's own
+// work, so those warps shuffle instead (no table, no barrier).
 // PART = rows padded to whole lanes: the last lane of a row may hold words
 // past W, masked word by word (otherwise a lane is all in or all out).
 template <int WPL, int K, int PH, bool FAST, bool LMASK, bool TRACK, bool SEG = false,
           bool PART = false>
 __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const TemporalCtx& c, int i) {
+    constexpr int ES = SEG ? kSegEdgeStride : kEdgeStride;
+    constexpr bool SHFL = SEG && WPL == 1;
     constexpr int NEW3 = PH % 3;          // ring-of-3 slot written at this step
     constexpr int PREV3 = (PH + 2) % 3;   // ... written one step ago
     constexpr int OLD3 = (PH + 1) % 3;    // ... written two steps ago
@@ -225,14 +239,14 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
             }
             // Words just left and right of this lane's span.
             uint32_t lw, rw;
-            if (SEG) {
+            if (SHFL) {
                 lw = __shfl_sync(0xffffffffu, P[WPL - 1], c.src_l);
                 rw = __shfl_sync(0xffffffffu, P[0], c.src_r);
-                lw = c.first_lane ? 0u : lw;
-                rw = c.last_lane ? 0u : rw;
+                lw = c.seg_first ? 0u : lw;
+                rw = c.seg_last ? 0u : rw;
             } else {   // published by the neighbour lanes last step
-                lw = c.eb[edge_last_side<K>() + edge_off(g - 1, PREV3)];
-                rw = c.eb[2 + edge_off(g - 1, PREV3)];
+                lw = c.el[edge_last_side<K, ES>() + edge_off<ES>(g - 1, PREV3)];
+                rw = c.er[edge_off<ES>(g - 1, PREV3)];
             }
 #pragma unroll
             for (int w = 0; w < WPL; ++w) {
@@ -265,9 +279,9 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
             } else {
 #pragma unroll
                 for (int w = 0; w < WPL; ++w) s.o[g - 1][NEW3][w] = res[w];
-                if (!SEG) {
-                    c.eb[1 + edge_off(g, NEW3)] = res[0];
-                    c.eb[1 + edge_last_side<K>() + edge_off(g, NEW3)] = res[WPL - 1];
+                if (!SHFL) {
+                    c.eb[1 + edge_off<ES>(g, NEW3)] = res[0];
+                    c.eb[1 + edge_last_side<K, ES>() + edge_off<ES>(g, NEW3)] = res[WPL - 1];
                 }
             }
         }
@@ -276,9 +290,9 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
     // Stage 0 (every step, so each step commits exactly one copy group):
     // publish this step's row, issue the row kRowsInFlight steps ahead, and
     // read the next step's row out of the ring.
-    if (!SEG) {
-        c.eb[1 + edge_off(0, NEW3)] = s.ld[NEW3][0];
-        c.eb[1 + edge_last_side<K>() + edge_off(0, NEW3)] = s.ld[NEW3][WPL - 1];
+    if (!SHFL) {
+        c.eb[1 + edge_off<ES>(0, NEW3)] = s.ld[NEW3][0];
+        c.eb[1 + edge_last_side<K, ES>() + edge_off<ES>(0, NEW3)] = s.ld[NEW3][WPL - 1];
     }
     // rd_slot holds step i+1's row; step i+kRowsInFlight's row goes kRowsInFlight-1
     // slots further on, into the slot read two steps ago.
@@ -287,7 +301,10 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
     cp_async_wait<kRowsInFlight - 1>();
     lds_words<WPL>(c.ring + s.rd_slot * c.ring_stride, s.ld[(PH + 1) % 3]);
     s.rd_slot = s.rd_slot == kRowRing - 1 ? 0 : s.rd_slot + 1;
-    if (!SEG) __syncthreads();
+    if (!SEG)
+        __syncthreads();
+    else if (!SHFL)
+        __syncwarp();
 }
 
 template <int WPL, int K, bool FAST, bool LMASK, bool TRACK, bool SEG = false, bool PART = false>
@@ -320,9 +337,9 @@ __device__ __forceinline__ uint32_t band_tile(const RowsLaunch& a, int band, int
     c.y1 = min(c.y0 + a.band, a.Y);
     c.B = c.y1 - c.y0;
     c.lane = threadIdx.x & 31;
-    c.first_lane = c.lane == 0;
-    c.last_lane = c.lane == 31;
     c.eb = edges + threadIdx.x;
+    c.el = c.eb;
+    c.er = c.eb + 2;
     const int xs = slice_idx * a.slice;
     const int x0 = xs - a.halo;
     c.base = x0 + (int)threadIdx.x * WPL;
@@ -331,7 +348,7 @@ __device__ __forceinline__ uint32_t band_tile(const RowsLaunch& a, int band, int
     const bool all_lanes_ok = x0 >= 0 && x0 + (int)blockDim.x * WPL <= a.W;
     set_word_masks<WPL>(c);
 
-    for (int t = threadIdx.x; t < 2 * edge_last_side<K>(); t += blockDim.x) edges[t] = 0u;
+    for (int t = threadIdx.x; t < 2 * edge_last_side<K, kEdgeStride>(); t += blockDim.x) edges[t] = 0u;
 
     TemporalRegs<WPL, K> s;
 #pragma unroll
@@ -395,7 +412,8 @@ rows_temporal_kernel(RowsLaunch a) {
 
 // Shared memory a launch needs: the row ring and the edge table.
 __host__ __device__ inline size_t temporal_smem_bytes(int K, int threads, int wpl) {
-    return ((size_t)kRowRing * threads * wpl + (size_t)2 * K * 3 * kEdgeStride) * sizeof(uint32_t);
+    return ((size_t)kRowRing * threads * wpl + (size_t)2 * edge_last_side<1, kEdgeStride>() * K) *
+           sizeof(uint32_t);
 }
 
 } // namespace golb200
