@@ -115,7 +115,7 @@ seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
         c.src = a.src;
         c.dst = a.dst;
         c.W = a.W;
-        c.pitch = a.pitch;
+        c.pitch = a.W;   // change-tracking grids are never padded
         c.Y = a.Y;
         c.B = a.band;
         c.y0 = ty * a.band;
