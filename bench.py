@@ -380,6 +380,22 @@ def bench_serving(device) -> dict:
     return r
 
 
+def run_extra(name: str) -> dict:
+    """Runs one extra workload (`bench.py --only name`) in a fresh process:
+    its own CUDA context and allocator state, so what ran before it here
+    (the dense steps, the other extras) cannot shape its numbers; the
+    serving loop's latencies in particular depend on host scheduling."""
+    try:
+        r = subprocess.run([sys.executable, os.path.abspath(__file__), "--only", name],
+                           capture_output=True, text=True, timeout=1200)
+    except subprocess.TimeoutExpired:
+        return {"error": "timed out"}
+    for ln in reversed(r.stdout.splitlines()):
+        if ln.startswith("{"):
+            return json.loads(ln)[name]
+    return {"error": f"exit {r.returncode}: {r.stderr.strip()[-300:]}"}
+
+
 def run_ours(args, d: Dist) -> None:
     import torch
 
@@ -545,9 +561,9 @@ def run_ours(args, d: Dist) -> None:
 
     sparse = batched = serving = None
     if d.rank == 0 and d.world == 1 and not args.no_extras:
-        sparse = bench_sparse(stream, d.local_rank)
-        batched = bench_batched(stream, d.local_rank)
-        serving = bench_serving(d.local_rank)
+        sparse = run_extra("sparse")
+        batched = run_extra("batched")
+        serving = run_extra("serving")
 
     if d.rank == 0:
         line = {
