@@ -90,6 +90,10 @@ def libref():
             lib.ref_pack_layout.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _u64, _u64, _vp]
             lib.ref_unpack_layout.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _u64, _u64, _vp]
             lib.ref_load_zeros.argtypes = [_u64, _u64, _vp]
+            lib.ref_bitwise_create.argtypes = [_vp, _u64, _u64]
+            lib.ref_bitwise_create.restype = _vp
+            lib.ref_bitwise_run.argtypes = [_vp, _u64]
+            lib.ref_bitwise_finish.argtypes = [_vp, _vp]
             _ref = lib
     return _ref
 
@@ -417,3 +421,25 @@ def ref_lexicon_patterns() -> dict:
                                        _ptr(cells)), "ref_lexicon_pattern")
         out[name.value.decode()] = cells
     return out
+
+
+class RefBitwise:
+    """The reference's GoLCpuBitwise<char,64,AdderOps> with its phases apart:
+    construction packs and initialises, run(iters) advances, finish() returns
+    the cell grid (and frees the instance)."""
+
+    def __init__(self, cells: np.ndarray):
+        cells = np.ascontiguousarray(cells, dtype=np.uint8)
+        self.shape = cells.shape
+        self._h = _need_ref().ref_bitwise_create(_ptr(cells), cells.shape[1], cells.shape[0])
+        if not self._h:
+            raise RuntimeError("ref_bitwise_create failed")
+
+    def run(self, iters: int) -> None:
+        _check(_need_ref().ref_bitwise_run(self._h, iters), "ref_bitwise_run")
+
+    def finish(self) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.uint8)
+        h, self._h = self._h, None
+        _check(_need_ref().ref_bitwise_finish(h, _ptr(out)), "ref_bitwise_finish")
+        return out

@@ -14,6 +14,8 @@
 //                                src/infrastructure/experiment_params.hpp:43)
 //   ref_run_cpu_bitwise_adder  : algorithms::GoLCpuBitwise<char, 32|64, AdderOps>
 //                                (src/algorithms/cpu-bitwise-general/gol_cpu_bitwise_general.hpp:32-120)
+//   ref_bitwise_create / _run / _finish : the same 64-bit algorithm with its
+//                                phases apart, so run() can be timed alone
 //   ref_pack_rows / ref_unpack_rows : GeneralBitGrid<uintW_t, AdderMode>
 //                                fill_grid / to_grid
 //                                (src/algorithms/_shared/bitwise/general_bit_grid.hpp:171-246)
@@ -157,6 +159,45 @@ int ref_run_cpu_bitwise_adder(int word_bits, const uint8_t* in, uint64_t x, uint
     } catch (const std::exception&) {
         return -1;
     }
+}
+
+// GoLCpuBitwise<char, 64, AdderOps> split into its phases so a caller can
+// time run() alone: create = set_params + set_and_format_input_data +
+// initialize_data_structures; run = run(iters), continuing from the
+// instance's current state; finish = finalize_data_structures +
+// fetch_result, then the instance is freed.
+void* ref_bitwise_create(const uint8_t* in, uint64_t x, uint64_t y) {
+    try {
+        auto* alg = new algorithms::GoLCpuBitwise<char, 64, algorithms::AdderOps>();
+        alg->set_params(make_params(x, y, 0, 0));
+        alg->set_and_format_input_data(grid_from(in, x, y));
+        alg->initialize_data_structures();
+        return alg;
+    } catch (const std::exception&) {
+        return nullptr;
+    }
+}
+
+int ref_bitwise_run(void* h, uint64_t iters) {
+    try {
+        static_cast<algorithms::GoLCpuBitwise<char, 64, algorithms::AdderOps>*>(h)->run(iters);
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+int ref_bitwise_finish(void* h, uint8_t* out) {
+    auto* alg = static_cast<algorithms::GoLCpuBitwise<char, 64, algorithms::AdderOps>*>(h);
+    int rc = 0;
+    try {
+        alg->finalize_data_structures();
+        if (out) grid_to(alg->fetch_result(), out);
+    } catch (const std::exception&) {
+        rc = -1;
+    }
+    delete alg;
+    return rc;
 }
 
 int ref_pack_rows(int word_bits, const uint8_t* cells, uint64_t x, uint64_t y, void* words) {
