@@ -200,7 +200,10 @@ bool plan_local_tiles(int W, int Y, int k, int tile_rows, int wpl, int num_sms, 
     if (k < 1 || k > kMaxTemporalSteps || W <= 0 || Y <= 0) return false;
     if (wpl == 0) wpl = 1;
     if ((wpl != 1 && wpl != 2 && wpl != 4) || W % wpl || k > kMaxKForWpl(wpl)) return false;
-    int band = tile_rows > 0 ? tile_rows : std::max(32, k);
+    // Default height: the smallest the skip rule allows (k rows), not below 8.
+    // On the sparse 16384^2 workload at k = 8, 8-row tiles ran at 49 T
+    // cell-updates/s against 40 T for 32-row ones: finer tiles skip more.
+    int band = tile_rows > 0 ? tile_rows : std::max(8, k);
     if (band < k) return false;                         // the 3x3 skip rule needs tiles >= K rows
     RowsPlan& p = lp->rows;
     p.wpl = wpl;

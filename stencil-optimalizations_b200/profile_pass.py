@@ -38,6 +38,7 @@ def main() -> None:
     ap.add_argument("--mode", choices=["dense", "local", "batch"], default="dense")
     ap.add_argument("--gens", type=int, default=400)
     ap.add_argument("--grids", type=int, default=32)
+    ap.add_argument("--tile-rows", type=int, default=0, help="change-tracking tile height (0 = auto)")
     a = ap.parse_args()
     if a.mode == "local":
         return run_local(a)
@@ -74,7 +75,7 @@ def run_local(a) -> None:
     x, y = a.size, a.height or a.size
     g = golb200.load_sparse_patches(x, y, seed=42)
     with golb200.GolB200(grid_dimensions=(x, y), temporal_steps=a.k if a.k <= 16 else 8,
-                         algorithm="local") as alg:
+                         algorithm="local", tile_rows=a.tile_rows) as alg:
         alg.set_and_format_input_data(g)
         alg.initialize_data_structures()
         t0 = time.perf_counter()
