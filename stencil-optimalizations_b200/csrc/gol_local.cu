@@ -7,7 +7,7 @@
 // previous step; per-block state words record which warp tiles changed.
 //
 // Here one step is a pass of K generations and a tile is a narrow x-slice
-// (6 lanes of words; a halo lane each side absorbs the unknown cells beyond
+// (2 lanes of words, 64 cells, by default; a halo lane each side absorbs the unknown cells beyond
 // it, whose errors move one cell per generation) times a band of rows, so
 // the skip rule needs tiles at least K cells high and wide (a pass reads K
 // cells around each cell). Per pass:
@@ -16,7 +16,7 @@
 //          (warp ballot + one atomic per warp), this pass's bytes are
 //          cleared, and the last CTA appends the list length to a census;
 //   tiles  persistent one-warp CTAs walk the list, several tiles per warp
-//          (one per 8-lane segment: the segmented-warp form of the K-stage
+//          (one per 4-lane segment: the segmented-warp form of the K-stage
 //          pipeline), compare each tile's result with its input and set
 //          changed[tile] when any of its cells differs after the pass.
 // No copies for skipped tiles: a tile skipped at pass p did not change at
@@ -26,6 +26,14 @@
 
 #include "gol_internal.h"
 #include "gol_rows_temporal.cuh"
+
+#ifndef GOL_TILE_LANES
+// Change-tracking tile width in lanes: its words plus a halo lane each side.
+// On the sparse 16384^2 workload (k = 8, 8-row tiles) 3, 4, 5, 8 and 16
+// lanes ran at 55, 62, 55, 49 and 32 T cell-updates/s: 4 lanes (2 words,
+// 64 cells) balances skipped area against halo lanes.
+#define GOL_TILE_LANES 4
+#endif
 
 namespace golb200 {
 
@@ -210,7 +218,7 @@ bool plan_local_tiles(int W, int Y, int k, int tile_rows, int wpl, int num_sms, 
     p.band = band;
     p.nbands = (Y + band - 1) / band;
     p.threads = 32;
-    constexpr int kTileLanes = 8;                        // 6 lanes of words + a halo lane each side
+    constexpr int kTileLanes = GOL_TILE_LANES;           // lanes of words + a halo lane each side
     if (W / wpl <= kTileLanes) {
         p.slice = W;
         p.halo = 0;
