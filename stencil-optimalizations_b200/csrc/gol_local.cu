@@ -141,7 +141,7 @@ seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
         c.seg_last = q == L - 1;
         c.ring = ring + lane * WPL;
         c.ring_saddr = (uint32_t)__cvta_generic_to_shared(c.ring);
-        c.ring_stride = 32 * WPL;
+        c.ring_stride = ring_slot_words<WPL, true>();
         set_word_masks<WPL>(c);
 
         TemporalRegs<WPL, K> s;
@@ -158,7 +158,6 @@ seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
         for (int j = 0; j < kRowsInFlight; ++j) issue_row<WPL, K>(c, j, j);
         cp_async_wait<kRowsInFlight - 1>();
         lds_words<WPL>(c.ring, s.ld[0]);
-        s.rd_slot = 1;
         s.diff = 0u;
 
         // Steady state while every segment's rows stay inside the grid: the

@@ -87,10 +87,10 @@ __device__ __forceinline__ void store_words(uint32_t* p, const uint32_t (&v)[WPL
 // and later reads back only its own words, so a per-thread
 // cp.async.wait_group (a hardware wait, no spin) orders the two. Rows and
 // lanes outside the grid are zero-filled by the copy itself (src-size 0).
-#ifndef GOL_ROW_RING
-#define GOL_ROW_RING 6
-#endif
-constexpr int kRowRing = GOL_ROW_RING;
+// Step i's row lives in slot i mod 6, i.e. two banks of three slots: the
+// steps are unrolled by three, so within a bank every slot offset is a
+// compile-time immediate and only the bank changes (once per three steps).
+constexpr int kRowRing = 6;
 constexpr int kRowsInFlight = kRowRing - 1;
 
 template <int WPL>
@@ -130,7 +130,8 @@ __device__ __forceinline__ void lds_words(const uint32_t* p, uint32_t (&v)[WPL])
 
 template <int WPL, int K>
 struct TemporalRegs {
-    int rd_slot;                  // ring slot of the row stage 0 reads next
+    uint32_t bank_cur, bank_oth;  // shared addresses of this lane's ring banks: steps 3t..3t+2
+                                  // keep their rows in bank_cur (slots 3*(t%2) .. +2)
     uint32_t diff;                // change tracking: OR of (new ^ old) over stored words
     uint32_t ld[3][WPL];          // stage-0 rows, slot = step % 3
     uint32_t h0[K][3][WPL];       // stage g's horizontal sums, bit plane 0
@@ -168,7 +169,7 @@ struct TemporalCtx {
     bool seg_first, seg_last;   // segment ends (their outer neighbour is dead)
     const uint32_t* ring;  // this lane's words in ring slot 0 (shared memory)
     uint32_t ring_saddr;   // same, as a shared-window address for cp.async
-    int ring_stride;       // words per ring slot (blockDim.x * WPL)
+    int ring_stride;       // words per ring slot: ring_slot_words<WPL, SEG>()
     int W, Y, y0, y1, B;
     int pitch;      // words from one row to the next: W, or W rounded up to WPL
                     // (then the words past W are zero and stay zero)
@@ -187,15 +188,39 @@ __device__ __forceinline__ void set_word_masks(TemporalCtx& c) {
         c.wmask[w] = (w < WPL && c.lane_ok && c.base + w < c.W) ? 0xffffffffu : 0u;
 }
 
-// Copies the row stage 0 consumes at step j (grid row y0 - K + j) into ring
-// slot `slot`, zero-filled outside the grid; commits it as one group.
+// Words per ring slot: the CTA's widest possible row of lanes (one warp for
+// segmented warps), so that slot offsets are compile-time constants.
+template <int WPL, bool SEG>
+__host__ __device__ constexpr int ring_slot_words() { return (SEG ? 32 : kTemporalMaxThreads) * WPL; }
+
+// Copies the row stage 0 consumes at step j (grid row y0 - K + j) to the
+// shared address `saddr` (this lane's words of a ring slot), zero-filled
+// outside the grid; commits it as one group.
 template <int WPL, int K>
-__device__ __forceinline__ void issue_row(const TemporalCtx& c, int j, int slot) {
+__device__ __forceinline__ void issue_row_at(const TemporalCtx& c, int j, uint32_t saddr) {
     const int r = c.y0 - K + j;
     const bool v = c.lane_ok && (unsigned)r < (unsigned)c.Y;
     const uint32_t* g = v ? c.src + (size_t)r * c.pitch + c.base : c.src;
-    cp_async_words<WPL>(c.ring_saddr + (uint32_t)(slot * c.ring_stride) * 4u, g, v);
+    cp_async_words<WPL>(saddr, g, v);
     cp_async_commit();
+}
+
+template <int WPL, int K>
+__device__ __forceinline__ void issue_row(const TemporalCtx& c, int j, int slot) {
+    issue_row_at<WPL, K>(c, j, c.ring_saddr + (uint32_t)(slot * c.ring_stride) * 4u);
+}
+
+// Reads this lane's words of a ring slot at a shared address.
+template <int WPL>
+__device__ __forceinline__ void lds_words_at(uint32_t saddr, uint32_t (&v)[WPL]) {
+    if constexpr (WPL == 4) {
+        asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                     : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]) : "r"(saddr) : "memory");
+    } else if constexpr (WPL == 2) {
+        asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v[0]), "=r"(v[1]) : "r"(saddr) : "memory");
+    } else {
+        asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v[0]) : "r"(saddr) : "memory");
+    }
 }
 
 // Step body. FAST = steady state: every stage active, every row inside the
@@ -294,13 +319,20 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
         c.eb[1 + edge_off<ES>(0, NEW3)] = s.ld[NEW3][0];
         c.eb[1 + edge_last_side<K, ES>() + edge_off<ES>(0, NEW3)] = s.ld[NEW3][WPL - 1];
     }
-    // rd_slot holds step i+1's row; step i+kRowsInFlight's row goes kRowsInFlight-1
-    // slots further on, into the slot read two steps ago.
-    const int wr_slot = s.rd_slot + (kRowsInFlight - 1) - (s.rd_slot >= kRowRing - (kRowsInFlight - 1) ? kRowRing : 0);
-    issue_row<WPL, K>(c, i + kRowsInFlight, wr_slot);
+    // Step i = 3t + PH reads row i+1 (slot (i+1) mod 6) and issues row i+5
+    // (slot (i+5) mod 6, the one read two steps ago): with bank_cur holding
+    // slots of steps 3t..3t+2, both are a bank plus a constant.
+    constexpr uint32_t SB = ring_slot_words<WPL, SEG>() * 4u;   // bytes per slot
+    const uint32_t rd = PH == 0 ? s.bank_cur + SB : PH == 1 ? s.bank_cur + 2 * SB : s.bank_oth;
+    const uint32_t wr = PH == 0 ? s.bank_oth + 2 * SB : PH == 1 ? s.bank_cur : s.bank_cur + SB;
+    issue_row_at<WPL, K>(c, i + kRowsInFlight, wr);
     cp_async_wait<kRowsInFlight - 1>();
-    lds_words<WPL>(c.ring + s.rd_slot * c.ring_stride, s.ld[(PH + 1) % 3]);
-    s.rd_slot = s.rd_slot == kRowRing - 1 ? 0 : s.rd_slot + 1;
+    lds_words_at<WPL>(rd, s.ld[(PH + 1) % 3]);
+    if (PH == 2) {   // steps 3t+3.. use the other bank
+        const uint32_t t = s.bank_cur;
+        s.bank_cur = s.bank_oth;
+        s.bank_oth = t;
+    }
     if (!SEG)
         __syncthreads();
     else if (!SHFL)
@@ -310,6 +342,11 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
 template <int WPL, int K, bool FAST, bool LMASK, bool TRACK, bool SEG = false, bool PART = false>
 __device__ __forceinline__ void temporal_steps(TemporalRegs<WPL, K>& s, const TemporalCtx& c,
                                                int i0, int i1) {
+    // i0 is a multiple of 3; the bank of steps i0..i0+2 is (i0 / 3) % 2.
+    constexpr uint32_t BANK = 3u * ring_slot_words<WPL, SEG>() * 4u;
+    const bool odd = (i0 / 3) & 1;
+    s.bank_cur = c.ring_saddr + (odd ? BANK : 0u);
+    s.bank_oth = c.ring_saddr + (odd ? 0u : BANK);
     for (int i = i0; i < i1; i += 3) {
         temporal_step<WPL, K, 0, FAST, LMASK, TRACK, SEG, PART>(s, c, i + 0);
         temporal_step<WPL, K, 1, FAST, LMASK, TRACK, SEG, PART>(s, c, i + 1);
@@ -325,8 +362,8 @@ __device__ __forceinline__ void temporal_steps(TemporalRegs<WPL, K>& s, const Te
 template <int WPL, int K, bool TRACK>
 __device__ __forceinline__ uint32_t band_tile(const RowsLaunch& a, int band, int slice_idx,
                                               uint32_t* smem) {
-    uint32_t* ring = smem;                    // kRowRing slots of blockDim.x * WPL words
-    uint32_t* edges = smem + kRowRing * blockDim.x * WPL;
+    uint32_t* ring = smem;                    // kRowRing slots of ring_slot_words words
+    uint32_t* edges = smem + kRowRing * ring_slot_words<WPL, false>();
     TemporalCtx c;
     c.src = a.src;
     c.dst = a.dst;
@@ -363,11 +400,10 @@ __device__ __forceinline__ uint32_t band_tile(const RowsLaunch& a, int band, int
     }
     c.ring = ring + threadIdx.x * WPL;
     c.ring_saddr = (uint32_t)__cvta_generic_to_shared(c.ring);
-    c.ring_stride = blockDim.x * WPL;
+    c.ring_stride = ring_slot_words<WPL, false>();
     for (int j = 0; j < kRowsInFlight; ++j) issue_row<WPL, K>(c, j, j);
     cp_async_wait<kRowsInFlight - 1>();
     lds_words<WPL>(c.ring, s.ld[0]);
-    s.rd_slot = 1;
     s.diff = 0u;
     __syncthreads();
 
@@ -412,7 +448,8 @@ rows_temporal_kernel(RowsLaunch a) {
 
 // Shared memory a launch needs: the row ring and the edge table.
 __host__ __device__ inline size_t temporal_smem_bytes(int K, int threads, int wpl) {
-    return ((size_t)kRowRing * threads * wpl + (size_t)2 * edge_last_side<1, kEdgeStride>() * K) *
+    (void)threads;   // the ring is sized for the widest CTA (compile-time slot offsets)
+    return ((size_t)kRowRing * kTemporalMaxThreads * wpl + (size_t)2 * edge_last_side<1, kEdgeStride>() * K) *
            sizeof(uint32_t);
 }
 
