@@ -541,7 +541,7 @@ def run_ours(args, d: Dist) -> None:
         vsize = 8192
         vcells = golb200.load_random_ones_zeros(vsize, vsize, SEED)
         best = None
-        for k in (1, 2, 4, 8, 16):
+        for k in SWEEP_K:
             ve = golb200.GolB200(grid_dimensions=(vsize, vsize), state_bits_count=32,
                                  temporal_steps=k, device=d.local_rank, stream=stream.cuda_stream)
             ve.set_and_format_input_data(vcells)
