@@ -23,17 +23,21 @@
 //   * Each stage keeps, in registers, the horizontal 3-cell sums of its last
 //     three input rows (a ring of 3) and two raw input rows; it never
 //     touches shared memory for row data.
-//   * Neighbour bits across lanes come from warp shuffles; across warps from
-//     a tiny shared-memory "edge" table (first/last word of each warp's
-//     span, per stage, double-buffered by step parity). One __syncthreads
-//     per step publishes them.
+//   * Neighbour bits across lanes come from a shared-memory "edge" table:
+//     every lane publishes the first and last word of each row it produces
+//     (per stage, in a ring of 3 step slots) and reads its neighbours'
+//     entries of the previous step. One __syncthreads per step separates
+//     the two. (Segmented one-warp kernels keep a per-warp table with zero
+//     entries at segment ends; one word per lane uses warp shuffles.)
 //   * Warm-up and drain steps test which stages are active and mask rows
 //     outside the grid; the steady-state steps between them run a branch-
 //     free body, so a step is one basic block whose K stages interleave.
 //
 // Ring indices depend on the step number mod 3, so the step body is a
-// template on that phase and the loop is unrolled by 3: all ring accesses
-// are compile-time register names, no moves.
+// template on that phase and the loop is unrolled by 3: all register-ring
+// accesses are compile-time register names, no moves, and the shared-
+// memory row ring (6 slots = two banks of 3) needs only a bank swap per
+// three steps.
 #pragma once
 
 #include <cstdint>
