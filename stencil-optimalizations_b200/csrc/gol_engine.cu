@@ -114,7 +114,7 @@ int alloc_local(gol_engine* e) {
     cudaError_t ce = cudaSuccess;
     if (!s.list) {
         for (auto& p : s.changed)
-            if (ce == cudaSuccess) ce = cudaMalloc(&p, nt);
+            if (ce == cudaSuccess) ce = cudaMalloc(&p, golb200::local_change_bytes(e->lplan));
         if (ce == cudaSuccess) ce = cudaMalloc(&s.list, nt * sizeof(int));
         if (ce == cudaSuccess) ce = cudaMalloc(&s.count, 4 * sizeof(int));
         if (ce == cudaSuccess) ce = cudaMalloc(&s.census, kCensusCap * sizeof(uint32_t));
@@ -126,8 +126,9 @@ int alloc_local(gol_engine* e) {
         }
     }
     // First pass of a round: every tile counts as changed.
-    ce = cudaMemsetAsync(s.changed[1], 1, nt, e->stream);
-    if (ce == cudaSuccess) ce = cudaMemsetAsync(s.changed[0], 0, nt, e->stream);
+    const size_t cb = golb200::local_change_bytes(e->lplan);
+    ce = cudaMemsetAsync(s.changed[1], 0xff, cb, e->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(s.changed[0], 0, cb, e->stream);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(s.pass_no, 0, sizeof(uint32_t), e->stream);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(s.count, 0, 4 * sizeof(int), e->stream);
     if (ce != cudaSuccess) return e->cuda_fail(ce, "change-tracking reset");
@@ -467,8 +468,8 @@ int gol_run(gol_engine* e, uint64_t n) {
             if ((rc = launch_pass(e, rem, e->stream, e->cur))) return rc;
             e->cur ^= 1;
             e->performed += rem;
-            const size_t nt = (size_t)e->lplan.tiles_x * e->lplan.tiles_y;
-            cudaError_t ce = cudaMemsetAsync(e->lst.changed[e->lparity ^ 1], 1, nt, e->stream);
+            cudaError_t ce = cudaMemsetAsync(e->lst.changed[e->lparity ^ 1], 0xff,
+                                             golb200::local_change_bytes(e->lplan), e->stream);
             if (ce != cudaSuccess) return e->cuda_fail(ce, "change-flag reset");
         }
         return GOL_OK;

@@ -54,8 +54,14 @@ void host_layout_to_rows(const void* words, size_t x, size_t y, int layout, uint
 void host_rows_to_layout(const uint32_t* rows, size_t x, size_t y, int layout, uint32_t wb,
                          uint32_t xb, uint32_t yb, void* words);
 
+// Bytes of one pass's change bits: a bit per tile, rows of
+// ceil(tiles_x / 32) words.
+inline size_t local_change_bytes(const LocalPlan& lp) {
+    return (size_t)lp.tiles_y * ((lp.tiles_x + 31) / 32) * sizeof(uint32_t);
+}
+
 struct LocalState {
-    uint8_t* changed[2] = {nullptr, nullptr};   // per tile, by pass parity
+    uint32_t* changed[2] = {nullptr, nullptr};  // change bits per tile, by pass parity
     int* list = nullptr;                        // active tiles of the current pass
     int* count = nullptr;                       // list lengths by pass parity, CTA ticket
     uint32_t* census = nullptr;                 // active tiles per pass

@@ -11,14 +11,15 @@
 // it, whose errors move one cell per generation) times a band of rows, so
 // the skip rule needs tiles at least K cells high and wide (a pass reads K
 // cells around each cell). Per pass:
-//   plan   one thread per tile reads the previous pass's `changed` bytes
-//          of its 3x3 neighbourhood, active tiles are appended to a list
-//          (warp ballot + one atomic per warp), this pass's bytes are
-//          cleared, and the last CTA appends the list length to a census;
+//   plan   one thread per 32 tiles of a tile row dilates the previous
+//          pass's change bits over the 3x3 neighbourhood, active tiles are
+//          appended to a list (warp scan + one atomic per warp), this pass's
+//          bits are cleared, and the last CTA appends the list length to a
+//          census;
 //   tiles  persistent one-warp CTAs walk the list, several tiles per warp
 //          (one per 4-lane segment: the segmented-warp form of the K-stage
-//          pipeline), compare each tile's result with its input and set
-//          changed[tile] when any of its cells differs after the pass.
+//          pipeline), compare each tile's result with its input and set the
+//          tile's change bit when any of its cells differs after the pass.
 // No copies for skipped tiles: a tile skipped at pass p did not change at
 // pass p-1 (it is in its own neighbourhood), so the buffer pass p writes —
 // the one pass p-1 read — already holds its current state.
@@ -41,40 +42,62 @@ namespace {
 
 constexpr int kPlanThreads = 256;
 
-__device__ __forceinline__ bool tile_active(const uint8_t* prev, int tx, int ty, int tiles_x,
-                                            int tiles_y) {
-    for (int dy = -1; dy <= 1; ++dy) {
-        const int y = ty + dy;
-        if (y < 0 || y >= tiles_y) continue;
-        for (int dx = -1; dx <= 1; ++dx) {
-            const int x = tx + dx;
-            if (x < 0 || x >= tiles_x) continue;
-            if (prev[y * tiles_x + x]) return true;
-        }
-    }
-    return false;
-}
+// Change flags are bits: tile (tx, ty) is bit tx % 32 of word
+// ty * change_words(tiles_x) + tx / 32.
+__host__ __device__ inline int change_words(int tiles_x) { return (tiles_x + 31) / 32; }
 
-// One thread per tile. Active tiles are appended to `list` a warp at a time
-// (ballot, one atomic per warp: consecutive tiles stay together, so a warp
-// of the tile kernel gets neighbouring tiles). counts[parity] is this pass's
-// list length (zero on entry); counts[parity ^ 1] is zeroed for the next
-// pass; counts[2] is the CTA ticket the last CTA uses to record the census.
+// One thread per flag word (32 tiles of a tile row). A tile is active if it
+// or one of its 8 neighbours changed in the previous pass: the OR of the
+// three flag rows around it, each shifted one bit left and right (with the
+// carry bits of the neighbouring words). Active tiles are appended to
+// `list` in order a warp at a time (scan of the per-thread counts, one
+// atomic per warp, so a warp of the tile kernel gets neighbouring tiles).
+// counts[parity] is this pass's list length (zero on entry); counts[parity
+// ^ 1] is zeroed for the next pass; counts[2] is the CTA ticket the last CTA
+// uses to record the census. This pass's flags are cleared on the way.
 __global__ void __launch_bounds__(kPlanThreads)
-plan_tiles_kernel(const uint8_t* __restrict__ prev, uint8_t* __restrict__ clear, int tiles_x,
+plan_tiles_kernel(const uint32_t* __restrict__ prev, uint32_t* __restrict__ clear, int tiles_x,
                   int tiles_y, int* __restrict__ list, int* counts, int parity,
                   uint32_t* __restrict__ census, uint32_t census_cap, uint32_t* __restrict__ pass_no) {
-    const int ntiles = tiles_x * tiles_y;
+    const int wx = change_words(tiles_x);
+    const int nw = wx * tiles_y;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     if (blockIdx.x == 0 && threadIdx.x == 0) counts[parity ^ 1] = 0;
-    const bool act = t < ntiles && tile_active(prev, t % tiles_x, t / tiles_x, tiles_x, tiles_y);
-    if (t < ntiles) clear[t] = 0;
-    const unsigned m = __ballot_sync(0xffffffffu, act);
+    uint32_t act = 0u;
+    int ty = 0, w = 0;
+    if (t < nw) {
+        ty = t / wx;
+        w = t - ty * wx;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int y = ty + dy;
+            if (y < 0 || y >= tiles_y) continue;
+            const uint32_t* row = prev + (size_t)y * wx;
+            const uint32_t v = row[w];
+            const uint32_t l = w > 0 ? row[w - 1] : 0u;
+            const uint32_t r = w + 1 < wx ? row[w + 1] : 0u;
+            act |= v | (v << 1) | (l >> 31) | (v >> 1) | (r << 31);
+        }
+        const int valid = tiles_x - 32 * w;   // tiles in this word
+        if (valid < 32) act &= (1u << valid) - 1u;
+        clear[t] = 0u;
+    }
+    const int n = __popc(act);
+    int incl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int wtotal = __shfl_sync(0xffffffffu, incl, 31);
     int base = 0;
-    if (lane == 0 && m) base = atomicAdd(counts + parity, __popc(m));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (act) list[base + __popc(m & ((1u << lane) - 1u))] = t;
+    if (lane == 31 && wtotal) base = atomicAdd(counts + parity, wtotal);
+    base = __shfl_sync(0xffffffffu, base, 31) + incl - n;
+    while (act) {
+        const int b = __ffs((int)act) - 1;
+        act &= act - 1u;
+        list[base++] = ty * tiles_x + 32 * w + b;
+    }
 
     __threadfence();
     __syncthreads();
@@ -94,7 +117,7 @@ plan_tiles_kernel(const uint8_t* __restrict__ prev, uint8_t* __restrict__ clear,
 struct TileList {
     const int* list;        // active tile indices (band * tiles_x + slice)
     const int* count;       // number of entries in `list`
-    uint8_t* changed;       // per tile, this pass
+    uint32_t* changed;      // change bits of this pass (cleared by the plan kernel)
     int tiles_x;
 };
 
@@ -178,7 +201,8 @@ seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
         const unsigned any = __ballot_sync(0xffffffffu, s.diff != 0u);
         if (has && q == 0) {
             const unsigned segmask = (L == 32 ? 0xffffffffu : ((1u << L) - 1u)) << (seg * L);
-            t.changed[tile] = (any & segmask) ? 1 : 0;
+            if (any & segmask)
+                atomicOr(t.changed + ty * change_words(t.tiles_x) + tx / 32, 1u << (tx % 32));
         }
     }
 }
@@ -240,8 +264,8 @@ cudaError_t launch_local_pass(const uint32_t* src, uint32_t* dst, int W, int Y, 
                               const LocalPlan& lp, const LocalState& st, int parity,
                               cudaStream_t stream) {
     const RowsPlan& p = lp.rows;
-    const int ntiles = lp.tiles_x * lp.tiles_y;
-    plan_tiles_kernel<<<(ntiles + kPlanThreads - 1) / kPlanThreads, kPlanThreads, 0, stream>>>(
+    const int nwords = change_words(lp.tiles_x) * lp.tiles_y;
+    plan_tiles_kernel<<<(nwords + kPlanThreads - 1) / kPlanThreads, kPlanThreads, 0, stream>>>(
         st.changed[parity ^ 1], st.changed[parity], lp.tiles_x, lp.tiles_y, st.list, st.count,
         parity, st.census, st.census_cap, st.pass_no);
     cudaError_t e = cudaPeekAtLastError();
