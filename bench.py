@@ -337,7 +337,7 @@ def bench_sparse(stream, device) -> dict:
     out = {"workload": f"{size}x{size} dead grid, 1% of 64x64 slots Bernoulli(0.35) seed {seed}, "
                        f"{gens} generations", "unit": UNIT}
     results = {}
-    for name, kw in (("local", dict(algorithm="local", temporal_steps=8)),
+    for name, kw in (("local", dict(algorithm="local", temporal_steps=6)),
                      ("dense", dict(temporal_steps=4))):
         e = golb200.GolB200(grid_dimensions=(size, size), device=device, stream=stream.cuda_stream, **kw)
         e.set_and_format_input_data(g)
@@ -350,6 +350,7 @@ def bench_sparse(stream, device) -> dict:
         ms = _events_ms(stream, lambda: e.run(gens), e.sync)
         out[f"value_{name}"] = size * size * gens / (ms * 1e-3) / 1e9
         if name == "local":
+            out["local_temporal_steps"] = kw["temporal_steps"]
             st = e.local_stats()
             out["computed_tile_fraction"] = st["computed_tiles"] / max(1, st["passes"] * st["tiles_per_pass"])
         e.finalize_data_structures()

@@ -7,7 +7,7 @@
 // previous step; per-block state words record which warp tiles changed.
 //
 // Here one step is a pass of K generations and a tile is a narrow x-slice
-// (2 lanes of words, 64 cells, by default; a halo lane each side absorbs the unknown cells beyond
+// (1 lane of words, 32 cells, by default; a halo lane each side absorbs the unknown cells beyond
 // it, whose errors move one cell per generation) times a band of rows, so
 // the skip rule needs tiles at least K cells high and wide (a pass reads K
 // cells around each cell). Per pass:
@@ -17,7 +17,7 @@
 //          bits are cleared, and the last CTA appends the list length to a
 //          census;
 //   tiles  persistent one-warp CTAs walk the list, several tiles per warp
-//          (one per 4-lane segment: the segmented-warp form of the K-stage
+//          (one per 3-lane segment: the segmented-warp form of the K-stage
 //          pipeline), compare each tile's result with its input and set the
 //          tile's change bit when any of its cells differs after the pass.
 // No copies for skipped tiles: a tile skipped at pass p did not change at
@@ -30,10 +30,10 @@
 
 #ifndef GOL_TILE_LANES
 // Change-tracking tile width in lanes: its words plus a halo lane each side.
-// On the sparse 16384^2 workload (k = 8, 8-row tiles) 3, 4, 5, 8 and 16
-// lanes ran at 55, 62, 55, 49 and 32 T cell-updates/s: 4 lanes (2 words,
-// 64 cells) balances skipped area against halo lanes.
-#define GOL_TILE_LANES 4
+// On the sparse 16384^2 workload (k = 6, 6-row tiles, one change bit per
+// tile) 3, 4 and 5 lanes ran at 85, 81 and 71 T cell-updates/s: one word
+// (32 cells) per tile skips the most.
+#define GOL_TILE_LANES 3
 #endif
 
 namespace golb200 {
@@ -231,10 +231,11 @@ bool plan_local_tiles(int W, int Y, int k, int tile_rows, int wpl, int num_sms, 
     if (k < 1 || k > kMaxTemporalSteps || W <= 0 || Y <= 0) return false;
     if (wpl == 0) wpl = 1;
     if ((wpl != 1 && wpl != 2 && wpl != 4) || W % wpl || k > kMaxKForWpl(wpl)) return false;
-    // Default height: the smallest the skip rule allows (k rows), not below 8.
-    // On the sparse 16384^2 workload at k = 8, 8-row tiles ran at 49 T
-    // cell-updates/s against 40 T for 32-row ones: finer tiles skip more.
-    int band = tile_rows > 0 ? tile_rows : std::max(8, k);
+    // Default height: the smallest the skip rule allows (k rows), not below 4.
+    // Finer tiles skip more: on the sparse 16384^2 workload 8-row tiles ran
+    // at 49 T cell-updates/s against 40 T for 32-row ones (k = 8), and 6-row
+    // ones at k = 6 at 85 T against 77 T for 8-row ones (32-cell tiles).
+    int band = tile_rows > 0 ? tile_rows : std::max(4, k);
     if (band < k) return false;                         // the 3x3 skip rule needs tiles >= K rows
     RowsPlan& p = lp->rows;
     p.wpl = wpl;
