@@ -7,8 +7,9 @@
 // previous step; per-block state words record which warp tiles changed.
 //
 // Here one step is a pass of K generations and a tile is a narrow x-slice
-// (1 lane of words, 32 cells, by default; a halo lane each side absorbs the unknown cells beyond
-// it, whose errors move one cell per generation) times a band of rows, so
+// (by default one lane of words, 32 cells; a halo lane each side absorbs
+// the unknown cells beyond it, whose errors move one cell per generation)
+// times a band of rows, so
 // the skip rule needs tiles at least K cells high and wide (a pass reads K
 // cells around each cell). Per pass:
 //   plan   one thread per 32 tiles of a tile row dilates the previous
