@@ -49,6 +49,17 @@ def test_sparse_patches_vs_oracle(x, y, iters, k):
     assert st["computed_tiles"] <= st["passes"] * st["tiles_per_pass"]
 
 
+@pytest.mark.parametrize("wpl,k,tile_rows", [(2, 4, 0), (4, 4, 8), (2, 8, 12), (1, 3, 0)])
+def test_wider_lanes_and_tile_heights(wpl, k, tile_rows):
+    """Change tracking with 2 and 4 words per lane (wider tiles and halos)
+    and explicit tile heights, on a sparse input that settles and moves."""
+    g = golb200.load_sparse_patches(2048, 768, seed=wpl * 10 + k, patch=64, fraction=0.05,
+                                    density=0.35)
+    n = 6 * k + 1
+    assert np.array_equal(run_local(g, n, k=k, tile_rows=tile_rows, lane_words=wpl),
+                          oracle.life_cells(g, n)), (wpl, k, tile_rows)
+
+
 def test_sparse_input_skips_most_tiles():
     g = golb200.load_sparse_patches(8192, 4096, seed=11, patch=64, fraction=0.002, density=0.35)
     out, st = run_local(g, 1000, k=8, stats=True)

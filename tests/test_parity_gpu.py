@@ -62,6 +62,20 @@ def test_shapes_vs_oracle(x, y):
             assert np.array_equal(out, ref), (x, y, iters, k)
 
 
+@pytest.mark.parametrize("wpl,ks", [(1, (1, 5, 16)), (2, (1, 3, 8)), (4, (1, 2, 4))])
+def test_forced_lane_widths(wpl, ks):
+    """Every words-per-lane width at its depths, on narrow, one-CTA and
+    x-sliced widths (32 * 1025 words at one word per lane needs 5 slices)."""
+    for x, y in ((128, 40), (4096, 37), (32 * 1025, 7)):
+        if (x // 32) % wpl:
+            continue
+        g = oracle.random_ones_zeros(x, y, x + wpl)
+        for k in ks:
+            n = 2 * k + 1
+            assert np.array_equal(run_engine(g, n, k=k, word_bits=32, lane_words=wpl),
+                                  oracle.life_cells(g, n)), (x, y, wpl, k)
+
+
 def test_word_bits_32_and_64_agree():
     g = oracle.random_ones_zeros(512, 100, 77)
     a = run_engine(g, 37, word_bits=32)
