@@ -16,12 +16,20 @@ first and the fastest k runs the headline.
          bytes: the grid read once and written once per launch), plus the
          integer-pipe view against a live LOP3 peak probe;
   cpu_baseline  the reference's own CPU path (oracle/_ref, GoLCpuBitwise
-         <char,64,AdderOps>) on a bounded sample on this host.
+         <char,64,AdderOps>) on a bounded sample on this host, one thread,
+         its run phase timed (its pack/unpack phases outside).
+
+Beside the headline (N = 1 only), each in a fresh `bench.py --only …`
+process: the 8192^2 32-bit variant is timed in-process; `sparse` (change
+tracking vs the dense engine on a settling 16384^2 input), `batched` (512
+uneven grids in one persistent launch vs one launch per pass per grid) and
+`serving` (a Poisson request stream; p50/p99 latency).
 
 `--impl reference` times the reference's CPU implementation instead, on all
-host threads. Multi-GPU (torchrun): every rank advances its own replica
-(the path has no exchange step); value = all ranks' cell-updates / the
-slowest rank's time.
+host threads (its run phase, row bands of the grid, one instance per
+thread). Multi-GPU (torchrun): every rank advances its own replica (the
+path has no exchange step); value = all ranks' cell-updates / the slowest
+rank's time.
 """
 from __future__ import annotations
 
