@@ -19,8 +19,8 @@ first and the fastest k runs the headline.
          <char,64,AdderOps>) on a bounded sample on this host, one thread,
          its run phase timed (its pack/unpack phases outside).
 
-Beside the headline (N = 1 only), each in a fresh `bench.py --only …`
-process: the 8192^2 32-bit variant is timed in-process; `sparse` (change
+Beside the headline (N = 1 only): the 8192^2 32-bit variant, timed in this
+process, and, each in a fresh `bench.py --only …` process, `sparse` (change
 tracking vs the dense engine on a settling 16384^2 input), `batched` (512
 uneven grids in one persistent launch vs one launch per pass per grid) and
 `serving` (a Poisson request stream; p50/p99 latency).
