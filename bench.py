@@ -75,7 +75,7 @@ def parse_args():
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the sparse, batched and serving measurements")
-    ap.add_argument("--only", choices=["sparse", "batched", "serving"],
+    ap.add_argument("--only", choices=["sparse", "published", "batched", "serving"],
                     help="measure just that configuration and print it")
     return ap.parse_args()
 
@@ -336,6 +336,33 @@ def _events_ms(stream, fn, sync):
     return a.elapsed_time(b)
 
 
+def _engine_rate(stream, device, cells, gens: int, **kw):
+    """Times `gens` generations of one engine on `cells` after a warm-up run
+    of the same length (which captures its graphs), restarting from the same
+    input. Returns (Gcell-updates/s, change-tracking census or None, result
+    as 64-bit row words)."""
+    import golb200
+    y, x = cells.shape
+    e = golb200.GolB200(grid_dimensions=(x, y), device=device, stream=stream.cuda_stream, **kw)
+    e.set_and_format_input_data(cells)
+    e.initialize_data_structures()
+    e.run(gens)
+    e.sync()
+    e.finalize_data_structures()
+    e.set_and_format_input_data(cells)
+    e.initialize_data_structures()
+    ms = _events_ms(stream, lambda: e.run(gens), e.sync)
+    st = e.local_stats() if kw.get("algorithm") == "local" else None
+    e.finalize_data_structures()
+    words = e.fetch_words(64)
+    e.close()
+    return x * y * gens / (ms * 1e-3) / 1e9, st, words
+
+
+def _tile_fraction(st) -> float:
+    return st["computed_tiles"] / max(1, st["passes"] * st["tiles_per_pass"])
+
+
 def bench_sparse(stream, device) -> dict:
     """16384^2 all-dead grid, 1% of 64x64 slots Bernoulli(0.35), 20000
     generations: change-tracking tiles vs the dense engine, same input."""
@@ -344,27 +371,44 @@ def bench_sparse(stream, device) -> dict:
     g = golb200.load_sparse_patches(size, size, seed, 64, 0.01, 0.35)
     out = {"workload": f"{size}x{size} dead grid, 1% of 64x64 slots Bernoulli(0.35) seed {seed}, "
                        f"{gens} generations", "unit": UNIT}
-    results = {}
-    for name, kw in (("local", dict(algorithm="local", temporal_steps=6)),
-                     ("dense", dict(temporal_steps=4))):
-        e = golb200.GolB200(grid_dimensions=(size, size), device=device, stream=stream.cuda_stream, **kw)
-        e.set_and_format_input_data(g)
-        e.initialize_data_structures()
-        e.run(gens)                      # warm-up: captures the engine's graphs
-        e.sync()
-        e.finalize_data_structures()
-        e.set_and_format_input_data(g)   # the timed run starts from the same input
-        e.initialize_data_structures()
-        ms = _events_ms(stream, lambda: e.run(gens), e.sync)
-        out[f"value_{name}"] = size * size * gens / (ms * 1e-3) / 1e9
-        if name == "local":
-            out["local_temporal_steps"] = kw["temporal_steps"]
-            st = e.local_stats()
-            out["computed_tile_fraction"] = st["computed_tiles"] / max(1, st["passes"] * st["tiles_per_pass"])
-        e.finalize_data_structures()
-        results[name] = e.fetch_words(64)
-        e.close()
-    out["local_equals_dense"] = bool(np.array_equal(results["local"], results["dense"]))
+    out["value_local"], st, local = _engine_rate(stream, device, g, gens, algorithm="local",
+                                                 temporal_steps=6)
+    out["local_temporal_steps"] = 6
+    out["computed_tile_fraction"] = _tile_fraction(st)
+    out["value_dense"], _, dense = _engine_rate(stream, device, g, gens, temporal_steps=4)
+    out["local_equals_dense"] = bool(np.array_equal(local, dense))
+    return out
+
+
+def bench_published(stream, device) -> dict:
+    """The reference's published change-tracking workloads at 16384^2: the
+    all-dead grid (`zeros`, no work) and the blinker lattice
+    (`always-changing`, every tile changes every generation), 4096
+    generations, change tracking beside the dense engine. The blinker
+    lattice has period 2, so at an even pass depth every tile is back to its
+    input after each pass and change tracking skips it; an odd depth (5)
+    keeps every tile changing and measures the full-work case."""
+    import golb200
+    size, gens = SIZE, 4096
+    out = {"workload": f"{size}x{size}, {gens} generations: zeros and always-changing loaders",
+           "unit": UNIT}
+    zeros = golb200.load_zeros(size, size)
+    out["zeros_value_local"], st, w = _engine_rate(stream, device, zeros, gens, algorithm="local",
+                                                   temporal_steps=6)
+    out["zeros_computed_tile_fraction"] = _tile_fraction(st)
+    out["zeros_result_dead"] = not bool(w.any())
+    blink = golb200.load_always_changing(size, size)
+    ref = None
+    for k in (5, 6):
+        v, st, w = _engine_rate(stream, device, blink, gens, algorithm="local", temporal_steps=k)
+        out[f"always_changing_value_local_k{k}"] = v
+        out[f"always_changing_computed_tile_fraction_k{k}"] = _tile_fraction(st)
+        ref = w if ref is None else ref
+        out[f"always_changing_k{k}_equals_k5"] = bool(np.array_equal(w, ref))
+    for k in (4, 5):
+        out[f"always_changing_value_dense_k{k}"], _, w = _engine_rate(stream, device, blink, gens,
+                                                                      temporal_steps=k)
+        out[f"always_changing_dense_k{k}_equals_local"] = bool(np.array_equal(w, ref))
     return out
 
 
@@ -597,9 +641,10 @@ def run_ours(args, d: Dist) -> None:
     if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(cells)
 
-    sparse = batched = serving = None
+    sparse = published = batched = serving = None
     if d.rank == 0 and d.world == 1 and not args.no_extras:
         sparse = run_extra("sparse")
+        published = run_extra("published")
         batched = run_extra("batched")
         serving = run_extra("serving")
 
@@ -639,6 +684,7 @@ def run_ours(args, d: Dist) -> None:
             },
             "variant_8192_32bit": var,
             "sparse_settling": sparse,
+            "published_workloads": published,
             "batched_uneven": batched,
             "serving": serving,
             "e2e": {"value": e2e_value, "unit": UNIT,
@@ -665,6 +711,7 @@ def main():
         torch.cuda.set_device(d.local_rank)
         s = torch.cuda.Stream()
         fn = {"sparse": lambda: bench_sparse(s, d.local_rank),
+              "published": lambda: bench_published(s, d.local_rank),
               "batched": lambda: bench_batched(s, d.local_rank),
               "serving": lambda: bench_serving(d.local_rank)}[args.only]
         print(json.dumps({args.only: fn()}), flush=True)

@@ -80,6 +80,11 @@ typedef struct gol_config {
     int32_t device;                 /* CUDA device ordinal                       */
     uint32_t lane_words;            /* 32-bit words per lane: 1, 2, 4 (0 = auto) */
     void* stream;                   /* cudaStream_t to use; NULL = own stream    */
+    uint32_t dense_pct;             /* change tracking: a pass with at least this
+                                       percentage of its tiles active runs the
+                                       dense kernel instead of the tile kernel
+                                       (0 = auto, 6; above 100 = never)         */
+    uint32_t reserved;              /* zero                                      */
 } gol_config;
 
 typedef struct gol_engine gol_engine;

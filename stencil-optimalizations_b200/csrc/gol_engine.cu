@@ -116,7 +116,7 @@ int alloc_local(gol_engine* e) {
         for (auto& p : s.changed)
             if (ce == cudaSuccess) ce = cudaMalloc(&p, golb200::local_change_bytes(e->lplan));
         if (ce == cudaSuccess) ce = cudaMalloc(&s.list, nt * sizeof(int));
-        if (ce == cudaSuccess) ce = cudaMalloc(&s.count, 4 * sizeof(int));
+        if (ce == cudaSuccess) ce = cudaMalloc(&s.count, golb200::kLocalCountWords * sizeof(int));
         if (ce == cudaSuccess) ce = cudaMalloc(&s.census, kCensusCap * sizeof(uint32_t));
         if (ce == cudaSuccess) ce = cudaMalloc(&s.pass_no, sizeof(uint32_t));
         s.census_cap = kCensusCap;
@@ -130,7 +130,7 @@ int alloc_local(gol_engine* e) {
     ce = cudaMemsetAsync(s.changed[1], 0xff, cb, e->stream);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(s.changed[0], 0, cb, e->stream);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(s.pass_no, 0, sizeof(uint32_t), e->stream);
-    if (ce == cudaSuccess) ce = cudaMemsetAsync(s.count, 0, 4 * sizeof(int), e->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(s.count, 0, golb200::kLocalCountWords * sizeof(int), e->stream);
     if (ce != cudaSuccess) return e->cuda_fail(ce, "change-tracking reset");
     e->lparity = 0;
     return GOL_OK;
@@ -392,7 +392,9 @@ int gol_init(gol_engine* e) {
         return e->fail(GOL_E_UNSUPPORTED, "no kernel plan for this width and depth");
     e->local = e->cfg.algorithm == GOL_ALG_LOCAL;
     if (e->local && !golb200::plan_local_tiles(e->W, e->Y, k, (int)e->cfg.tile_rows,
-                                               (int)e->cfg.lane_words, sms, &e->lplan))
+                                               (int)e->cfg.lane_words, sms,
+                                               (int)std::min<uint32_t>(e->cfg.dense_pct, 101u),
+                                               &e->lplan))
         return e->fail(GOL_E_UNSUPPORTED,
                        "no change-tracking tile plan (tile_rows must be >= temporal_steps)");
     e->k = k;

@@ -40,7 +40,10 @@ struct LocalPlan {
     int seg_lanes = 0; // lanes per tile (its words plus a halo lane each side)
     int segs = 0;      // tiles carried by one warp at once
     int tiles_x = 0, tiles_y = 0;
-    int ctas = 0;      // persistent one-warp CTAs of the tile kernel
+    int ctas = 0;      // persistent CTAs of the tile kernel (capped at one wave)
+    int num_sms = 0;
+    RowsPlan dense;    // the dense form of a pass (row bands over the whole grid)
+    int dense_min = 0; // active tiles from which a pass runs dense (INT_MAX = never)
 };
 
 // Word layouts (gol_layouts.cu): X_BITS x Y_BITS cells per word.
@@ -60,19 +63,26 @@ inline size_t local_change_bytes(const LocalPlan& lp) {
     return (size_t)lp.tiles_y * ((lp.tiles_x + 31) / 32) * sizeof(uint32_t);
 }
 
+constexpr int kLocalCountWords = 6;
+
 struct LocalState {
     uint32_t* changed[2] = {nullptr, nullptr};  // change bits per tile, by pass parity
     int* list = nullptr;                        // active tiles of the current pass
-    int* count = nullptr;                       // list lengths by pass parity, CTA ticket
+    int* count = nullptr;                       // kLocalCountWords plan words: list lengths
+                                                // by pass parity, CTA ticket, dense choice
     uint32_t* census = nullptr;                 // active tiles per pass
     uint32_t census_cap = 0;
     uint32_t* pass_no = nullptr;                // passes recorded so far
 };
 
-bool plan_local_tiles(int W, int Y, int k, int tile_rows, int wpl, int num_sms, LocalPlan* lp);
+// dense_pct: active-tile share (percent) from which a pass runs dense;
+// 0 = the default, above 100 = never.
+bool plan_local_tiles(int W, int Y, int k, int tile_rows, int wpl, int num_sms, int dense_pct,
+                      LocalPlan* lp);
 
 // One change-tracking pass: plan (reads changed[parity ^ 1], clears
-// changed[parity]) then the tile kernel (writes changed[parity]).
+// changed[parity]) then the tile kernel or, from dense_min active tiles, the
+// dense tracked kernel (either writes changed[parity]).
 cudaError_t launch_local_pass(const uint32_t* src, uint32_t* dst, int W, int Y, int k,
                               const LocalPlan& lp, const LocalState& st, int parity,
                               cudaStream_t stream);

@@ -24,7 +24,16 @@
 // No copies for skipped tiles: a tile skipped at pass p did not change at
 // pass p-1 (it is in its own neighbourhood), so the buffer pass p writes —
 // the one pass p-1 read — already holds its current state.
+//   dense  when the plan finds at least `dense_min` active tiles the tile
+//          kernel returns at once and the row-band kernel runs the whole
+//          grid instead, comparing each output row with its input and
+//          setting the change bits of the tiles that differ. Its bits equal
+//          the tile kernel's (same tiles, same comparison), so the two modes
+//          hand over from pass to pass either way. Each tile is computed
+//          about 6x as fast there as by a tile warp (no halo lanes, no
+//          per-tile warm-up), so the dense pass wins above a few percent.
 #include <algorithm>
+#include <climits>
 
 #include "gol_internal.h"
 #include "gol_rows_temporal.cuh"
@@ -37,6 +46,20 @@
 #define GOL_TILE_LANES 3
 #endif
 
+#ifndef GOL_LOCAL_CARVEOUT
+// Shared-memory carveout (percent of the maximum) preferred by all three
+// kernels of a pass, so that the SMs keep one L1/shared split from kernel to
+// kernel; -1 leaves the driver's choice. On the sparse 16384^2 workload
+// (k = 6) the driver's choice ran at 79 T cell-updates/s, a common 100 %
+// at 77.6 T.
+#define GOL_LOCAL_CARVEOUT -1
+#endif
+
+#ifndef GOL_LOCAL_DENSE_PCT
+// Active-tile share (percent) from which a change-tracking pass runs dense.
+#define GOL_LOCAL_DENSE_PCT 6
+#endif
+
 namespace golb200 {
 
 namespace {
@@ -47,23 +70,36 @@ constexpr int kPlanThreads = 256;
 // ty * change_words(tiles_x) + tx / 32.
 __host__ __device__ inline int change_words(int tiles_x) { return (tiles_x + 31) / 32; }
 
+// The plan's device words (PlanCounts): list lengths by pass parity, the
+// last CTA's ticket, whether the last planned pass had at least dense_min
+// active tiles, and whether each parity's pass runs dense.
+enum PlanCounts { kListLen0 = 0, kTicket = 2, kDenseHint = 3, kDense0 = 4 };
+static_assert(kDense0 + 2 <= kLocalCountWords, "plan words");
+
 // One thread per flag word (32 tiles of a tile row). A tile is active if it
 // or one of its 8 neighbours changed in the previous pass: the OR of the
 // three flag rows around it, each shifted one bit left and right (with the
 // carry bits of the neighbouring words). Active tiles are appended to
 // `list` in order a warp at a time (scan of the per-thread counts, one
-// atomic per warp, so a warp of the tile kernel gets neighbouring tiles).
+// atomic per warp, so a warp of the tile kernel gets neighbouring tiles;
+// the warp then writes its entries together, in consecutive slots).
 // counts[parity] is this pass's list length (zero on entry); counts[parity
-// ^ 1] is zeroed for the next pass; counts[2] is the CTA ticket the last CTA
-// uses to record the census. This pass's flags are cleared on the way.
+// ^ 1] is zeroed for the next pass; the last CTA decides the pass's form
+// and records the census (tiles computed: all of them in a dense pass).
+// A pass runs dense when it has at least dense_min active tiles, or when
+// the previous one had: then the list is not written at all (the count
+// still is), at the price of one dense pass too many when activity drops.
+// This pass's flags are cleared on the way.
 __global__ void __launch_bounds__(kPlanThreads)
 plan_tiles_kernel(const uint32_t* __restrict__ prev, uint32_t* __restrict__ clear, int tiles_x,
                   int tiles_y, int* __restrict__ list, int* counts, int parity,
-                  uint32_t* __restrict__ census, uint32_t census_cap, uint32_t* __restrict__ pass_no) {
+                  uint32_t* __restrict__ census, uint32_t census_cap, uint32_t* __restrict__ pass_no,
+                  int dense_min) {
     const int wx = change_words(tiles_x);
     const int nw = wx * tiles_y;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
+    const bool skip_list = counts[kDenseHint] != 0;
     if (blockIdx.x == 0 && threadIdx.x == 0) counts[parity ^ 1] = 0;
     uint32_t act = 0u;
     int ty = 0, w = 0;
@@ -94,21 +130,32 @@ plan_tiles_kernel(const uint32_t* __restrict__ prev, uint32_t* __restrict__ clea
     int base = 0;
     if (lane == 31 && wtotal) base = atomicAdd(counts + parity, wtotal);
     base = __shfl_sync(0xffffffffu, base, 31) + incl - n;
-    while (act) {
-        const int b = __ffs((int)act) - 1;
-        act &= act - 1u;
-        list[base++] = ty * tiles_x + 32 * w + b;
+    if (!skip_list && wtotal) {
+        // Lane j's tiles, written by the lanes of their bits: consecutive
+        // set bits go to consecutive slots. Only lanes with tiles take a turn.
+        for (uint32_t busy = __ballot_sync(0xffffffffu, act != 0u); busy; busy &= busy - 1u) {
+            const int j = __ffs((int)busy) - 1;
+            const uint32_t aj = __shfl_sync(0xffffffffu, act, j);
+            const int bj = __shfl_sync(0xffffffffu, base, j);
+            const int tj = __shfl_sync(0xffffffffu, ty * tiles_x + 32 * w, j);
+            if ((aj >> lane) & 1u) list[bj + __popc(aj & ((1u << lane) - 1u))] = tj + lane;
+        }
     }
 
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
-        unsigned* ticket = reinterpret_cast<unsigned*>(counts + 2);
+        unsigned* ticket = reinterpret_cast<unsigned*>(counts + kTicket);
         if (atomicAdd(ticket, 1u) == gridDim.x - 1) {   // every CTA has appended
             __threadfence();
             const int total = atomicAdd(counts + parity, 0);
+            const bool dense = skip_list || total >= dense_min;
+            counts[kDense0 + parity] = dense ? 1 : 0;
+            counts[kDenseHint] = total >= dense_min ? 1 : 0;
             const uint32_t p = *pass_no;
-            if (census && p < census_cap) census[p] = (uint32_t)total;
+            // Tiles computed this pass: every tile when the pass runs dense.
+            const uint32_t computed = dense ? (uint32_t)tiles_x * tiles_y : (uint32_t)total;
+            if (census && p < census_cap) census[p] = computed;
             *pass_no = p + 1;
             *ticket = 0u;
         }
@@ -120,24 +167,48 @@ struct TileList {
     const int* count;       // number of entries in `list`
     uint32_t* changed;      // change bits of this pass (cleared by the plan kernel)
     int tiles_x;
+    const int* dense;       // nonzero: this pass runs dense (the tile kernel returns)
 };
+
+#ifndef GOL_TILE_WARPS
+// Warps of the tile kernel per CTA (each works alone, with its own shared
+// memory). One: with three the compiler gave the (1-word, depth-6) kernel
+// 118 registers instead of 96, 15 resident warps per SM instead of 21.
+#define GOL_TILE_WARPS 1
+#endif
+constexpr int kTileWarps = GOL_TILE_WARPS;
 
 // One warp, up to `segs` tiles at once (segment s takes list entry
 // base + s). Each segment streams its tile's band through the K stages with
 // change tracking; a ballot over the segment's lanes gives changed[tile].
+// When the dense form is enabled this kernel is launched after it, as a
+// programmatic dependent: the two never touch the same data in one pass
+// (one of them returns at once), so a tile pass starts without waiting,
+// but every CTA waits for the dense kernel before it ends, because later
+// work in the stream waits for this kernel only.
 template <int WPL, int K>
-__global__ void __launch_bounds__(32)
+__global__ void __launch_bounds__(32 * kTileWarps)
 seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
-    __shared__ __align__(16) uint32_t ring[kRowRing * 32 * WPL];
+    __shared__ __align__(16) uint32_t rings[kTileWarps][kRowRing * 32 * WPL];
     constexpr int kEdgeWords = WPL == 1 ? 1 : seg_edge_words(K);   // one word per lane: shuffles
-    __shared__ uint32_t etab[kEdgeWords];
+    __shared__ uint32_t etabs[kTileWarps][kEdgeWords];
+    const int dense = *t.dense;
+    const int n = *t.count;   // both loads in flight together
+    if (dense) {   // a dense pass
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+        return;
+    }
     const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    uint32_t* ring = rings[warp];
+    uint32_t* etab = etabs[warp];
+    const int gwarp = blockIdx.x * kTileWarps + warp;
+    const int nwarps = gridDim.x * kTileWarps;
     const int L = seg_lanes;
     const int seg = lane / L, q = lane - seg * L;
     for (int t = lane; t < kEdgeWords; t += 32) etab[t] = 0u;
     __syncwarp();
-    const int n = *t.count;
-    for (int first = blockIdx.x * segs; first < n; first += gridDim.x * segs) {
+    for (int first = gwarp * segs; first < n; first += nwarps * segs) {
         const int idx = first + seg;
         const bool has = seg < segs && idx < n;
         const int tile = has ? t.list[idx] : 0;
@@ -179,7 +250,7 @@ seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
                 s.o[g][0][w] = s.o[g][1][w] = s.o[g][2][w] = 0u;
             }
         }
-        for (int j = 0; j < kRowsInFlight; ++j) issue_row<WPL, K>(c, j, j);
+        for (int j = 0; j < kRowsInFlight; ++j) issue_row<WPL, K, 1, true>(c, j, j);
         cp_async_wait<kRowsInFlight - 1>();
         lds_words<WPL>(c.ring, s.ld[0]);
         s.diff = 0u;
@@ -206,13 +277,92 @@ seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
                 atomicOr(t.changed + ty * change_words(t.tiles_x) + tx / 32, 1u << (tx % 32));
         }
     }
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
+// The dense form of a change-tracking pass, launched every pass before the
+// tile kernel and returning at once unless the plan chose it; a grid of
+// resident CTAs (one wave) walks the row bands. It lets the tile kernel's
+// CTAs be scheduled at once: in a dense pass they wait on the SMs' spare
+// room, in a tile pass they start while this grid exits.
+template <int WPL, int K>
+__global__ void __launch_bounds__(kTemporalMaxThreads, GOL_TEMPORAL_MIN_BLOCKS)
+rows_tracked_kernel(RowsLaunch a, TileTrack tt, const int* __restrict__ dense, int nbands,
+                    int nunits) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    if (!*dense) return;
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x)
+        band_tile<WPL, K, 2>(a, u % nbands, u / nbands, smem, tt);
+}
+
+// Lane width of the dense tracked pass for depth k: the widest whose
+// register rings fit (one kernel per depth).
+constexpr int tracked_wpl(int k) { return k <= kMaxKForWpl(4) ? 4 : (k <= kMaxKForWpl(2) ? 2 : 1); }
+
+// Sets a kernel's preferred carveout once (GOL_LOCAL_CARVEOUT).
+template <typename F>
+cudaError_t set_carveout(F* kernel) {
+    if (GOL_LOCAL_CARVEOUT < 0) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                GOL_LOCAL_CARVEOUT);
+}
+
+template <int K>
+cudaError_t launch_tracked_one(const RowsLaunch& a, const TileTrack& tt, const int* dense,
+                               const RowsPlan& p, int num_sms, cudaStream_t stream) {
+    constexpr int WPL = tracked_wpl(K);
+    static const cudaError_t attr_ok = [] {
+        cudaError_t e = cudaFuncSetAttribute(rows_tracked_kernel<WPL, K>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)temporal_smem_bytes(K, kTemporalMaxThreads, WPL, true));
+        return e == cudaSuccess ? set_carveout(rows_tracked_kernel<WPL, K>) : e;
+    }();
+    if (attr_ok != cudaSuccess) return attr_ok;
+    const size_t smem = temporal_smem_bytes(K, p.threads, WPL, true);
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rows_tracked_kernel<WPL, K>,
+                                                                  p.threads, smem);
+    if (e != cudaSuccess) return e;
+    const int units = p.nbands * p.nslices;
+    const int grid = std::max(1, std::min(units, std::max(1, per_sm) * num_sms));
+    rows_tracked_kernel<WPL, K><<<grid, p.threads, smem, stream>>>(a, tt, dense, p.nbands, units);
+    return cudaPeekAtLastError();
+}
+
+template <int K>
+cudaError_t dispatch_tracked(int k, const RowsLaunch& a, const TileTrack& tt, const int* dense,
+                             const RowsPlan& p, int num_sms, cudaStream_t stream) {
+    if constexpr (K > kMaxTemporalSteps) {
+        return cudaErrorInvalidValue;
+    } else {
+        if (k == K) return launch_tracked_one<K>(a, tt, dense, p, num_sms, stream);
+        return dispatch_tracked<K + 1>(k, a, tt, dense, p, num_sms, stream);
+    }
+}
+
+// The tile kernel's grid: lp.ctas, capped at one wave of resident CTAs (it
+// walks the list); a programmatic dependent of the dense form when enabled.
 template <int WPL, int K>
 cudaError_t launch_tiles_one(const RowsLaunch& a, const TileList& t, const LocalPlan& lp,
                              cudaStream_t stream) {
-    seg_tiles_kernel<WPL, K><<<lp.ctas, 32, 0, stream>>>(a, t, lp.seg_lanes, lp.segs);
-    return cudaPeekAtLastError();
+    static const int per_sm = [] {
+        int n = 0;
+        if (set_carveout(seg_tiles_kernel<WPL, K>) != cudaSuccess) return -1;
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, seg_tiles_kernel<WPL, K>,
+                                                             32 * kTileWarps, 0) == cudaSuccess ? n : 0;
+    }();
+    if (per_sm < 0) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(per_sm > 0 ? std::max(1, std::min(lp.ctas, per_sm * lp.num_sms)) : lp.ctas);
+    cfg.blockDim = dim3(32 * kTileWarps);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = lp.dense_min == INT_MAX ? 0 : 1;
+    return cudaLaunchKernelEx(&cfg, seg_tiles_kernel<WPL, K>, a, t, lp.seg_lanes, lp.segs);
 }
 
 template <int WPL, int K>
@@ -228,7 +378,8 @@ cudaError_t dispatch_tiles(int k, const RowsLaunch& a, const TileList& t, const 
 
 } // namespace
 
-bool plan_local_tiles(int W, int Y, int k, int tile_rows, int wpl, int num_sms, LocalPlan* lp) {
+bool plan_local_tiles(int W, int Y, int k, int tile_rows, int wpl, int num_sms, int dense_pct,
+                      LocalPlan* lp) {
     if (k < 1 || k > kMaxTemporalSteps || W <= 0 || Y <= 0) return false;
     if (wpl == 0) wpl = 1;
     if ((wpl != 1 && wpl != 2 && wpl != 4) || W % wpl || k > kMaxKForWpl(wpl)) return false;
@@ -258,7 +409,17 @@ bool plan_local_tiles(int W, int Y, int k, int tile_rows, int wpl, int num_sms, 
     lp->tiles_x = p.nslices;
     lp->tiles_y = p.nbands;
     const int warps = (lp->tiles_x * lp->tiles_y + lp->segs - 1) / lp->segs;
-    lp->ctas = std::max(1, std::min(warps, num_sms * 24));
+    lp->ctas = std::max(1, (std::min(warps, num_sms * 24) + kTileWarps - 1) / kTileWarps);
+    lp->num_sms = num_sms;
+    // The dense form: the row-band plan at the kernel's lane width. Its
+    // lanes start at multiples of that width and tiles are 1, 2 or 4 words
+    // wide (or the whole row), so no lane straddles two change words.
+    // dense_pct 0 = the default share, above 100 = never.
+    const long long ntiles = (long long)lp->tiles_x * lp->tiles_y;
+    if (dense_pct == 0) dense_pct = GOL_LOCAL_DENSE_PCT;
+    lp->dense_min = INT_MAX;
+    if (dense_pct <= 100 && plan_rows(W, Y, k, 0, tracked_wpl(k), num_sms, &lp->dense))
+        lp->dense_min = (int)std::max(1LL, (ntiles * dense_pct + 99) / 100);
     return true;
 }
 
@@ -267,13 +428,22 @@ cudaError_t launch_local_pass(const uint32_t* src, uint32_t* dst, int W, int Y, 
                               cudaStream_t stream) {
     const RowsPlan& p = lp.rows;
     const int nwords = change_words(lp.tiles_x) * lp.tiles_y;
+    static const cudaError_t plan_attr = set_carveout(plan_tiles_kernel);
+    if (plan_attr != cudaSuccess) return plan_attr;
     plan_tiles_kernel<<<(nwords + kPlanThreads - 1) / kPlanThreads, kPlanThreads, 0, stream>>>(
         st.changed[parity ^ 1], st.changed[parity], lp.tiles_x, lp.tiles_y, st.list, st.count,
-        parity, st.census, st.census_cap, st.pass_no);
+        parity, st.census, st.census_cap, st.pass_no, lp.dense_min);
     cudaError_t e = cudaPeekAtLastError();
     if (e != cudaSuccess) return e;
+    if (lp.dense_min != INT_MAX) {
+        const RowsPlan& d = lp.dense;
+        RowsLaunch da{src, dst, W, Y, d.band, d.slice, d.halo, W};
+        TileTrack tt{st.changed[parity], p.band, p.slice, change_words(lp.tiles_x)};
+        e = dispatch_tracked<1>(k, da, tt, st.count + kDense0 + parity, d, lp.num_sms, stream);
+        if (e != cudaSuccess) return e;
+    }
     RowsLaunch a{src, dst, W, Y, p.band, p.slice, p.halo, W};
-    TileList t{st.list, st.count + parity, st.changed[parity], lp.tiles_x};
+    TileList t{st.list, st.count + parity, st.changed[parity], lp.tiles_x, st.count + kDense0 + parity};
     switch (p.wpl) {
         case 4: return dispatch_tiles<4, 1>(k, a, t, lp, stream);
         case 2: return dispatch_tiles<2, 1>(k, a, t, lp, stream);

@@ -137,6 +137,9 @@ struct TemporalRegs {
     uint32_t bank_cur, bank_oth;  // shared addresses of this lane's ring banks: steps 3t..3t+2
                                   // keep their rows in bank_cur (slots 3*(t%2) .. +2)
     uint32_t diff;                // change tracking: OR of (new ^ old) over stored words
+                                  // (per tile row: bit w = word w of the lane changed)
+    int flush_row;                // per tile row: the next row that closes a tile row,
+    int flush_ty;                 // ... and its tile row
     uint32_t ld[3][WPL];          // stage-0 rows, slot = step % 3
     uint32_t h0[K][3][WPL];       // stage g's horizontal sums, bit plane 0
     uint32_t h1[K][3][WPL];       //                            bit plane 1
@@ -163,6 +166,14 @@ __host__ __device__ constexpr int edge_last_side() { return K * 3 * ES; }
 // Words of a segmented warp's edge table for depth K.
 __host__ __device__ constexpr int seg_edge_words(int K) { return 2 * K * 3 * kSegEdgeStride; }
 
+// Per-tile change bits written by a dense pass (change tracking): tile
+// (tx, ty) covers words [tx * words, +words) of rows [ty * rows, +rows) and is
+// bit tx % 32 of changed[ty * cw + tx / 32].
+struct TileTrack {
+    uint32_t* changed;
+    int rows, words, cw;
+};
+
 struct TemporalCtx {
     const uint32_t* src;
     uint32_t* dst;
@@ -182,6 +193,9 @@ struct TemporalCtx {
     bool own;       // ... and inside this CTA's slice (not halo): stored
     int src_l, src_r;   // segmented warps: lanes holding the words left / right
     uint32_t wmask[4];  // per word of the lane: all ones inside the grid, else 0
+    TileTrack tt;       // per-tile change bits (TRACK == 2):
+    uint32_t tbit[4];   // the tile bit of each word of the lane in its change word
+    int tfw;            // that change word (-1 for lanes that store nothing)
 };
 
 // Word masks of a lane whose words start at `base` in a W-word row.
@@ -197,21 +211,38 @@ __device__ __forceinline__ void set_word_masks(TemporalCtx& c) {
 template <int WPL, bool SEG>
 __host__ __device__ constexpr int ring_slot_words() { return (SEG ? 32 : kTemporalMaxThreads) * WPL; }
 
+// Change tracking compares each output row with the same grid row before
+// the pass. CTA-wide tracked passes (TRACK 2) stage that row like stage 0's
+// rows, in a second ring right after the first (same slot numbering, this
+// byte offset): the copy for step j's output row (y0 - 3K + j) travels with
+// stage 0's row of step j. (Tile warps, TRACK 1, load it when storing:
+// their many resident warps hide the latency, and their shared memory
+// stays small.)
+template <int WPL, bool SEG>
+__host__ __device__ constexpr uint32_t old_ring_offset() { return kRowRing * ring_slot_words<WPL, SEG>() * 4u; }
+
 // Copies the row stage 0 consumes at step j (grid row y0 - K + j) to the
 // shared address `saddr` (this lane's words of a ring slot), zero-filled
-// outside the grid; commits it as one group.
-template <int WPL, int K>
+// outside the grid, with TRACK 2 the output row of step j to the old-row
+// ring; commits them as one group.
+template <int WPL, int K, int TRACK = 0, bool SEG = false>
 __device__ __forceinline__ void issue_row_at(const TemporalCtx& c, int j, uint32_t saddr) {
     const int r = c.y0 - K + j;
     const bool v = c.lane_ok && (unsigned)r < (unsigned)c.Y;
     const uint32_t* g = v ? c.src + (size_t)r * c.pitch + c.base : c.src;
     cp_async_words<WPL>(saddr, g, v);
+    if (TRACK == 2) {
+        const int ro = r - 2 * K;
+        const bool vo = c.lane_ok && (unsigned)ro < (unsigned)c.Y;
+        const uint32_t* go = vo ? c.src + (size_t)ro * c.pitch + c.base : c.src;
+        cp_async_words<WPL>(saddr + old_ring_offset<WPL, SEG>(), go, vo);
+    }
     cp_async_commit();
 }
 
-template <int WPL, int K>
+template <int WPL, int K, int TRACK = 0, bool SEG = false>
 __device__ __forceinline__ void issue_row(const TemporalCtx& c, int j, int slot) {
-    issue_row_at<WPL, K>(c, j, c.ring_saddr + (uint32_t)(slot * c.ring_stride) * 4u);
+    issue_row_at<WPL, K, TRACK, SEG>(c, j, c.ring_saddr + (uint32_t)(slot * c.ring_stride) * 4u);
 }
 
 // Reads this lane's words of a ring slot at a shared address.
@@ -227,6 +258,43 @@ __device__ __forceinline__ void lds_words_at(uint32_t saddr, uint32_t (&v)[WPL])
     }
 }
 
+// Tile bits of a lane's words for a per-tile-row tracked pass. A lane's
+// words never straddle two change words: they start at a multiple of WPL
+// and a change word spans 32 * tt.words words, both powers of two (or
+// tt.words = W, one tile column).
+template <int WPL>
+__device__ __forceinline__ void set_tile_bits(TemporalCtx& c) {
+    const int ts = c.tt.words;
+#pragma unroll
+    for (int w = 0; w < 4; ++w) c.tbit[w] = w < WPL ? 1u << (((c.base + w) / ts) & 31) : 0u;
+    c.tfw = c.own ? (c.base / ts) >> 5 : -1;
+}
+
+// Closes tile row s.flush_ty of a per-tile-row tracked pass: each lane turns
+// its changed-word bits into tile bits of its change word, a segmented OR
+// over the runs of lanes sharing a change word (shuffles by doubling: lanes
+// are in word order) gathers them, and the first lane of each run sets them
+// with one atomic. Every lane of the warp takes part.
+template <int WPL, int K>
+__device__ __forceinline__ void flush_tile_row(TemporalRegs<WPL, K>& s, const TemporalCtx& c) {
+    uint32_t m = 0u;
+#pragma unroll
+    for (int w = 0; w < WPL; ++w) m |= ((s.diff >> w) & 1u) ? c.tbit[w] : 0u;
+    const int fw = c.tfw;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t om = __shfl_down_sync(0xffffffffu, m, o);
+        const int ofw = __shfl_down_sync(0xffffffffu, fw, o);
+        if (c.lane + o < 32 && ofw == fw) m |= om;
+    }
+    const int pfw = __shfl_up_sync(0xffffffffu, fw, 1);
+    if (fw >= 0 && m != 0u && (c.lane == 0 || pfw != fw))
+        atomicOr(c.tt.changed + (size_t)s.flush_ty * c.tt.cw + fw, m);
+    s.diff = 0u;
+    s.flush_row = min(s.flush_row + c.tt.rows, c.y1 - 1);
+    s.flush_ty += 1;
+}
+
 // Step body. FAST = steady state: every stage active, every row inside the
 // grid, so no activity tests or row masks (the whole step is one basic
 // block and the K stages' independent chains interleave). LMASK forces the
@@ -240,7 +308,10 @@ __device__ __forceinline__ void lds_words_at(uint32_t saddr, uint32_t (&v)[WPL])
 // work, so those warps shuffle instead (no table, no barrier).
 // PART = rows padded to whole lanes: the last lane of a row may hold words
 // past W, masked word by word (otherwise a lane is all in or all out).
-template <int WPL, int K, int PH, bool FAST, bool LMASK, bool TRACK, bool SEG = false,
+// TRACK: 0 none; 1 = OR of (new ^ old) over every stored word (s.diff);
+// 2 = per-tile change bits, closed at each tile row's last row (CTA-wide
+// kernels only: every lane of a CTA is on the same row at a step).
+template <int WPL, int K, int PH, bool FAST, bool LMASK, int TRACK, bool SEG = false,
           bool PART = false>
 __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const TemporalCtx& c, int i) {
     constexpr int ES = SEG ? kSegEdgeStride : kEdgeStride;
@@ -248,6 +319,7 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
     constexpr int NEW3 = PH % 3;          // ring-of-3 slot written at this step
     constexpr int PREV3 = (PH + 2) % 3;   // ... written one step ago
     constexpr int OLD3 = (PH + 1) % 3;    // ... written two steps ago
+    constexpr uint32_t SB = ring_slot_words<WPL, SEG>() * 4u;   // bytes per ring slot
 
     // Stages run high to low so that stage g reads stage g-1's rows from the
     // previous steps before stage g-1 overwrites its ring slot.
@@ -300,9 +372,17 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
                     store_words<WPL>(c.dst + (size_t)row * c.pitch + c.base, res);
                     if (TRACK) {   // compare with the same row before the pass
                         uint32_t old[WPL];
-                        load_words<WPL>(c.src + (size_t)row * c.pitch + c.base, old);
+                        if (TRACK == 2)   // old-row ring slot i mod 6
+                            lds_words_at<WPL>(s.bank_cur + PH * SB + old_ring_offset<WPL, SEG>(), old);
+                        else
+                            load_words<WPL>(c.src + (size_t)row * c.pitch + c.base, old);
 #pragma unroll
-                        for (int w = 0; w < WPL; ++w) s.diff |= res[w] ^ old[w];
+                        for (int w = 0; w < WPL; ++w) {
+                            if (TRACK == 1)
+                                s.diff |= res[w] ^ old[w];
+                            else
+                                s.diff |= (res[w] != old[w] ? 1u : 0u) << w;
+                        }
                     }
                 }
             } else {
@@ -326,10 +406,9 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
     // Step i = 3t + PH reads row i+1 (slot (i+1) mod 6) and issues row i+5
     // (slot (i+5) mod 6, the one read two steps ago): with bank_cur holding
     // slots of steps 3t..3t+2, both are a bank plus a constant.
-    constexpr uint32_t SB = ring_slot_words<WPL, SEG>() * 4u;   // bytes per slot
     const uint32_t rd = PH == 0 ? s.bank_cur + SB : PH == 1 ? s.bank_cur + 2 * SB : s.bank_oth;
     const uint32_t wr = PH == 0 ? s.bank_oth + 2 * SB : PH == 1 ? s.bank_cur : s.bank_cur + SB;
-    issue_row_at<WPL, K>(c, i + kRowsInFlight, wr);
+    issue_row_at<WPL, K, TRACK, SEG>(c, i + kRowsInFlight, wr);
     cp_async_wait<kRowsInFlight - 1>();
     lds_words_at<WPL>(rd, s.ld[(PH + 1) % 3]);
     if (PH == 2) {   // steps 3t+3.. use the other bank
@@ -337,13 +416,16 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
         s.bank_cur = s.bank_oth;
         s.bank_oth = t;
     }
+    // Tile rows close after the step's stages (a branch there would split
+    // the step body, whose stages otherwise interleave as one block).
+    if (TRACK == 2 && c.y0 - 3 * K + i == s.flush_row) flush_tile_row<WPL, K>(s, c);
     if (!SEG)
         __syncthreads();
     else if (!SHFL)
         __syncwarp();
 }
 
-template <int WPL, int K, bool FAST, bool LMASK, bool TRACK, bool SEG = false, bool PART = false>
+template <int WPL, int K, bool FAST, bool LMASK, int TRACK, bool SEG = false, bool PART = false>
 __device__ __forceinline__ void temporal_steps(TemporalRegs<WPL, K>& s, const TemporalCtx& c,
                                                int i0, int i1) {
     // i0 is a multiple of 3; the bank of steps i0..i0+2 is (i0 / 3) % 2.
@@ -361,13 +443,15 @@ __device__ __forceinline__ void temporal_steps(TemporalRegs<WPL, K>& s, const Te
 // One tile of one pass: output rows [band*a.band, +a.band) of x-slice
 // `slice_idx`, K generations from a.src into a.dst. The CTA's shared memory
 // (temporal_smem_bytes) is reused from call to call: every copy is drained
-// before returning. With TRACK, returns this thread's OR of (new ^ old) over
-// the words it stored (0 when its part of the tile did not change).
-template <int WPL, int K, bool TRACK>
+// before returning. With TRACK 1, returns this thread's OR of (new ^ old)
+// over the words it stored (0 when its part of the tile did not change);
+// with TRACK 2, sets the change bits `tt` of the tiles it changed.
+template <int WPL, int K, int TRACK>
 __device__ __forceinline__ uint32_t band_tile(const RowsLaunch& a, int band, int slice_idx,
-                                              uint32_t* smem) {
+                                              uint32_t* smem, TileTrack tt = {}) {
     uint32_t* ring = smem;                    // kRowRing slots of ring_slot_words words
-    uint32_t* edges = smem + kRowRing * ring_slot_words<WPL, false>();
+    // (with TRACK 2, the old-row ring of the same size follows)
+    uint32_t* edges = smem + kRowRing * ring_slot_words<WPL, false>() * (TRACK == 2 ? 2 : 1);
     TemporalCtx c;
     c.src = a.src;
     c.dst = a.dst;
@@ -388,6 +472,8 @@ __device__ __forceinline__ uint32_t band_tile(const RowsLaunch& a, int band, int
     c.own = c.lane_ok && c.base >= xs && c.base < xs + a.slice;
     const bool all_lanes_ok = x0 >= 0 && x0 + (int)blockDim.x * WPL <= a.W;
     set_word_masks<WPL>(c);
+    c.tt = tt;
+    if (TRACK == 2) set_tile_bits<WPL>(c);
 
     for (int t = threadIdx.x; t < 2 * edge_last_side<K, kEdgeStride>(); t += blockDim.x) edges[t] = 0u;
 
@@ -405,10 +491,14 @@ __device__ __forceinline__ uint32_t band_tile(const RowsLaunch& a, int band, int
     c.ring = ring + threadIdx.x * WPL;
     c.ring_saddr = (uint32_t)__cvta_generic_to_shared(c.ring);
     c.ring_stride = ring_slot_words<WPL, false>();
-    for (int j = 0; j < kRowsInFlight; ++j) issue_row<WPL, K>(c, j, j);
+    for (int j = 0; j < kRowsInFlight; ++j) issue_row<WPL, K, TRACK>(c, j, j);
     cp_async_wait<kRowsInFlight - 1>();
     lds_words<WPL>(c.ring, s.ld[0]);
     s.diff = 0u;
+    if (TRACK == 2) {
+        s.flush_ty = c.y0 / tt.rows;
+        s.flush_row = min((s.flush_ty + 1) * tt.rows - 1, c.y1 - 1);
+    }
     __syncthreads();
 
     // Steps [f0, f1) run the steady-state body: all stages active (i >= 3K),
@@ -447,13 +537,15 @@ __global__ void __launch_bounds__(kTemporalMaxThreads, GOL_TEMPORAL_MIN_BLOCKS)
 rows_temporal_kernel(RowsLaunch a) {
     extern __shared__ __align__(16) uint32_t smem[];
     pdl_trigger_and_wait();
-    band_tile<WPL, K, false>(a, blockIdx.x, blockIdx.y, smem);
+    band_tile<WPL, K, 0>(a, blockIdx.x, blockIdx.y, smem);
 }
 
-// Shared memory a launch needs: the row ring and the edge table.
-__host__ __device__ inline size_t temporal_smem_bytes(int K, int threads, int wpl) {
+// Shared memory a launch needs: the row ring (two with change tracking:
+// rows and old rows) and the edge table.
+__host__ __device__ inline size_t temporal_smem_bytes(int K, int threads, int wpl, bool track = false) {
     (void)threads;   // the ring is sized for the widest CTA (compile-time slot offsets)
-    return ((size_t)kRowRing * kTemporalMaxThreads * wpl + (size_t)2 * edge_last_side<1, kEdgeStride>() * K) *
+    return ((size_t)kRowRing * kTemporalMaxThreads * wpl * (track ? 2 : 1) +
+            (size_t)2 * edge_last_side<1, kEdgeStride>() * K) *
            sizeof(uint32_t);
 }
 

@@ -64,6 +64,8 @@ class GolConfig(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("lane_words", ctypes.c_uint32),
         ("stream", ctypes.c_void_p),
+        ("dense_pct", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
     ]
 
 
@@ -208,6 +210,8 @@ class ExperimentParams:
     temporal_steps: int = 0               # k (0 = auto)
     lane_words: int = 0                   # 32-bit words per lane (0 = auto)
     tile_rows: int = 0                    # change-tracking tile height (0 = auto)
+    dense_pct: int = 0                    # change tracking: active-tile percentage from
+                                          # which a pass runs dense (0 = auto, > 100 never)
     algorithm: str = "auto"
     device: int = 0
     stream: int | None = None             # cudaStream_t as an integer
@@ -239,6 +243,7 @@ class GolB200:
         cfg.temporal_steps = int(p.temporal_steps)
         cfg.lane_words = int(p.lane_words)
         cfg.tile_rows = int(p.tile_rows)
+        cfg.dense_pct = int(p.dense_pct)
         cfg.thread_block_size = int(p.thread_block_size)
         cfg.max_runtime_seconds = int(p.max_runtime_seconds)
         cfg.device = int(p.device)

@@ -9,9 +9,11 @@ dense (default): k-generation passes of the row-band kernel on the dense
 benchmark input (Bernoulli(0.5), seed 42, from the reference's
 RandomOnesZerosDataLoader); each pass reads one device buffer and writes the
 other through gol_rows_pass; prints the mean per-launch time (CUDA events).
-local: the change-tracking engine on the sparse input (1 % of 64x64 slots
-Bernoulli(0.35), seed 42), --gens generations; prints the run time and the
-fraction of tiles computed.
+local: the change-tracking engine, --gens generations, on the sparse input
+(1 % of 64x64 slots Bernoulli(0.35), seed 42), the blinker lattice of the
+reference's always-changing loader (--input blinkers) or the dense benchmark
+input (--input random); prints the run time and the fraction of tiles
+computed. --dense-pct sets the active-tile share from which passes run dense.
 batch: the first --grids grids of the uneven batched workload (seed 42), one
 persistent launch after a warm-up launch; prints the launch time.
 """
@@ -39,6 +41,8 @@ def main() -> None:
     ap.add_argument("--gens", type=int, default=400)
     ap.add_argument("--grids", type=int, default=32)
     ap.add_argument("--tile-rows", type=int, default=0, help="change-tracking tile height (0 = auto)")
+    ap.add_argument("--input", choices=["sparse", "blinkers", "random"], default="sparse")
+    ap.add_argument("--dense-pct", type=int, default=0)
     a = ap.parse_args()
     if a.mode == "local":
         return run_local(a)
@@ -73,9 +77,14 @@ def main() -> None:
 def run_local(a) -> None:
     import time
     x, y = a.size, a.height or a.size
-    g = golb200.load_sparse_patches(x, y, seed=42)
+    if a.input == "blinkers":
+        g = golb200.load_always_changing(x, y)
+    elif a.input == "random":
+        g = golb200.load_random_ones_zeros(x, y, 42)
+    else:
+        g = golb200.load_sparse_patches(x, y, seed=42)
     with golb200.GolB200(grid_dimensions=(x, y), temporal_steps=a.k if a.k <= 16 else 8,
-                         algorithm="local", tile_rows=a.tile_rows) as alg:
+                         algorithm="local", tile_rows=a.tile_rows, dense_pct=a.dense_pct) as alg:
         alg.set_and_format_input_data(g)
         alg.initialize_data_structures()
         t0 = time.perf_counter()

@@ -79,8 +79,10 @@ def test_still_life_retires_all_tiles():
         alg.finalize_data_structures()
         assert np.array_equal(alg.fetch_result(), g)
     per = st["per_pass"]
-    assert st["passes"] == 100 and per[0] == st["tiles_per_pass"]   # first pass: every tile
-    assert int(per[1:].sum()) == 0          # nothing changed in it: nothing recomputed after
+    # The first pass computes every tile (dense), and so does the next: a pass
+    # after one with that many active tiles is planned without a tile list.
+    assert st["passes"] == 100 and list(per[:2]) == [st["tiles_per_pass"]] * 2
+    assert int(per[2:].sum()) == 0          # nothing changed: nothing recomputed after
 
 
 def test_oscillators_with_even_depth_and_odd_remainder():
@@ -126,3 +128,63 @@ def test_sparse_benchmark_size_local_equals_dense():
     assert np.array_equal(dense, local)
     ref = oracle.life_cells(g, 256)
     assert np.array_equal(run_local(g, 256, k=8), ref)
+
+
+@pytest.mark.parametrize("k", [5, 6])
+def test_published_loaders(k):
+    """The reference's change-tracking benchmark inputs: the blinker lattice
+    (period 2) and the all-dead grid. At an odd depth every tile of the
+    lattice changes every pass; at an even one every tile returns to its
+    input, so after the first two passes (dense: all tiles active, then
+    the pass planned without a list) only the top two tile rows are
+    computed again (the lattice's row-0 blinkers die against the dead
+    outside)."""
+    n = 4 * k + 1
+    blink = golb200.load_always_changing(1024, 512)
+    out, st = run_local(blink, n, k=k, stats=True)
+    assert np.array_equal(out, oracle.life_cells(blink, n))
+    full = st["passes"] * st["tiles_per_pass"]
+    if k % 2:
+        assert st["computed_tiles"] == full
+    else:
+        assert st["computed_tiles"] < 2.1 * st["tiles_per_pass"]
+    zeros = golb200.load_zeros(1024, 512)
+    out, st = run_local(zeros, n, k=k, stats=True)
+    assert not out.any()
+    assert st["computed_tiles"] <= 2 * st["tiles_per_pass"]
+
+
+@pytest.mark.parametrize("x,y,k,wpl,dense_pct", [
+    (1024, 512, 6, 0, 1), (1024, 512, 6, 0, 30), (1024, 512, 6, 0, 101),
+    (2048, 384, 4, 4, 20), (2048, 384, 5, 2, 20), (1152, 200, 3, 0, 15),
+    (32768, 192, 6, 0, 10),     # the dense form cut into x-slices
+    (64, 130, 5, 0, 50),        # one tile column
+])
+def test_dense_passes_hand_over(x, y, k, wpl, dense_pct):
+    """A settling random grid crosses the dense threshold: passes run dense
+    while many tiles are active and as tiles later, each mode planning from
+    the other's change bits. Results against the oracle for thresholds from
+    "almost always dense" (1 %) to "never" (above 100 %)."""
+    g = golb200.load_bernoulli(x, y, seed=x + y + k, density=0.3)
+    n = 40 * k + (k - 1)
+    out, st = run_local(g, n, k=k, stats=True, lane_words=wpl, dense_pct=dense_pct)
+    assert np.array_equal(out, oracle.life_cells(g, n)), (x, y, k, wpl, dense_pct)
+    full = st["passes"] * st["tiles_per_pass"]
+    assert st["computed_tiles"] <= full
+    if dense_pct == 1:      # a soup keeps more than 1 % of its tiles active
+        assert st["computed_tiles"] == full
+
+
+def test_dense_pass_census_counts_every_tile():
+    """A pass that runs dense computes, and records, every tile."""
+    g = golb200.load_bernoulli(1024, 512, seed=3, density=0.5)
+    out, st = run_local(g, 5 * 6, k=6, stats=True, dense_pct=1)
+    assert np.array_equal(out, oracle.life_cells(g, 30))
+    per = None
+    with golb200.GolB200(grid_dimensions=(1024, 512), temporal_steps=6, algorithm="local",
+                         dense_pct=1) as alg:
+        alg.set_and_format_input_data(g)
+        alg.initialize_data_structures()
+        alg.run(30)
+        per = alg.local_stats(max_entries=8)["per_pass"]
+    assert list(per) == [st["tiles_per_pass"]] * 5
