@@ -387,7 +387,8 @@ def bench_published(stream, device) -> dict:
     generations, change tracking beside the dense engine. The blinker
     lattice has period 2, so at an even pass depth every tile is back to its
     input after each pass and change tracking skips it; an odd depth (5)
-    keeps every tile changing and measures the full-work case."""
+    keeps every tile changing and measures the full-work case. Then change
+    tracking on the dense benchmark's own random grid."""
     import golb200
     size, gens = SIZE, 4096
     out = {"workload": f"{size}x{size}, {gens} generations: zeros and always-changing loaders",
@@ -409,6 +410,14 @@ def bench_published(stream, device) -> dict:
         out[f"always_changing_value_dense_k{k}"], _, w = _engine_rate(stream, device, blink, gens,
                                                                       temporal_steps=k)
         out[f"always_changing_dense_k{k}_equals_local"] = bool(np.array_equal(w, ref))
+    # The dense benchmark's own input (Bernoulli(0.5) seed 42) with change
+    # tracking: every tile active at first, about half of them by the end.
+    soup = golb200.load_random_ones_zeros(size, size, SEED)
+    out["random_value_local_k6"], st, w = _engine_rate(stream, device, soup, gens, algorithm="local",
+                                                       temporal_steps=6)
+    out["random_computed_tile_fraction_k6"] = _tile_fraction(st)
+    _, _, wd = _engine_rate(stream, device, soup, gens, temporal_steps=4)
+    out["random_local_equals_dense"] = bool(np.array_equal(w, wd))
     return out
 
 

@@ -83,7 +83,7 @@ typedef struct gol_config {
     uint32_t dense_pct;             /* change tracking: a pass with at least this
                                        percentage of its tiles active runs the
                                        dense kernel instead of the tile kernel
-                                       (0 = auto, 6; above 100 = never)         */
+                                       (0 = auto, 10; above 100 = never)        */
     uint32_t reserved;              /* zero                                      */
 } gol_config;
 

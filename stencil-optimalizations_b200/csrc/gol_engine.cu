@@ -385,7 +385,11 @@ int gol_init(gol_engine* e) {
         }
     }
     int k = (int)e->cfg.temporal_steps;
-    if (k <= 0) k = 4;
+    // Auto depth: 4 (the dense optimum on B200); 6 with change tracking,
+    // where a pass of k generations sees oscillators whose period divides k
+    // as still (period 2 blinkers and period 3 pulsars are most of the ash
+    // a random grid settles into).
+    if (k <= 0) k = e->cfg.algorithm == GOL_ALG_LOCAL ? 6 : 4;
     const int sms = golb200::device_sm_count(e->cfg.device);
     if (!golb200::plan_rows(e->W, e->Y, k, (int)e->cfg.thread_block_size,
                             (int)e->cfg.lane_words, sms, &e->plan))
