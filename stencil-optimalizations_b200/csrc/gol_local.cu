@@ -49,9 +49,9 @@
 #ifndef GOL_LOCAL_CARVEOUT
 // Shared-memory carveout (percent of the maximum) preferred by all three
 // kernels of a pass, so that the SMs keep one L1/shared split from kernel to
-// kernel; -1 leaves the driver's choice. On the sparse 16384^2 workload
-// (k = 6) the driver's choice ran at 79 T cell-updates/s, a common 100 %
-// at 77.6 T.
+// kernel; -1 leaves the CUDA driver's choice. On the sparse 16384^2
+// workload (k = 6) the CUDA driver's choice ran at 79 T cell-updates/s, a
+// common 100 % at 77.6 T.
 #define GOL_LOCAL_CARVEOUT -1
 #endif
 
