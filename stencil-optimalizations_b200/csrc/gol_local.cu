@@ -85,8 +85,7 @@ static_assert(kDense0 + 2 <= kLocalCountWords, "plan words");
 // three flag rows around it, each shifted one bit left and right (with the
 // carry bits of the neighbouring words). Active tiles are appended to
 // `list` in order a warp at a time (scan of the per-thread counts, one
-// atomic per warp, so a warp of the tile kernel gets neighbouring tiles;
-// the warp then writes its entries together, in consecutive slots).
+// atomic per warp, so a warp of the tile kernel gets neighbouring tiles).
 // counts[parity] is this pass's list length (zero on entry); counts[parity
 // ^ 1] is zeroed for the next pass; the last CTA decides the pass's form
 // and records the census (tiles computed: all of them in a dense pass).
@@ -134,15 +133,15 @@ plan_tiles_kernel(const uint32_t* __restrict__ prev, uint32_t* __restrict__ clea
     int base = 0;
     if (lane == 31 && wtotal) base = atomicAdd(counts + parity, wtotal);
     base = __shfl_sync(0xffffffffu, base, 31) + incl - n;
-    if (!skip_list && wtotal) {
-        // Lane j's tiles, written by the lanes of their bits: consecutive
-        // set bits go to consecutive slots. Only lanes with tiles take a turn.
-        for (uint32_t busy = __ballot_sync(0xffffffffu, act != 0u); busy; busy &= busy - 1u) {
-            const int j = __ffs((int)busy) - 1;
-            const uint32_t aj = __shfl_sync(0xffffffffu, act, j);
-            const int bj = __shfl_sync(0xffffffffu, base, j);
-            const int tj = __shfl_sync(0xffffffffu, ty * tiles_x + 32 * w, j);
-            if ((aj >> lane) & 1u) list[bj + __popc(aj & ((1u << lane) - 1u))] = tj + lane;
+    // Each lane writes its own tiles, all lanes at once. (A warp writing the
+    // lanes' runs one after another, coalesced, cost the plan kernel 1.2 us
+    // more per pass on the sparse 16384^2 workload; big lists, where it would
+    // pay, come only after dense-level passes, which skip the list.)
+    if (!skip_list) {
+        while (act) {
+            const int b = __ffs((int)act) - 1;
+            act &= act - 1u;
+            list[base++] = ty * tiles_x + 32 * w + b;
         }
     }
 
