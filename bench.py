@@ -75,7 +75,7 @@ def parse_args():
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the sparse, batched and serving measurements")
-    ap.add_argument("--only", choices=["sparse", "published", "batched", "serving"],
+    ap.add_argument("--only", choices=["sparse", "published", "batched", "serving", "hbm"],
                     help="measure just that configuration and print it")
     return ap.parse_args()
 
@@ -309,14 +309,15 @@ def measured_peaks() -> dict:
         return {}
 
 
-def ncu_traffic(k: int, wpl: int) -> float | None:
-    """DRAM bytes per launch of the pass kernel from a committed ncu summary."""
+def ncu_traffic(kernel: str, size: int = SIZE) -> float | None:
+    """DRAM bytes per launch of a pass kernel from a committed ncu summary
+    (profiles/ncu_traffic.json, keyed "kernel@size")."""
     try:
         with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
             d = json.load(f)
     except (OSError, ValueError):
         return None
-    ent = d.get(f"rows_temporal_kernel<{wpl},{k}>@{SIZE}")
+    ent = d.get(f"{kernel}@{size}")
     return None if ent is None else float(ent["dram_bytes_per_launch"])
 
 
@@ -377,6 +378,9 @@ def bench_sparse(stream, device) -> dict:
     out["computed_tile_fraction"] = _tile_fraction(st)
     out["value_dense"], _, dense = _engine_rate(stream, device, g, gens, temporal_steps=4)
     out["local_equals_dense"] = bool(np.array_equal(local, dense))
+    import oracle
+    want = oracle.life_rows(oracle.pack_rows(g, 64), size, gens, 64)
+    out["bit_exact_vs_oracle_full_length"] = bool(np.array_equal(local, want))
     return out
 
 
@@ -421,15 +425,135 @@ def bench_published(stream, device) -> dict:
     return out
 
 
+HBM_SIZE = 32768
+HBM_SWEEP_K = (1, 2, 3, 4, 5, 6, 8)
+
+
+def bench_hbm(stream, device) -> dict:
+    """The dense engine on a grid larger than L2: 32768^2 Bernoulli(0.5) seed
+    42 (128 MiB per buffer; the two buffers are 268 MB against the 126 MB
+    L2), depth swept 1..8. Per depth: cell-updates/s, the algorithmic HBM
+    rate (grid read and written once per pass) against the measured HBM
+    peak, and the integer view against the live LOP3 probe. Depths agree
+    with each other and k = 1 with the oracle."""
+    import torch
+
+    import golb200
+    import oracle
+    size, gens = HBM_SIZE, 384
+    cells = golb200.load_random_ones_zeros(size, size, SEED)
+    peaks = measured_peaks()
+    hbm_peak = peaks.get("hbm_gbs") or 6650.0
+    int_peak = golb200.probe_int_peak(stream.cuda_stream)
+    grid_bytes = size * size // 8
+    rows = {}
+    results = {}
+    for k in HBM_SWEEP_K:
+        e = golb200.GolB200(grid_dimensions=(size, size), state_bits_count=64, temporal_steps=k,
+                            device=device, stream=stream.cuda_stream)
+        e.set_and_format_input_data(cells)
+        e.initialize_data_structures()
+        e.run(gens)           # warm-up (graph capture)
+        e.sync()
+        ms = min(_events_ms(stream, lambda: e.run(gens), e.sync) for _ in range(3))
+        passes = gens // k + (1 if gens % k else 0)
+        pass_ms = ms / passes
+        plan = e.plan()
+        e.close()
+        cu = size * size * gens / (ms * 1e-3)
+        gbs = 2 * grid_bytes / (pass_ms * 1e-3) / 1e9
+        rows[str(k)] = {"value": cu / 1e9, "pass_us": pass_ms * 1e3, "hbm_gbs": gbs,
+                        "hbm_frac": gbs / hbm_peak,
+                        "int_frac": cu * ALG_INT_OPS_PER_CELL / int_peak,
+                        "words_per_lane": plan["words_per_lane"], "band_rows": plan["band_rows"],
+                        "kernel": "rows_stream_kernel" if k == 1 else "rows_temporal_kernel"}
+    # parity: every depth gives the k = 1 grid after 96 generations, and
+    # k = 1 equals the oracle
+    chk = 96
+    for k in HBM_SWEEP_K:
+        e = golb200.GolB200(grid_dimensions=(size, size), state_bits_count=64, temporal_steps=k,
+                            device=device, stream=stream.cuda_stream)
+        e.set_and_format_input_data(cells)
+        e.initialize_data_structures()
+        e.run(chk)
+        e.finalize_data_structures()
+        results[k] = e.fetch_words(64)
+        e.close()
+    want = oracle.life_rows(oracle.pack_rows(cells, 64), size, chk, 64)
+    del cells
+    torch.cuda.synchronize()
+    return {"workload": f"dense {size}x{size} Bernoulli(0.5) seed {SEED}, 64-bit rows, {gens} "
+                        f"generations per timing (min of 3)", "unit": UNIT,
+            "hbm_peak_gbs": hbm_peak, "int_peak_lane_ops": int_peak, "per_k": rows,
+            "k1_bit_exact_vs_oracle_96_gens": bool(np.array_equal(results[1], want)),
+            "all_depths_equal_96_gens": all(np.array_equal(results[k], results[1]) for k in results)}
+
+
+def _plain_graphs_multistream(work, inputs, device, nstreams: int = 8) -> tuple:
+    """The fair plain baseline: every grid through the one-grid engine
+    (gol_run: its own plan, CUDA graphs of 16 passes), grids dealt round-robin
+    to `nstreams` streams so independent grids overlap on the device. Returns
+    (ms of the timed run, the engines' results as 64-bit row words)."""
+    import torch
+
+    import golb200
+    streams = [torch.cuda.Stream(device=device) for _ in range(nstreams)]
+    master = torch.cuda.Stream(device=device)
+    engines = []
+    for i, (d, w) in enumerate(zip(work, inputs)):
+        e = golb200.GolB200(grid_dimensions=(d["x"], d["y"]), state_bits_count=64, temporal_steps=4,
+                            device=device, stream=streams[i % nstreams].cuda_stream)
+        engines.append(e)
+
+    def load():
+        for e, w in zip(engines, inputs):
+            e.set_input_words(w, 64)
+            e.initialize_data_structures()
+        torch.cuda.synchronize()
+
+    def run_all() -> float:
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(master)
+        for st in streams:
+            st.wait_event(a)
+        for e, d in zip(engines, work):
+            e.run(d["gens"])
+        for st in streams:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            master.wait_event(ev)
+        b.record(master)
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    load()
+    run_all()                                   # warm-up: captures every engine's graphs
+    for e in engines:
+        e.finalize_data_structures()
+    load()
+    ms = run_all()
+    out = []
+    for e in engines:
+        e.finalize_data_structures()
+        out.append(e.fetch_words(64))
+        e.close()
+    return ms, out
+
+
 def bench_batched(stream, device, n: int = 512, seed: int = SEED) -> dict:
     """512 grids, sides log-uniform [256, 4096] (multiples of 64), density
-    U[0.2, 0.5], generations log-uniform [64, 4096]: one persistent launch
-    vs one launch per pass per grid on the same GPU."""
+    U[0.2, 0.5], generations log-uniform [64, 4096]: one persistent launch,
+    against (1) one launch per pass per grid on one stream and (2) every grid
+    through the one-grid engine's graph-chunked gol_run over 8 streams; every
+    grid's batched result checked against the oracle."""
     import concurrent.futures as cf
 
     import golb200
+    import oracle
     work = golb200.workload_uneven(seed, n, 256, 4096, 64, (0.2, 0.5), (64, 4096))
     b = golb200.GolBatch(device=device, stream=stream.cuda_stream)
+    inputs = []
     with cf.ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as pool:
         for i in range(0, n, 32):
             chunk = work[i:i + 32]
@@ -437,26 +561,44 @@ def bench_batched(stream, device, n: int = 512, seed: int = SEED) -> dict:
                                                                    d["density"]), chunk))
             for d, c in zip(chunk, grids):
                 b.add(c, d["gens"])
+                inputs.append(oracle.pack_rows(c, 64))
     b.upload()
     info = b.info()
     b.run()
     b.sync()                                        # warm-up (and graph capture)
     batched = [_events_ms(stream, b.run, b.sync) for _ in range(3)]
-    sample = [b.fetch(i) for i in range(0, n, 64)]
+    results = [oracle.pack_rows(b.fetch(i), 64) for i in range(n)]
     b.run_plain(4)
     b.sync()
     plain = [_events_ms(stream, lambda: b.run_plain(4), b.sync) for _ in range(2)]
-    same = all(np.array_equal(b.fetch(i), s) for i, s in zip(range(0, n, 64), sample))
+    same = all(np.array_equal(oracle.pack_rows(b.fetch(i), 64), results[i]) for i in range(0, n, 64))
     b.close()
+    ms_graphs, graph_results = _plain_graphs_multistream(work, inputs, device)
+    graphs_same = all(np.array_equal(graph_results[i], results[i]) for i in range(n))
+
+    def check(i):
+        d = work[i]
+        want = oracle.life_rows(inputs[i], d["x"], d["gens"], 64,
+                                threads=1 if inputs[i].size < (1 << 16) else 4)
+        return bool(np.array_equal(results[i], want))
+    with cf.ThreadPoolExecutor(max_workers=max(1, (os.cpu_count() or 2) // 2)) as pool:
+        ok = list(pool.map(check, range(n)))
     cu = info["cell_updates"]
     vb = cu / (min(batched) * 1e-3) / 1e9
     vp = cu / (min(plain) * 1e-3) / 1e9
+    vg = cu / (ms_graphs * 1e-3) / 1e9
     return {"workload": f"{n} grids, sides log-uniform [256, 4096] x64, density U[0.2, 0.5], "
                         f"generations log-uniform [64, 4096], seed {seed}",
             "cell_updates": cu, "work_items": info["items"], "unit": UNIT,
-            "value_batched": vb, "value_plain_per_grid": vp, "speedup": vb / vp,
-            "ms_batched": min(batched), "ms_plain": min(plain),
-            "batched_equals_plain_on_sample": same}
+            "value_batched": vb, "ms_batched": min(batched),
+            "value_plain_per_grid": vp, "ms_plain": min(plain), "speedup": vb / vp,
+            "value_plain_graphs_multistream": vg, "ms_plain_graphs_multistream": ms_graphs,
+            "speedup_vs_graphs_multistream": vb / vg,
+            "plain_graphs_multistream": "each grid through gol_run (its own plan, CUDA graphs "
+                                        "of 16 passes), 8 streams, one engine per grid",
+            "batched_equals_plain_on_sample": same,
+            "batched_equals_graphs_multistream_all": graphs_same,
+            "batched_all_equal_oracle": all(ok), "grids_checked_vs_oracle": len(ok)}
 
 
 def bench_serving(device) -> dict:
@@ -532,17 +674,16 @@ def run_ours(args, d: Dist) -> None:
         dist.broadcast(t, 0)
         best_k = int(t.item())
 
-    # -- bit-exactness of the benchmark configuration ------------------------
+    # -- bit-exactness of the benchmark configuration at its full length ------
     bit_exact = None
     if not args.no_check and d.rank == 0:
         import oracle
-        chk = 256
         e = make_engine(best_k)
-        e.run(chk)
+        e.run(gens)
         e.finalize_data_structures()
         got = e.fetch_words(64)
         e.close()
-        want = oracle.life_rows(oracle.pack_rows(cells, 64), size, chk, 64)
+        want = oracle.life_rows(oracle.pack_rows(cells, 64), size, gens, 64)
         bit_exact = bool(np.array_equal(got, want))
 
     # -- headline: device-resident timed steps -------------------------------
@@ -569,22 +710,12 @@ def run_ours(args, d: Dist) -> None:
     clk = clocks.stop()
     total_ms = d.max(sum(step_ms))
     value = replica_throughput(d.world, cell_updates * args.steps, total_ms * 1e-3) / 1e9
-    passes = gens // best_k + (1 if gens % best_k else 0)
 
-    # -- dominant kernel: per-launch duration (one pass of k generations) ----
-    src = e.device_grid_ptr()
-    scratch = torch.empty(size * size // 32, dtype=torch.int32, device=dev)
-    evs = []
-    for i in range(24):
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        golb200.rows_pass(src, scratch.data_ptr(), size, size, best_k, plan["band_rows"],
-                          stream.cuda_stream)
-        b.record(stream)
-        evs.append((a, b))
-    torch.cuda.synchronize()
-    launch_ms = statistics.mean(a.elapsed_time(b) for a, b in evs[4:])
+    # -- dominant kernel: its in-step duration (one pass of k generations) ---
+    # Every launch of the timed steps is this kernel (the step is one graph of
+    # passes), so the per-pass time is the step's device time over its passes.
+    passes = gens // best_k + (1 if gens % best_k else 0)
+    launch_ms = total_ms / args.steps / passes
     grid_bytes = size * size // 8
     alg_bytes = 2 * grid_bytes                       # read once + write once per pass
     achieved_gbs = alg_bytes / (launch_ms * 1e-3) / 1e9
@@ -596,6 +727,27 @@ def run_ours(args, d: Dist) -> None:
     pass_cell_updates = size * size * best_k
     int_achieved = pass_cell_updates * ALG_INT_OPS_PER_CELL / (launch_ms * 1e-3)
     e.close()
+    kernel = (f"rows_stream_kernel<{plan['words_per_lane']}>" if best_k == 1 else
+              f"rows_temporal_kernel<{plan['words_per_lane']},{best_k}>")
+    hbm_view = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved_gbs / hbm_peak, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": alg_bytes,
+                "note": "bytes = grid read once + written once per k-generation pass "
+                        "(0.25/k B per cell-update)"}
+    int_view = {"bound": "alu", "achieved": int_achieved / 1e12, "peak": int_peak / 1e12,
+                "unit": "Tlane-ops/s", "frac": int_achieved / int_peak,
+                "peak_source": "live LOP3 probe (gol_probe_int_peak): 64 lanes/clk/SM",
+                "ops_per_cell_update": ALG_INT_OPS_PER_CELL,
+                "note": "algorithmic ops = the reference full adder's 33 word-ops per 64 cells"}
+    # One generation per pass is HBM-bound; deeper passes are bound by the
+    # integer (ALU) pipe (ncu: ALU 84 %, DRAM 12 % at k = 4).
+    primary, secondary = (hbm_view, int_view) if best_k == 1 else (int_view, hbm_view)
+    roofline = dict(primary)
+    roofline.update({"traffic": ncu_traffic(kernel, size), "kernel": kernel,
+                     "launch_ms": launch_ms,
+                     "launch_ms_source": "in-step: ms_per_step / passes per step (CUDA events "
+                                         "around the captured graphs of the timed steps)",
+                     "other_view": secondary})
 
     # -- 32-bit variant at 8192^2 (reported beside the headline) -------------
     var = None
@@ -610,13 +762,27 @@ def run_ours(args, d: Dist) -> None:
             ve.initialize_data_structures()
             timed_run(ve, 256)
             ms = timed_run(ve, gens)
+            ve_plan = ve.plan()
             ve.close()
             r = vsize * vsize * gens / (ms * 1e-3) / 1e9
             if best is None or r > best[1]:
-                best = (k, r)
+                best = (k, r, ve_plan)
         var = {"workload": f"dense {vsize}x{vsize} Bernoulli(0.5) seed {SEED}, 32-bit rows, "
                            f"{gens} generations", "value": best[1], "unit": UNIT,
-               "temporal_steps": best[0]}
+               "temporal_steps": best[0], "plan": best[2]}
+        if not args.no_check:
+            import oracle
+            ve = golb200.GolB200(grid_dimensions=(vsize, vsize), state_bits_count=32,
+                                 temporal_steps=best[0], device=d.local_rank,
+                                 stream=stream.cuda_stream)
+            ve.set_and_format_input_data(vcells)
+            ve.initialize_data_structures()
+            ve.run(gens)
+            ve.finalize_data_structures()
+            got = ve.fetch_words(32)
+            ve.close()
+            want = oracle.life_rows(oracle.pack_rows(vcells, 32), vsize, gens, 32)
+            var["bit_exact_vs_oracle_full_length"] = bool(np.array_equal(got, want))
 
     # -- e2e through the public API with host buffers -------------------------
     e2e_times, phases = [], {"set_input": [], "init": [], "run": [], "finalize": [], "fetch": []}
@@ -650,8 +816,9 @@ def run_ours(args, d: Dist) -> None:
     if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(cells)
 
-    sparse = published = batched = serving = None
+    sparse = published = batched = serving = hbm = None
     if d.rank == 0 and d.world == 1 and not args.no_extras:
+        hbm = run_extra("hbm")
         sparse = run_extra("sparse")
         published = run_extra("published")
         batched = run_extra("batched")
@@ -672,26 +839,11 @@ def run_ours(args, d: Dist) -> None:
                 "l2": "flushed between timed steps (256 MiB write, outside the events)",
                 "parallelism": f"replicas x{d.world}" if d.world > 1 else "single GPU",
             },
-            "bit_exact_vs_oracle_256_gens": bit_exact,
+            "bit_exact_vs_oracle_full_length": bit_exact,
             "k_sweep": {str(k): round(v, 1) for k, v in sweep.items()},
-            "roofline": {
-                "bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved_gbs / hbm_peak, "traffic": ncu_traffic(best_k, plan["words_per_lane"]),
-                "peak_source": peak_src,
-                "kernel": f"rows_temporal_kernel<{plan['words_per_lane']},{best_k}>",
-                "launch_ms": launch_ms,
-                "algorithmic_bytes_per_launch": alg_bytes,
-                "note": "bytes = grid read once + written once per k-generation pass "
-                        "(0.25/k B per cell-update)",
-            },
-            "int_roofline": {
-                "achieved": int_achieved, "peak": int_peak, "unit": "lane-ops/s",
-                "frac": int_achieved / int_peak,
-                "ops_per_cell_update": ALG_INT_OPS_PER_CELL,
-                "note": "algorithmic ops = the reference full-adder's 33 word-ops per 64 cells; "
-                        "peak = live LOP3 probe (gol_probe_int_peak)",
-            },
+            "roofline": roofline,
             "variant_8192_32bit": var,
+            "larger_than_l2_32768": hbm,
             "sparse_settling": sparse,
             "published_workloads": published,
             "batched_uneven": batched,
@@ -722,7 +874,8 @@ def main():
         fn = {"sparse": lambda: bench_sparse(s, d.local_rank),
               "published": lambda: bench_published(s, d.local_rank),
               "batched": lambda: bench_batched(s, d.local_rank),
-              "serving": lambda: bench_serving(d.local_rank)}[args.only]
+              "serving": lambda: bench_serving(d.local_rank),
+              "hbm": lambda: bench_hbm(s, d.local_rank)}[args.only]
         print(json.dumps({args.only: fn()}), flush=True)
         return
     if d.world > 1:

@@ -273,7 +273,10 @@ int gol_rows_pass_ex(const void* d_src, void* d_dst, uint64_t x, uint64_t y, uin
  * with GOL_E_UNSUPPORTED. Every GPU that loads the library holds that array
  * until the process exits. The first call on a device looks up the array's
  * device address (cudaGetSymbolAddress, with that device current); make that
- * first call before any stream capture. All calls share the one array:
+ * first call before any stream capture. That address is cached for the life
+ * of the process: it becomes stale if the caller resets the device
+ * (cudaDeviceReset), after which this entry point must not be called on that
+ * device again. All calls share the one array:
  * calls that overlap on the GPU (other streams, other threads) race and must
  * be serialised by the caller. k = 0 picks 4. Asynchronous on `stream`. */
 #define GOL_NOALLOC_MAX_BYTES (32u << 20)

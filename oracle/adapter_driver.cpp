@@ -8,7 +8,10 @@
 //
 // Built by `make -C oracle adapter` from the reference sources in place, into
 // oracle/_ref/adapter_driver. Usage:
-//   adapter_driver X Y ITERATIONS SEED [temporal_steps] [local]
+//   adapter_driver X Y ITERATIONS SEED [temporal_steps] [local|k1]
+// `k1` registers the adapter with its depth forced to one generation per
+// pass (GolB200Algorithm<char, GOL_ALG_AUTO, 1>) and checks that the engine
+// ran at that depth.
 // Exit status 0 iff the engine's grid equals the reference's.
 #include <cstdio>
 #include <cstdlib>
@@ -65,6 +68,22 @@ int main(int argc, char** argv) {
         if (argc > 6 && std::strcmp(argv[6], "local") == 0) {
             golb200::GolB200Algorithm<char, GOL_ALG_LOCAL> alg;
             for (int round = 0; round < 2; ++round) got = perform(alg, p, input, round == 1);
+        } else if (argc > 6 && std::strcmp(argv[6], "k1") == 0) {
+            golb200::GolB200Algorithm<char, GOL_ALG_AUTO, 1> alg;
+            for (int round = 0; round < 2; ++round) {
+                got = perform(alg, p, input, round == 1);
+                // gol_plan reports the depth of an initialised engine: run one
+                // more generation-free round to read it back
+                alg.set_and_format_input_data(input);
+                alg.initialize_data_structures();
+                uint32_t depth = 0;
+                if (gol_plan(alg.engine(), &depth, nullptr, nullptr) != GOL_OK || depth != 1) {
+                    std::fprintf(stderr, "engine depth %u, expected 1\n", depth);
+                    return 4;
+                }
+                alg.finalize_data_structures();
+                std::printf("engine depth: %u generation per pass\n", depth);
+            }
         } else {
             golb200::GolB200Algorithm<char> alg;
             for (int round = 0; round < 2; ++round) got = perform(alg, p, input, round == 1);

@@ -314,50 +314,77 @@ int gor_unpack_layout(int layout, int word_bits, const void* words, uint64_t x, 
         WT is4 = (WT)~s0 & (WT)~s1 & s2;                                                     \
         return is3 | (is4 & cc);                                                             \
     }                                                                                        \
-    static void gor_rows_##BITS(const WT* src, WT* dst, int64_t wx, int64_t y, int64_t y0,  \
-                                int64_t y1) {                                                \
+    /* Rows [y0, y1): words outside the grid read as 0. `zero` is a row of  \
+     * wx zero words standing in for the rows above and below the grid, so   \
+     * the inner words need no bounds tests (only the first and last word of  \
+     * a row look past its ends).                                            */ \
+    __attribute__((target_clones("avx2", "default")))                                      \
+    static void gor_rows_##BITS(const WT* src, WT* dst, const WT* zero, int64_t wx, int64_t y, \
+                                int64_t y0, int64_t y1) {                                    \
         for (int64_t yy = y0; yy < y1; ++yy) {                                               \
-            const WT* up = (yy > 0) ? src + (yy - 1) * wx : NULL;                            \
+            const WT* up = (yy > 0) ? src + (yy - 1) * wx : zero;                            \
             const WT* mid = src + yy * wx;                                                   \
-            const WT* dn = (yy + 1 < y) ? src + (yy + 1) * wx : NULL;                        \
-            for (int64_t xw = 0; xw < wx; ++xw) {                                            \
-                WT lt = 0, ct = 0, rt = 0, lc = 0, cc, rc = 0, lb = 0, cb = 0, rb = 0;       \
-                cc = mid[xw];                                                                \
-                if (xw > 0) lc = mid[xw - 1];                                                \
-                if (xw + 1 < wx) rc = mid[xw + 1];                                           \
-                if (up) {                                                                    \
-                    ct = up[xw];                                                             \
-                    if (xw > 0) lt = up[xw - 1];                                             \
-                    if (xw + 1 < wx) rt = up[xw + 1];                                        \
-                }                                                                            \
-                if (dn) {                                                                    \
-                    cb = dn[xw];                                                             \
-                    if (xw > 0) lb = dn[xw - 1];                                             \
-                    if (xw + 1 < wx) rb = dn[xw + 1];                                        \
-                }                                                                            \
-                dst[yy * wx + xw] = gor_word_##BITS(lt, ct, rt, lc, cc, rc, lb, cb, rb);     \
+            const WT* dn = (yy + 1 < y) ? src + (yy + 1) * wx : zero;                        \
+            WT* out = dst + yy * wx;                                                         \
+            if (wx == 1) {                                                                   \
+                out[0] = gor_word_##BITS(0, up[0], 0, 0, mid[0], 0, 0, dn[0], 0);            \
+                continue;                                                                    \
             }                                                                                \
+            out[0] = gor_word_##BITS(0, up[0], up[1], 0, mid[0], mid[1], 0, dn[0], dn[1]);   \
+            for (int64_t xw = 1; xw + 1 < wx; ++xw)                                          \
+                out[xw] = gor_word_##BITS(up[xw - 1], up[xw], up[xw + 1], mid[xw - 1],       \
+                                          mid[xw], mid[xw + 1], dn[xw - 1], dn[xw],          \
+                                          dn[xw + 1]);                                       \
+            const int64_t e = wx - 1;                                                        \
+            out[e] = gor_word_##BITS(up[e - 1], up[e], 0, mid[e - 1], mid[e], 0, dn[e - 1],  \
+                                     dn[e], 0);                                              \
         }                                                                                    \
     }
 
 GOR_DEFINE_ROWS(uint64_t, 64)
 GOR_DEFINE_ROWS(uint32_t, 32)
 
-/* Worker team: each generation splits the rows into `threads` contiguous
- * ranges; a generation finishes (join) before the next one starts. */
+/* Worker team: the rows are split into `threads` contiguous ranges, one per
+ * thread, for the whole run; a barrier separates the generations (every
+ * thread reads the previous generation's buffer, then writes its own rows of
+ * the next one). Started threads wait at a gate until the whole team exists
+ * (or give up with it, if a thread could not be created). */
+typedef struct {
+    pthread_mutex_t mu;
+    pthread_cond_t cv;
+    int state; /* 0 wait, 1 go, -1 abandon */
+} gor_gate;
+
 typedef struct {
     int word_bits;
-    const void* src;
-    void* dst;
+    void* buf[2];
+    const void* zero; /* a row of wx zero words */
     int64_t wx, y, y0, y1;
+    uint64_t iters;
+    pthread_barrier_t* bar;
+    gor_gate* gate;
 } gor_job;
 
 static void* gor_job_run(void* arg) {
     gor_job* j = (gor_job*)arg;
-    if (j->word_bits == 64)
-        gor_rows_64((const uint64_t*)j->src, (uint64_t*)j->dst, j->wx, j->y, j->y0, j->y1);
-    else
-        gor_rows_32((const uint32_t*)j->src, (uint32_t*)j->dst, j->wx, j->y, j->y0, j->y1);
+    if (j->gate) {
+        pthread_mutex_lock(&j->gate->mu);
+        while (j->gate->state == 0) pthread_cond_wait(&j->gate->cv, &j->gate->mu);
+        const int go = j->gate->state == 1;
+        pthread_mutex_unlock(&j->gate->mu);
+        if (!go) return NULL;
+    }
+    for (uint64_t it = 0; it < j->iters; ++it) {
+        const void* src = j->buf[it & 1];
+        void* dst = j->buf[(it & 1) ^ 1];
+        if (j->word_bits == 64)
+            gor_rows_64((const uint64_t*)src, (uint64_t*)dst, (const uint64_t*)j->zero, j->wx,
+                        j->y, j->y0, j->y1);
+        else
+            gor_rows_32((const uint32_t*)src, (uint32_t*)dst, (const uint32_t*)j->zero, j->wx,
+                        j->y, j->y0, j->y1);
+        if (j->bar) pthread_barrier_wait(j->bar);
+    }
     return NULL;
 }
 
@@ -378,36 +405,58 @@ int gor_life_rows(int word_bits, const void* in, uint64_t x, uint64_t y, uint64_
     if ((uint64_t)threads > y) threads = y ? (int)y : 1;
     if (threads > 512) threads = 512;
     void* tmp = malloc(bytes ? bytes : 8);
-    if (!tmp) return -1;
+    void* zero = calloc(wx ? wx : 1, 8);
+    if (!tmp || !zero) {
+        free(tmp);
+        free(zero);
+        return -1;
+    }
     memcpy(out, in, bytes);
-    void* src = out;
-    void* dst = tmp;
+    if (y == 0 || iters == 0 || wx == 0) {
+        free(tmp);
+        free(zero);
+        return 0;
+    }
+    int64_t per = ((int64_t)y + threads - 1) / threads;
+    int n = (int)(((int64_t)y + per - 1) / per); /* ranges that hold rows */
+    pthread_barrier_t bar;
+    if (n > 1 && pthread_barrier_init(&bar, NULL, (unsigned)n) != 0) n = 1;
+    if (n == 1) per = (int64_t)y;
+    gor_gate gate = {PTHREAD_MUTEX_INITIALIZER, PTHREAD_COND_INITIALIZER, 0};
     gor_job jobs[512];
     pthread_t tids[512];
-    for (uint64_t it = 0; it < iters; ++it) {
-        int64_t per = ((int64_t)y + threads - 1) / threads;
-        int started = 0;
-        for (int t = 0; t < threads; ++t) {
-            int64_t y0 = t * per, y1 = y0 + per;
-            if (y1 > (int64_t)y) y1 = (int64_t)y;
-            if (y0 >= y1) break;
-            jobs[t] = (gor_job){word_bits, src, dst, (int64_t)wx, (int64_t)y, y0, y1};
-            if (t == 0) continue; /* the calling thread runs range 0 */
-            if (pthread_create(&tids[t], NULL, gor_job_run, &jobs[t]) != 0) {
-                gor_job_run(&jobs[t]);
-                tids[t] = 0;
-            }
-            started = t;
-        }
-        if (y) gor_job_run(&jobs[0]);
-        for (int t = 1; t <= started; ++t)
-            if (tids[t]) pthread_join(tids[t], NULL);
-        void* tt = src;
-        src = dst;
-        dst = tt;
+    for (int t = 0; t < n; ++t) {
+        int64_t y0 = t * per, y1 = y0 + per;
+        if (y1 > (int64_t)y) y1 = (int64_t)y;
+        jobs[t] = (gor_job){word_bits, {out, tmp}, zero, (int64_t)wx, (int64_t)y, y0, y1, iters,
+                            n > 1 ? &bar : NULL, n > 1 ? &gate : NULL};
     }
-    if (src != out) memcpy(out, src, bytes);
+    int started = 0;
+    for (int t = 1; t < n; ++t) {
+        if (pthread_create(&tids[t], NULL, gor_job_run, &jobs[t]) != 0) break;
+        started = t;
+    }
+    const int whole = started == n - 1;
+    if (n > 1) {
+        pthread_mutex_lock(&gate.mu);
+        gate.state = whole ? 1 : -1;
+        pthread_cond_broadcast(&gate.cv);
+        pthread_mutex_unlock(&gate.mu);
+    }
+    if (whole) {
+        jobs[0].gate = NULL;
+        gor_job_run(&jobs[0]);
+    }
+    for (int t = 1; t <= started; ++t) pthread_join(tids[t], NULL);
+    if (n > 1) pthread_barrier_destroy(&bar);
+    if (!whole) { /* no team: one thread, all rows */
+        jobs[0] = (gor_job){word_bits, {out, tmp}, zero, (int64_t)wx, (int64_t)y, 0, (int64_t)y,
+                            iters, NULL, NULL};
+        gor_job_run(&jobs[0]);
+    }
+    if (iters & 1) memcpy(out, tmp, bytes);
     free(tmp);
+    free(zero);
     return 0;
 }
 

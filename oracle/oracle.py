@@ -27,6 +27,11 @@ ORACLE_SO = os.path.join(HERE, "libgoloracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libgolref.so")
 LEX_SO = os.path.join(HERE, "_ref", "libgollexref.so")
 
+# Where the reference's sources are read from when the checkers are built
+# (one environment variable; the default is where this build's recipe finds
+# them). Nothing at run time reads them.
+REFERENCE_SRC = os.environ.get("GOL_REFERENCE_SRC", "/root/reference/src")
+
 LAYOUT_COLUMNS = 1
 LAYOUT_TILES = 2
 
@@ -45,10 +50,10 @@ def build(with_ref: bool | None = None) -> None:
     """Compiles the oracle (and the reference harness when its sources exist)."""
     targets = ["all"]
     if with_ref is None:
-        with_ref = os.path.isdir("/root/reference/src")
+        with_ref = os.path.isdir(REFERENCE_SRC)
     if with_ref:
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE, *targets], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, *targets, f"REF_SRC={REFERENCE_SRC}"], check=True)
 
 
 def _ptr(a: np.ndarray):

@@ -22,12 +22,17 @@ struct RowsPlan {
     int slice = 0;     // words per x-slice (= W when one CTA spans the row)
     int nslices = 0;   // CTAs along x
     int halo = 0;      // x-halo words each side of a slice (0 when unsliced)
+    bool stream = false;   // k = 1 streaming kernel (gol_rows_stream.cuh): band = rows
+                           // per thread, nslices = CTAs across the row, no halo
 };
 
 // Picks words-per-lane and CTA shape for a W-word by Y-row grid and depth k.
 // wpl = 0 chooses the widest lane access whose rings fit k; 1, 2 or 4 forces
 // it. Returns false for k outside 1..16 or a wpl that W or k rules out.
-bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPlan* plan);
+// k = 1 plans the streaming kernel (band_rows = rows per thread, 0 = auto)
+// unless allow_stream is false (callers that need the K-stage geometry).
+bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPlan* plan,
+               bool allow_stream = true);
 
 // One pass of k generations (1 <= k <= kMaxKForWpl(plan.wpl)). pitch: words
 // from one row to the next (0 = W).

@@ -3,8 +3,16 @@
 #include <algorithm>
 
 #include "gol_internal.h"
+#include "gol_rows_stream.cuh"
 #include "gol_rows_temporal.cuh"
 #include "gol_word_ops.cuh"
+
+#ifndef GOL_STREAM_THREADS
+#define GOL_STREAM_THREADS 128   // CTA size of the one-generation streaming kernel
+#endif
+#ifndef GOL_STREAM_CTAS_PER_SM
+#define GOL_STREAM_CTAS_PER_SM 16   // default band: about this many CTAs per SM per pass
+#endif
 
 namespace golb200 {
 
@@ -36,6 +44,24 @@ cudaError_t launch_one(const RowsLaunch& a, const RowsPlan& p, cudaStream_t stre
     return cudaLaunchKernelEx(&cfg, rows_temporal_kernel<WPL, K>, a);
 }
 
+// The one-generation streaming kernel, also a programmatic dependent.
+template <int WPL>
+cudaError_t launch_stream(const RowsLaunch& a, const RowsPlan& p, cudaStream_t stream) {
+    cudaLaunchConfig_t cfg = {};
+    const long long ctas = (long long)p.nslices * p.nbands;
+    if (ctas > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    cfg.gridDim = dim3((unsigned)ctas);
+    cfg.blockDim = dim3(p.threads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, rows_stream_kernel<WPL>, a);
+}
+
 template <int WPL, int K>
 cudaError_t dispatch_k(int k, const RowsLaunch& a, const RowsPlan& p, cudaStream_t stream) {
     if constexpr (K > kMaxKForWpl(WPL)) {
@@ -54,7 +80,8 @@ int device_sm_count(int device) {
     return n > 0 ? n : 148;
 }
 
-bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPlan* plan) {
+bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPlan* plan,
+               bool allow_stream) {
     if (k < 1 || k > kMaxTemporalSteps || W <= 0) return false;
     if (wpl != 0) {
         if ((wpl != 1 && wpl != 2 && wpl != 4) || W % wpl || k > kMaxKForWpl(wpl)) return false;
@@ -70,6 +97,27 @@ bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPla
     }
     plan->wpl = wpl;
     const int lanes = W / wpl;
+    plan->stream = k == 1 && allow_stream;
+    if (plan->stream) {
+        // One generation: lanes of wpl words across the row in CTAs of up to
+        // GOL_STREAM_THREADS threads, each thread walking `band` rows. The
+        // default band gives about GOL_STREAM_CTAS_PER_SM CTAs per SM (many
+        // resident warps, several waves), never below 8 rows (each band
+        // re-reads one halo row above and one below) nor above 64.
+        plan->threads = std::min(GOL_STREAM_THREADS, (lanes + 31) / 32 * 32);
+        plan->nslices = (lanes + plan->threads - 1) / plan->threads;
+        plan->slice = plan->threads * wpl;
+        plan->halo = 0;
+        int band = band_rows;
+        if (band <= 0) {
+            const long long ctas = (long long)GOL_STREAM_CTAS_PER_SM * num_sms;
+            band = (int)std::min<long long>(64, std::max<long long>(8, ((long long)Y * plan->nslices + ctas - 1) / ctas));
+        }
+        band = std::min(band, std::max(Y, 1));
+        plan->band = band;
+        plan->nbands = (Y + band - 1) / band;
+        return true;
+    }
     if (lanes <= kTemporalMaxThreads) {
         plan->slice = W;
         plan->nslices = 1;
@@ -102,6 +150,15 @@ cudaError_t launch_rows_pass(const uint32_t* src, uint32_t* dst, int W, int Y, i
                              const RowsPlan& p, cudaStream_t stream, int pitch) {
     if (Y <= 0 || W <= 0) return cudaSuccess;
     RowsLaunch a{src, dst, W, Y, p.band, p.slice, p.halo, pitch ? pitch : W};
+    if (p.stream) {
+        if (k != 1) return cudaErrorInvalidValue;
+        switch (p.wpl) {
+            case 4: return launch_stream<4>(a, p, stream);
+            case 2: return launch_stream<2>(a, p, stream);
+            case 1: return launch_stream<1>(a, p, stream);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (p.wpl) {
         case 4: return dispatch_k<4, 1>(k, a, p, stream);
         case 2: return dispatch_k<2, 1>(k, a, p, stream);

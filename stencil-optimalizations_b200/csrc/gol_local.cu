@@ -421,7 +421,7 @@ bool plan_local_tiles(int W, int Y, int k, int tile_rows, int wpl, int num_sms, 
     const long long ntiles = (long long)lp->tiles_x * lp->tiles_y;
     if (dense_pct == 0) dense_pct = GOL_LOCAL_DENSE_PCT;
     lp->dense_min = INT_MAX;
-    if (dense_pct <= 100 && plan_rows(W, Y, k, 0, tracked_wpl(k), num_sms, &lp->dense))
+    if (dense_pct <= 100 && plan_rows(W, Y, k, 0, tracked_wpl(k), num_sms, &lp->dense, false))
         lp->dense_min = (int)std::max(1LL, (ntiles * dense_pct + 99) / 100);
     return true;
 }

@@ -13,6 +13,9 @@
 // until the process exits. In host code its name is only a host-side
 // stand-in, not a device address, so the address is looked up once per
 // device with cudaGetSymbolAddress (with that device current) and cached.
+// The cached address belongs to the device's current context: after a
+// cudaDeviceReset it is stale, and calls on that device must not be made
+// again in this process.
 #include <mutex>
 
 #include "gol_b200.h"
@@ -50,6 +53,9 @@ extern "C" int gol_rows_run_noalloc(const void* d_in, void* d_out, uint64_t x, u
     if (((uintptr_t)d_in | (uintptr_t)d_out) & 15u) return GOL_E_INVALID;
     if (k == 0) k = 4;
     if (k > (uint32_t)golb200::kMaxTemporalSteps) return GOL_E_INVALID;
+    // The same limits as every other entry point (x / 32 and y fit the
+    // kernels' int indices), before any size arithmetic can wrap.
+    if (x / 32 > (1ull << 30) || y > (1ull << 30)) return GOL_E_INVALID;
     const uint64_t bytes = x / 8 * y;
     if (bytes > kNoAllocMaxBytes) return GOL_E_UNSUPPORTED;   // grid larger than the scratch
     const int W = (int)(x / 32), Y = (int)y;

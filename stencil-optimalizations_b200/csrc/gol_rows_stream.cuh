@@ -1,0 +1,129 @@
+// One-generation streaming kernel: the HBM-bound pass.
+//
+// What it replaces in the reference: the plain one-generation word kernel
+// (src/algorithms/cuda-naive-bitwise/cuda_naive_bitwise_kernel.cu:32-79),
+// which loads the 3x3 neighbourhood of every word (9 loads per word, cells
+// outside the grid read as 0 through `load`, :24-30) and launches once per
+// generation (:58-79).
+//
+// A single generation does about 12 integer operations per 32-cell word
+// against 8 bytes of HBM traffic, so the pass is bound by HBM, not by the
+// integer pipe: what matters is bytes in flight, coalescing and no wasted
+// traffic. So, unlike the K-stage pipeline of gol_rows_temporal.cuh (one
+// barrier per row, a deep register pipeline, two CTAs per SM):
+//   * a thread owns WPL consecutive words of a row (one 16/8/4-byte load and
+//     store) and walks down a band of `band` rows, reading band + 2 rows;
+//   * loads are issued P rows ahead into a register ring (P a multiple of 3,
+//     the loop unrolled by P, so every ring slot and the 3-row ring of
+//     horizontal sums are compile-time register names);
+//   * no shared memory and no barriers: the word left and right of a lane's
+//     span come from its warp neighbours by shuffle, and lanes 0 and 31 load
+//     them from global memory (the same 32-byte sectors the neighbouring
+//     warps read, so an L1/L2 hit, not extra HBM traffic);
+//   * few registers, so many warps per SM keep enough bytes in flight.
+// The halo rows (one above and one below each band) are read by both
+// neighbouring bands; bands with adjacent blockIdx.y run at the same time,
+// so the second read hits L2.
+#pragma once
+
+#include <cstdint>
+
+#include "gol_rows_temporal.cuh"
+#include "gol_word_ops.cuh"
+
+namespace golb200 {
+
+constexpr int kStreamMaxThreads = 256;
+constexpr int kStreamAhead = 6;   // rows in flight per thread (multiple of 3)
+
+template <int WPL>
+__device__ __forceinline__ void stream_load(const uint32_t* p, bool v, uint32_t (&w)[WPL]) {
+    if (v) {
+        load_words<WPL>(p, w);
+    } else {
+#pragma unroll
+        for (int i = 0; i < WPL; ++i) w[i] = 0u;
+    }
+}
+
+// a.band = output rows per thread (any positive value); a.slice = words
+// per CTA across the row (blockDim.x lanes of WPL words). The grid is 1-D:
+// CTA b takes slice b % nslices of band b / nslices, so CTAs with adjacent
+// indices share rows (and their halo rows meet in L2). a.halo is unused (the
+// row is never cut with halo lanes: lanes at a CTA boundary read their outer
+// words from memory).
+template <int WPL>
+__global__ void __launch_bounds__(kStreamMaxThreads)
+rows_stream_kernel(RowsLaunch a) {
+    constexpr int P = kStreamAhead;
+    static_assert(P % 3 == 0, "the ring of horizontal sums is indexed by row mod 3");
+    pdl_trigger_and_wait();
+    const int lane = threadIdx.x & 31;
+    const int nslices = (a.W + a.slice - 1) / a.slice;
+    const int slice = (int)(blockIdx.x % (unsigned)nslices);
+    const int band = (int)(blockIdx.x / (unsigned)nslices);
+    const int base = slice * a.slice + (int)threadIdx.x * WPL;
+    const bool ok = base < a.W;   // W % WPL == 0: a lane is wholly inside or outside
+    const bool load_l = ok && lane == 0 && base > 0;
+    const bool load_r = ok && lane == 31 && base + WPL < a.W;
+    const int y0 = band * a.band;
+    const int y1 = min(y0 + a.band, a.Y);
+    const int n = y1 - y0 + 2;    // rows y0 - 1 .. y1 are read
+    const uint32_t* col = a.src + base;
+
+    uint32_t v[P][WPL], vl[P], vr[P];   // rows in flight: words, outer left / right word
+
+    // Issues the load of read-row i (grid row y0 - 1 + i) into ring slot s.
+    auto issue = [&](int s, int i) {
+        const int y = y0 - 1 + i;
+        const bool rv = i < n && (unsigned)y < (unsigned)a.Y;
+        const uint32_t* p = col + (size_t)(rv ? y : 0) * a.pitch;
+        stream_load<WPL>(p, ok && rv, v[s]);
+        vl[s] = (load_l && rv) ? __ldg(p - 1) : 0u;
+        vr[s] = (load_r && rv) ? __ldg(p + WPL) : 0u;
+    };
+#pragma unroll
+    for (int s = 0; s < P; ++s) issue(s, s);
+
+    uint32_t h0[3][WPL], h1[3][WPL], c[3][WPL];   // by read-row mod 3
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int w = 0; w < WPL; ++w) h0[r][w] = h1[r][w] = c[r][w] = 0u;
+
+    for (int i0 = 0; i0 < n; i0 += P) {   // n is uniform across the CTA
+#pragma unroll
+        for (int j = 0; j < P; ++j) {
+            const int i = i0 + j;
+            if (i >= n) break;
+            const int r = j % 3;   // == i % 3 (i0 is a multiple of P, P of 3)
+            // Neighbour words: the lane to the left's last word and the lane
+            // to the right's first word (zero past the grid), or from memory
+            // at the warp's ends.
+            uint32_t lw = __shfl_up_sync(0xffffffffu, v[j][WPL - 1], 1);
+            uint32_t rw = __shfl_down_sync(0xffffffffu, v[j][0], 1);
+            if (lane == 0) lw = vl[j];
+            if (lane == 31) rw = vr[j];
+#pragma unroll
+            for (int w = 0; w < WPL; ++w) {
+                const uint32_t l = w == 0 ? lw : v[j][w - 1];
+                const uint32_t rr = w == WPL - 1 ? rw : v[j][w + 1];
+                hsum(l, v[j][w], rr, h0[r][w], h1[r][w]);
+                c[r][w] = v[j][w];
+            }
+            issue(j, i + P);   // slot j is free again
+            if (i >= 2) {      // output row y0 + i - 2 from read-rows i-2, i-1, i
+                const int rm = (j + 1) % 3;   // (i - 2) mod 3
+                const int rc = (j + 2) % 3;   // (i - 1) mod 3
+                uint32_t res[WPL];
+#pragma unroll
+                for (int w = 0; w < WPL; ++w)
+                    res[w] = next_word(h0[rm][w], h1[rm][w], h0[rc][w], h1[rc][w], h0[r][w],
+                                       h1[r][w], c[rc][w]);
+                if (ok) store_words<WPL>(a.dst + (size_t)(y0 + i - 2) * a.pitch + base, res);
+            }
+        }
+    }
+}
+
+} // namespace golb200

@@ -23,8 +23,14 @@
 
 namespace golb200 {
 
-template <typename cell_t, uint32_t Algo = GOL_ALG_AUTO>
+// Depth: 0 takes ExperimentParams::temporal_steps (whose default, 1, and 0
+// let the engine pick its depth: the reference's default of one generation
+// per step would be the slowest choice here); 1..16 forces that depth, so
+// registering GolB200Algorithm<char, GOL_ALG_AUTO, 1> gives the
+// one-generation (HBM-streaming) kernel under its own algorithm name.
+template <typename cell_t, uint32_t Algo = GOL_ALG_AUTO, uint32_t Depth = 0>
 class GolB200Algorithm : public infrastructure::Algorithm<2, cell_t> {
+    static_assert(Depth <= 16, "depth is 1..16, or 0 for the parameters' choice");
   public:
     using DataGrid = infrastructure::Grid<2, cell_t>;
     using size_type = std::size_t;
@@ -68,14 +74,22 @@ class GolB200Algorithm : public infrastructure::Algorithm<2, cell_t> {
 
     std::size_t actually_performed_iterations() const override { return gol_performed(engine_); }
 
+    // The engine behind the adapter (for gol_plan, gol_local_stats and the
+    // like); null before the first set_and_format_input_data.
+    gol_engine* engine() const { return engine_; }
+
   private:
     void ensure_engine() {
         gol_config cfg;
         gol_config_init(&cfg, x_, y_);
         cfg.algorithm = Algo;
         cfg.word_bits = this->params.state_bits_count == 32 ? 32 : 64;
-        cfg.temporal_steps = this->params.temporal_steps > 1 ? (uint32_t)this->params.temporal_steps : 0;
-        cfg.thread_block_size = 0;   // the reference's block size has no meaning for band kernels
+        cfg.temporal_steps =
+            Depth ? Depth : (this->params.temporal_steps > 1 ? (uint32_t)this->params.temporal_steps : 0);
+        // ExperimentParams::thread_block_size is a CUDA block size in threads
+        // for the reference's kernels; the row-band kernels size their CTAs
+        // from the grid's width, so it is not passed on (band height: auto).
+        cfg.thread_block_size = 0;
         cfg.max_runtime_seconds =
             this->params.max_runtime_seconds == (std::size_t)infrastructure::StopWatch::MAX_TIME
                 ? 0

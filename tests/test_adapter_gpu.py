@@ -18,8 +18,12 @@ DRIVER = os.path.join(ROOT, "oracle", "_ref", "adapter_driver")
 @pytest.mark.parametrize("args", [["256", "128", "100", "42"],
                                   ["512", "320", "77", "7", "4"],
                                   ["1024", "96", "64", "3", "8", "local"],
-                                  ["128", "64", "0", "5"]])
+                                  ["128", "64", "0", "5"],
+                                  ["512", "200", "33", "9", "1", "k1"],
+                                  ["2048", "64", "20", "4", "6", "k1"]])
 def test_engine_behind_reference_algorithm_interface(args):
     r = subprocess.run([DRIVER, *args], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "valid (equals GoLCpuNaive)" in r.stdout
+    if "k1" in args:
+        assert "engine depth: 1 generation per pass" in r.stdout

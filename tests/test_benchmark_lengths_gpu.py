@@ -1,0 +1,77 @@
+"""Bit-exact parity at the lengths the benchmark times, for every benchmark
+configuration, against the threaded bit-sliced oracle (the reference's
+GoLCpuBitwise<AdderOps> restated, itself pinned to the reference's own CPU
+build by tests/test_oracle.py). The reference validates the final grid after
+the full run the same way (experiment_manager.hpp:272-307).
+
+  dense 16384^2, 64-bit rows, Bernoulli(0.5) seed 42, 4096 generations, k = 4 and 8
+  dense 8192^2, 32-bit rows, 4096 generations
+  sparse 16384^2 (1 % of 64x64 slots Bernoulli(0.35)), 20000 generations, change tracking
+  the 512 uneven grids of the batched workload after one batched launch
+"""
+import os
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+import pytest
+
+import golb200
+import oracle
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+GENS = 4096
+
+
+def engine_words(cells, gens, word_bits, **kw):
+    y, x = cells.shape
+    with golb200.GolB200(grid_dimensions=(x, y), state_bits_count=word_bits, **kw) as alg:
+        alg.set_and_format_input_data(cells)
+        alg.initialize_data_structures()
+        alg.run(gens)
+        alg.finalize_data_structures()
+        assert alg.actually_performed_iterations() == gens
+        return alg.fetch_words(word_bits)
+
+
+@pytest.mark.parametrize("size,word_bits,k", [(16384, 64, 4), (16384, 64, 8), (8192, 32, 0),
+                                              (8192, 32, 8)])
+def test_dense_configs_at_full_length(size, word_bits, k):
+    cells = oracle.random_ones_zeros(size, size, 42)
+    got = engine_words(cells, GENS, word_bits, temporal_steps=k)
+    want = oracle.life_rows(oracle.pack_rows(cells, word_bits), size, GENS, word_bits)
+    assert np.array_equal(got, want), (size, word_bits, k)
+
+
+def test_sparse_change_tracking_at_full_length():
+    size, gens = 16384, 20000
+    cells = golb200.load_sparse_patches(size, size, 42, 64, 0.01, 0.35)
+    got = engine_words(cells, gens, 64, algorithm="local")
+    want = oracle.life_rows(oracle.pack_rows(cells, 64), size, gens, 64)
+    assert np.array_equal(got, want)
+
+
+def oracle_grid(words: np.ndarray, x: int, gens: int) -> np.ndarray:
+    """The oracle on one grid: one thread for small grids (many run at once)."""
+    threads = 1 if words.size < (1 << 16) else 4
+    return oracle.life_rows(words, x, gens, 64, threads=threads)
+
+
+def test_batched_workload_every_grid():
+    work = golb200.workload_uneven(42, 512, 256, 4096, 64, (0.2, 0.5), (64, 4096))
+    inputs = []
+    with golb200.GolBatch() as b:
+        for d in work:
+            cells = golb200.load_bernoulli(d["x"], d["y"], d["cell_seed"], d["density"])
+            inputs.append(oracle.pack_rows(cells, 64))
+            b.add(cells, d["gens"])
+        b.upload()
+        b.run()
+        b.sync()
+        got = [oracle.pack_rows(b.fetch(i), 64) for i in range(len(work))]
+    workers = max(1, (os.cpu_count() or 1) // 2)
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        want = list(pool.map(lambda i: oracle_grid(inputs[i], work[i]["x"], work[i]["gens"]),
+                             range(len(work))))
+    bad = [i for i in range(len(work)) if not np.array_equal(got[i], want[i])]
+    assert not bad, bad[:10]

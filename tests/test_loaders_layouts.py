@@ -44,7 +44,7 @@ OWN_DICTIONARY = """
     };
 """
 
-REF_PATTERNS = "/root/reference/src/infrastructure/gol-lexicon/patterns.cpp"
+REF_PATTERNS = os.path.join(oracle.REFERENCE_SRC, "infrastructure", "gol-lexicon", "patterns.cpp")
 
 
 def test_zeros_loader():

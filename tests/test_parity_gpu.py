@@ -76,6 +76,38 @@ def test_forced_lane_widths(wpl, ks):
                                   oracle.life_cells(g, n)), (x, y, wpl, k)
 
 
+@pytest.mark.parametrize("wpl", [1, 2, 4])
+def test_one_generation_streaming_kernel(wpl):
+    """k = 1 runs the streaming kernel (gol_rows_stream.cuh): any rows per
+    thread (band), rows across several CTAs (lanes 0 and 31 of each warp read
+    their outer words from memory), bands cut by the grid's last row."""
+    for x, y in ((128, 1), (96, 7), (4096 + 128, 45), (32 * 1025, 5), (16384, 33)):
+        if (x // 32) % wpl:
+            continue
+        g = oracle.random_ones_zeros(x, y, 3 * x + y + wpl)
+        for band in (1, 2, 3, 4, 7, 64):
+            for n in (1, 2, 5):
+                out = run_engine(g, n, k=1, word_bits=32, band=band, lane_words=wpl)
+                assert np.array_equal(out, oracle.life_cells(g, n)), (x, y, wpl, band, n)
+
+
+def test_streaming_kernel_stateless_pass():
+    """gol_rows_pass_ex with k = 1 (the streaming kernel) between two device
+    grids, chained, against the oracle."""
+    torch = pytest.importorskip("torch")
+    s = torch.cuda.current_stream().cuda_stream
+    for x, y, wpl in ((8192, 70, 0), (4096 + 64, 19, 2), (32 * 257, 11, 1)):
+        g = oracle.random_ones_zeros(x, y, x ^ y)
+        a = torch.from_numpy(oracle.pack_rows(g, 32).view(np.int32)).cuda()
+        b = torch.empty_like(a)
+        for _ in range(9):
+            golb200.rows_pass(a.data_ptr(), b.data_ptr(), x, y, 1, 0, s, wpl)
+            a, b = b, a
+        torch.cuda.synchronize()
+        got = a.cpu().numpy().view(np.uint32)
+        assert np.array_equal(got, oracle.pack_rows(oracle.life_cells(g, 9), 32)), (x, y, wpl)
+
+
 def test_word_bits_32_and_64_agree():
     g = oracle.random_ones_zeros(512, 100, 77)
     a = run_engine(g, 37, word_bits=32)
