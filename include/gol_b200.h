@@ -352,6 +352,26 @@ int gol_batch_probe_timeout(int32_t device, uint64_t spin_limit, int32_t* status
 /* Census of the last gol_batch_run: SM clock cycles its work items spent
  * waiting on dependencies and computing, summed over items. */
 int gol_batch_census(gol_batch* b, uint64_t* wait_cycles, uint64_t* work_cycles);
+
+/* Change tracking in the batch (the rule of the reference's change-tracking
+ * kernels, cuda_naive_local.cu:125-161 and cuda_local_one_cell.cu:172-200,
+ * on the batch's work items as tiles): an item of pass p is computed only if
+ * it or one of its 8 neighbour items changed in pass p-1; a grid whose pass
+ * changed nothing is still from then on, and its remaining items end at
+ * once. GOL_TRACK_AUTO (default) tracks grids of at least 8 passes until
+ * gol_batch_retune has seen a run; gol_batch_retune then keeps tracking per
+ * grid where the run skipped at least 5 % of its items (finest tiles, 16-row
+ * bands, from 50 %) and runs the others dense. Both take effect at the next
+ * upload/run. */
+enum gol_track_mode { GOL_TRACK_AUTO = 0, GOL_TRACK_OFF = 1, GOL_TRACK_ON = 2 };
+int gol_batch_set_tracking(gol_batch* b, int32_t grid_id, int32_t mode);
+int gol_batch_retune(gol_batch* b);
+/* Work items of the last run computed and skipped (skipped: tracked grids). */
+int gol_batch_tiles(gol_batch* b, uint64_t* computed, uint64_t* skipped);
+/* One grid of the last run: whether it tracked changes, its items computed
+ * and skipped, and the pass from which it was still (0xFFFFFFFF: never). */
+int gol_batch_grid_stats(gol_batch* b, int32_t grid_id, uint32_t* tracked, uint32_t* computed,
+                         uint32_t* skipped, uint32_t* still_pass);
 void* gol_batch_stream(gol_batch* b);
 const char* gol_batch_last_error(const gol_batch* b);
 void gol_batch_destroy(gol_batch* b);
@@ -391,6 +411,24 @@ int gol_serve_stats(const gol_server* s, uint64_t* queued, uint64_t* running, ui
                     uint64_t* cell_updates, uint64_t* arena_free_bytes);
 /* Waits for every queued round. */
 int gol_serve_drain(gol_server* s);
+/* Scheduling policy, for requests submitted and rounds planned from then on:
+ * GOL_SERVE_FIFO (default) admits in arrival order and advances every
+ * running request by `quantum` generations per round; GOL_SERVE_SRPT admits
+ * the queued request with the least work (cells x generations) first and
+ * scales a small grid's per-round generations up by 2^20 / its cells, so
+ * small requests finish in few rounds. */
+enum gol_serve_policy { GOL_SERVE_FIFO = 0, GOL_SERVE_SRPT = 1 };
+int gol_serve_set_policy(gol_server* s, int32_t policy);
+/* Change tracking for requests submitted from then on (GOL_TRACK_AUTO: those
+ * of at least 8 passes; _ON, _OFF). A tracked request keeps its change flags
+ * resident in its slot between rounds and skips the tiles (work items) whose
+ * 3x3 neighbourhood did not change in the previous pass; once a whole pass
+ * changes nothing the request is finished at the end of that round, before
+ * its remaining generations (they could not change it). */
+int gol_serve_set_tracking(gol_server* s, int32_t mode);
+/* Work items computed and skipped over all rounds so far, and the number of
+ * requests finished early because they became still. */
+int gol_serve_tiles(gol_server* s, uint64_t* computed, uint64_t* skipped, uint64_t* early_finished);
 const char* gol_serve_last_error(const gol_server* s);
 void* gol_serve_stream(gol_server* s);
 void gol_serve_destroy(gol_server* s);

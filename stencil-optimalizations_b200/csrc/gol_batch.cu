@@ -69,10 +69,13 @@ __device__ __forceinline__ void st_release(int* p, int v) {
     asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-template <int WPL, int K>
-__device__ __forceinline__ void seg_group(const BatchGrid& G, int group, int slice_idx,
-                                          const uint32_t* src, uint32_t* dst, uint32_t* ring,
-                                          uint32_t* etab) {
+// One work item: the K-stage pipeline over the item's segments. With TRACK,
+// every stored word is compared with the same word before the pass and the
+// return value is this lane's OR of the differences (0: its part unchanged).
+template <int WPL, int K, bool TRACK>
+__device__ __forceinline__ uint32_t seg_group(const BatchGrid& G, int group, int slice_idx,
+                                              const uint32_t* src, uint32_t* dst, uint32_t* ring,
+                                              uint32_t* etab) {
     const int lane = threadIdx.x & 31;
     const int L = G.seg_lanes;
     const int seg = lane / L, q = lane - seg * L;
@@ -126,26 +129,34 @@ __device__ __forceinline__ void seg_group(const BatchGrid& G, int group, int sli
     const int f0 = 3 * K;
     const int f1 = min(G.band + 2 * K - 1, G.Y - y0_last + K - 1);
     const int fast_end = f1 > f0 ? f0 + (f1 - f0) / 3 * 3 : f0;
+    constexpr int TR = TRACK ? 1 : 0;
     if (fast_end > f0) {
-        temporal_steps<WPL, K, false, false, false, true, true>(s, c, 0, f0);
-        temporal_steps<WPL, K, true, true, false, true, true>(s, c, f0, fast_end);
-        temporal_steps<WPL, K, false, false, false, true, true>(s, c, fast_end, nsteps);
+        temporal_steps<WPL, K, false, false, TR, true, true>(s, c, 0, f0);
+        temporal_steps<WPL, K, true, true, TR, true, true>(s, c, f0, fast_end);
+        temporal_steps<WPL, K, false, false, TR, true, true>(s, c, fast_end, nsteps);
     } else {
-        temporal_steps<WPL, K, false, false, false, true, true>(s, c, 0, nsteps);
+        temporal_steps<WPL, K, false, false, TR, true, true>(s, c, 0, nsteps);
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
+    return s.diff;
 }
 
-template <int WPL>
-__device__ __forceinline__ void seg_dispatch(int k, const BatchGrid& G, int group, int slice,
-                                             const uint32_t* src, uint32_t* dst, uint32_t* ring,
-                                             uint32_t* etab) {
+template <int WPL, bool TRACK>
+__device__ __forceinline__ uint32_t seg_dispatch(int k, const BatchGrid& G, int group, int slice,
+                                                 const uint32_t* src, uint32_t* dst,
+                                                 uint32_t* ring, uint32_t* etab) {
     switch (k) {
-        case 1: seg_group<WPL, 1>(G, group, slice, src, dst, ring, etab); break;
-        case 2: seg_group<WPL, 2>(G, group, slice, src, dst, ring, etab); break;
-        case 3: seg_group<WPL, 3>(G, group, slice, src, dst, ring, etab); break;
-        default: seg_group<WPL, 4>(G, group, slice, src, dst, ring, etab); break;
+        case 1: return seg_group<WPL, 1, TRACK>(G, group, slice, src, dst, ring, etab);
+        case 2: return seg_group<WPL, 2, TRACK>(G, group, slice, src, dst, ring, etab);
+        case 3: return seg_group<WPL, 3, TRACK>(G, group, slice, src, dst, ring, etab);
+        default: return seg_group<WPL, 4, TRACK>(G, group, slice, src, dst, ring, etab);
     }
+}
+
+__device__ __forceinline__ void release_max(int* p, int v) {
+    // Monotone release: an item of a still grid may finish before the item
+    // of the previous pass on the same counter (it does not wait for it).
+    asm volatile("red.release.gpu.global.max.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 // WPL_ONLY = 1, 2 or 4: every grid of the launch uses that many words per
@@ -154,7 +165,21 @@ __device__ __forceinline__ void seg_dispatch(int k, const BatchGrid& G, int grou
 // own width. Warps of one SM that run different bodies compete for the
 // instruction cache, which halved throughput in measurements, so the
 // planner gives a batch one width and one depth.
-template <int WPL_ONLY>
+//
+// TRACK: grids with a change-tracking region (G.trk) skip the items whose
+// 3x3 neighbour items did not change in the previous pass, the rule of the
+// reference's change-tracking kernels (cuda_naive_local.cu:125-161,
+// cuda_local_one_cell.cu:172-200). A skipped item needs no copy: it did not
+// change in the previous pass (it is its own neighbour), so the buffer it
+// would write — the one the previous pass read — already holds its state.
+// Computed items compare every stored word with its input and publish a
+// change flag before releasing their counter. When every item of a pass is
+// done and none changed, the grid is still from the next pass on (the
+// "retired" pass): later items of that grid end at once, without waiting for
+// their dependencies or touching the grid, and both buffers hold the result.
+// census: [0] SM cycles waiting on dependencies, [1] working, [2] items
+// computed, [3] items skipped (tracked grids).
+template <int WPL_ONLY, bool TRACK>
 __global__ void __launch_bounds__(32, GOL_BATCH_MIN_BLOCKS)
 batch_kernel(const BatchGrid* __restrict__ grids, const BatchItem* __restrict__ items, int nitems,
              int* ticket, int* done, int* status, unsigned long long* census, long long spin_limit) {
@@ -170,19 +195,45 @@ batch_kernel(const BatchGrid* __restrict__ grids, const BatchItem* __restrict__ 
     while (t < nitems) {
         const BatchItem it = items[t];
         const BatchGrid G = grids[it.grid];
-        int* mine = done + G.done_base + it.group * G.nslices + it.slice;
+        const int cell = it.group * G.nslices + it.slice;
+        int* mine = done + G.done_base + cell;
+        const int nper = G.ngroups * G.nslices;   // items per pass
+        // A pass shorter than k (the last, when k does not divide the
+        // generations) is not covered by the k-generation change flags: an
+        // oscillator whose period divides k looks still to them. It computes
+        // every item.
+        const int k = it.pass == G.passes - 1 ? G.last_k : G.k;
+        if (TRACK && G.trk && k == G.k) {
+            const unsigned still = *(volatile const uint32_t*)(G.trk + 2 * nper);
+            if ((unsigned)(G.pass0 + it.pass) >= still) {   // the grid stopped changing
+                int next = 0;
+                if (lane == 0) {
+                    next = atomicAdd(ticket, 1);
+                    // every flag from the still pass on is zero; writing this
+                    // pass's keeps a later reader from seeing an older one
+                    *(volatile uint32_t*)(G.trk + (((G.parity0 + it.pass) & 1) ? nper : 0) + cell) = 0u;
+                    release_max(mine, it.pass + 1);
+                    atomicAdd(G.gstat + 1, 1u);
+                    if (G.rflag) *(volatile int*)G.rflag = 1;
+                    if (census) atomicAdd(census + 3, 1ull);
+                }
+                t = __shfl_sync(0xffffffffu, next, 0);
+                continue;
+            }
+        }
+        // the 3x3 neighbourhood of (group, slice)
+        const int jlo = max(it.group - 1, 0), jhi = min(it.group + 1, G.ngroups - 1);
+        const int slo = max(it.slice - 1, 0), shi = min(it.slice + 1, G.nslices - 1);
+        const int nj = jhi - jlo + 1, ns = shi - slo + 1;
+        const int dep = lane < nj * ns ? (jlo + lane / ns) * G.nslices + slo + lane % ns : -1;
         const long long t_wait = clock64();
         if (it.pass > 0) {
-            // Lane d polls dependency d (3x3 neighbourhood of (group, slice))
-            // until it reached this pass; then every lane acquires every
-            // counter (each is already there), so each lane's own copies below
-            // are ordered after the producers' releases.
-            const int jlo = max(it.group - 1, 0), jhi = min(it.group + 1, G.ngroups - 1);
-            const int slo = max(it.slice - 1, 0), shi = min(it.slice + 1, G.nslices - 1);
-            const int nj = jhi - jlo + 1, ns = shi - slo + 1;
+            // Lane d polls dependency d until it reached this pass; then every
+            // lane acquires every counter (each is already there), so each
+            // lane's own copies below are ordered after the producers' releases.
             bool ok = true;
-            if (lane < nj * ns) {
-                const int* p = done + G.done_base + (jlo + lane / ns) * G.nslices + slo + lane % ns;
+            if (dep >= 0) {
+                const int* p = done + G.done_base + dep;
                 long long spins = 0;
                 while (ld_acquire(p) < it.pass) {
                     if (++spins > spin_limit || *(volatile int*)status != 0) {
@@ -205,28 +256,59 @@ batch_kernel(const BatchGrid* __restrict__ grids, const BatchItem* __restrict__ 
         int next = 0;
         if (lane == 0) next = atomicAdd(ticket, 1);
         const long long t_work = clock64();
-        const int k = it.pass == G.passes - 1 ? G.last_k : G.k;
-        // Selects, not an index: a dynamically indexed descriptor would be
-        // kept in local memory for the whole item.
         const bool odd = (G.parity0 + it.pass) & 1;
-        const uint32_t* src = odd ? G.buf[1] : G.buf[0];
-        uint32_t* dst = odd ? G.buf[0] : G.buf[1];
-        if constexpr (WPL_ONLY != 0) {
-            seg_dispatch<WPL_ONLY>(k, G, it.group, it.slice, src, dst, ring, etab);
-        } else {
-            switch (G.wpl) {
-                case 4: seg_dispatch<4>(k, G, it.group, it.slice, src, dst, ring, etab); break;
-                case 2: seg_dispatch<2>(k, G, it.group, it.slice, src, dst, ring, etab); break;
-                default: seg_dispatch<1>(k, G, it.group, it.slice, src, dst, ring, etab); break;
-            }
+        bool compute = true;
+        if (TRACK && G.trk && k == G.k) {   // did the neighbourhood change in the previous pass?
+            const uint32_t* prev = G.trk + (odd ? 0 : nper);   // parity of pass - 1
+            const uint32_t f = dep >= 0 ? *(volatile const uint32_t*)(prev + dep) : 0u;
+            compute = __any_sync(0xffffffffu, f != 0u);
         }
+        bool changed = false;
+        if (compute) {
+            // Selects, not an index: a dynamically indexed descriptor would be
+            // kept in local memory for the whole item.
+            const uint32_t* src = odd ? G.buf[1] : G.buf[0];
+            uint32_t* dst = odd ? G.buf[0] : G.buf[1];
+            uint32_t diff;
+            if constexpr (WPL_ONLY != 0) {
+                diff = seg_dispatch<WPL_ONLY, TRACK>(k, G, it.group, it.slice, src, dst, ring, etab);
+            } else {
+                switch (G.wpl) {
+                    case 4: diff = seg_dispatch<4, TRACK>(k, G, it.group, it.slice, src, dst, ring, etab); break;
+                    case 2: diff = seg_dispatch<2, TRACK>(k, G, it.group, it.slice, src, dst, ring, etab); break;
+                    default: diff = seg_dispatch<1, TRACK>(k, G, it.group, it.slice, src, dst, ring, etab); break;
+                }
+            }
+            changed = TRACK && __any_sync(0xffffffffu, diff != 0u);
+        }
+        if (TRACK && G.trk && lane == 0)   // this pass's flag, read by the next pass
+            *(volatile uint32_t*)(G.trk + (odd ? nper : 0) + cell) =
+                (changed || k != G.k) ? 1u : 0u;
         __threadfence();
         __syncwarp();
         if (lane == 0) {
-            st_release(mine, it.pass + 1);
+            if (TRACK && G.trk)
+                release_max(mine, it.pass + 1);
+            else
+                st_release(mine, it.pass + 1);
+            atomicAdd(G.gstat + (compute ? 0 : 1), 1u);
+            if (TRACK && G.trk) {
+                // Last item of this pass: if none changed, the grid is still
+                // from the next pass on.
+                if (changed || k != G.k) atomicAdd(G.pstat + 2 * it.pass + 1, 1);
+                __threadfence();
+                if (atomicAdd(G.pstat + 2 * it.pass, 1) == nper - 1) {
+                    __threadfence();
+                    if (atomicAdd(G.pstat + 2 * it.pass + 1, 0) == 0) {
+                        atomicMin(G.trk + 2 * nper, (unsigned)(G.pass0 + it.pass + 1));
+                        if (G.rflag) *(volatile int*)G.rflag = 1;
+                    }
+                }
+            }
             if (census) {   // SM cycles spent waiting on dependencies / computing
                 atomicAdd(census + 0, (unsigned long long)(t_work - t_wait));
                 atomicAdd(census + 1, (unsigned long long)(clock64() - t_work));
+                atomicAdd(census + (compute ? 2 : 3), 1ull);
             }
         }
         t = __shfl_sync(0xffffffffu, next, 0);
@@ -346,20 +428,29 @@ size_t order_batch_items(const BatchGrid* grids, size_t ngrids, BatchItem* out) 
     return n;
 }
 
-template <int W>
+template <int W, bool TR>
 static int ctas_per_sm_of() {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<W>, 32, 0) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<W, TR>, 32, 0) !=
+        cudaSuccess)
         per_sm = 1;
     return std::max(1, per_sm);
 }
 
-int batch_kernel_ctas_per_sm(int wpl_only) {
+int batch_kernel_ctas_per_sm(int wpl_only, bool track) {
+    if (track) {
+        switch (wpl_only) {
+            case 4: return ctas_per_sm_of<4, true>();
+            case 2: return ctas_per_sm_of<2, true>();
+            case 1: return ctas_per_sm_of<1, true>();
+            default: return ctas_per_sm_of<0, true>();
+        }
+    }
     switch (wpl_only) {
-        case 4: return ctas_per_sm_of<4>();
-        case 2: return ctas_per_sm_of<2>();
-        case 1: return ctas_per_sm_of<1>();
-        default: return ctas_per_sm_of<0>();
+        case 4: return ctas_per_sm_of<4, false>();
+        case 2: return ctas_per_sm_of<2, false>();
+        case 1: return ctas_per_sm_of<1, false>();
+        default: return ctas_per_sm_of<0, false>();
     }
 }
 
@@ -390,32 +481,40 @@ void batch_grid_from_choice(const GridChoice& ch, int W, int Y, BatchGrid* g) {
     g->halo = ch.halo;
 }
 
+template <int W, bool TR>
+static void launch_batch_variant(int ctas, cudaStream_t stream, const BatchGrid* g,
+                                 const BatchItem* items, int nitems, int* ticket, int* done,
+                                 int* status, unsigned long long* census, long long spin_limit) {
+    batch_kernel<W, TR><<<ctas, 32, 0, stream>>>(g, items, nitems, ticket, done, status, census,
+                                                 spin_limit);
+}
+
 cudaError_t launch_batch_kernel(const BatchGrid* d_grids, const BatchItem* d_items, int nitems,
                                 int* d_ticket, int* d_done, int* d_status, int num_sms,
                                 cudaStream_t stream, unsigned long long* d_census, int wpl_only,
-                                long long spin_limit) {
+                                long long spin_limit, bool track) {
     if (spin_limit <= 0) spin_limit = kSpinLimit;
     if (nitems <= 0) return cudaSuccess;
     // every CTA resident at once (the dependency waits rely on it)
-    const int ctas = std::min(nitems, num_sms * batch_kernel_ctas_per_sm(wpl_only));
-    switch (wpl_only) {
-        case 4:
-            batch_kernel<4><<<ctas, 32, 0, stream>>>(d_grids, d_items, nitems, d_ticket, d_done,
-                                                     d_status, d_census, spin_limit);
-            break;
-        case 2:
-            batch_kernel<2><<<ctas, 32, 0, stream>>>(d_grids, d_items, nitems, d_ticket, d_done,
-                                                     d_status, d_census, spin_limit);
-            break;
-        case 1:
-            batch_kernel<1><<<ctas, 32, 0, stream>>>(d_grids, d_items, nitems, d_ticket, d_done,
-                                                     d_status, d_census, spin_limit);
-            break;
-        default:
-            batch_kernel<0><<<ctas, 32, 0, stream>>>(d_grids, d_items, nitems, d_ticket, d_done,
-                                                     d_status, d_census, spin_limit);
-            break;
+    const int ctas = std::min(nitems, num_sms * batch_kernel_ctas_per_sm(wpl_only, track));
+#define GOL_BATCH_ARGS ctas, stream, d_grids, d_items, nitems, d_ticket, d_done, d_status, d_census, \
+                       spin_limit
+    if (track) {
+        switch (wpl_only) {
+            case 4: launch_batch_variant<4, true>(GOL_BATCH_ARGS); break;
+            case 2: launch_batch_variant<2, true>(GOL_BATCH_ARGS); break;
+            case 1: launch_batch_variant<1, true>(GOL_BATCH_ARGS); break;
+            default: launch_batch_variant<0, true>(GOL_BATCH_ARGS); break;
+        }
+    } else {
+        switch (wpl_only) {
+            case 4: launch_batch_variant<4, false>(GOL_BATCH_ARGS); break;
+            case 2: launch_batch_variant<2, false>(GOL_BATCH_ARGS); break;
+            case 1: launch_batch_variant<1, false>(GOL_BATCH_ARGS); break;
+            default: launch_batch_variant<0, false>(GOL_BATCH_ARGS); break;
+        }
     }
+#undef GOL_BATCH_ARGS
     return cudaPeekAtLastError();
 }
 
@@ -444,6 +543,12 @@ struct gol_batch {
         int pitch = 0;                    // words per row on the device (W padded to wpl)
         size_t stride = 0;                // words from buf[0] to buf[1] (the input region's size)
         int result_buf = 0;               // buffer holding the last run's result
+        int track_mode = GOL_TRACK_AUTO;  // gol_batch_set_tracking
+        bool tracked = false;             // the uploaded plan tracks changes
+        size_t trk_offset = 0;            // words into d_trk (tracked grids)
+        size_t pstat_offset = 0;          // ints into d_pstat (tracked grids)
+        int tile_rows_hint = 0;           // band height from the last retune (0: the planner's)
+        int auto_track = -1;              // the last retune's choice in auto mode (-1: none yet)
     };
     std::vector<Entry> grids;
 
@@ -458,7 +563,13 @@ struct gol_batch {
     int* d_done = nullptr;
     int* d_ticket = nullptr;
     int* d_status = nullptr;
-    unsigned long long* d_census = nullptr;   // wait / work SM cycles of the last run
+    unsigned long long* d_census = nullptr;   // wait / work SM cycles, items computed / skipped
+    uint32_t* d_trk = nullptr;            // change flags and still pass of the tracked grids
+    size_t trk_words = 0;
+    int* d_pstat = nullptr;               // per pass of each tracked grid: items done, changed
+    size_t pstat_words = 0;
+    uint32_t* d_gstat = nullptr;          // per grid: items computed, skipped
+    bool track_any = false;
     int nitems = 0, ngroups_total = 0;
     int wpl_only = 0;                     // lane width shared by every grid (0: mixed)
     bool uploaded = false, ran = false;
@@ -478,12 +589,25 @@ struct gol_batch {
 
 namespace {
 
+// Grids of at least this many passes track changes unless told otherwise
+// (a short run has little time to settle).
+constexpr int kTrackMinPasses = 8;
+constexpr double kRetuneMinSkip = 0.05;    // skipped share below which a grid runs dense
+constexpr double kRetuneFineSkip = 0.5;    // skipped share from which it gets the finest tiles
+constexpr int kRetuneFineRows = 16;        // the planner's smallest band
+
+int forced_band(const gol_batch::Entry& e) { return e.force_band ? e.force_band : e.tile_rows_hint; }
+
 void batch_free_device(gol_batch* b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
     for (void* p : {(void*)b->arena, (void*)b->d_grids, (void*)b->d_items, (void*)b->d_done,
-                    (void*)b->d_ticket, (void*)b->d_status, (void*)b->d_census})
+                    (void*)b->d_ticket, (void*)b->d_status, (void*)b->d_census, (void*)b->d_trk,
+                    (void*)b->d_pstat, (void*)b->d_gstat})
         if (p) cudaFree(p);
+    b->d_trk = nullptr;
+    b->d_pstat = nullptr;
+    b->d_gstat = nullptr;
     b->arena = nullptr;
     b->d_grids = nullptr;
     b->d_items = nullptr;
@@ -599,7 +723,7 @@ int gol_batch_upload(gol_batch* b) {
                 const auto& e = b->grids[i];
                 ok = golb200::choose_batch_plan(e.W, e.Y, std::max<uint64_t>(e.gens, 1),
                                                 e.force_wpl ? e.force_wpl : wpl,
-                                                e.force_k ? e.force_k : k, e.force_band, &ch[i]);
+                                                e.force_k ? e.force_k : k, forced_band(e), &ch[i]);
                 total_work += ok && e.gens ? ch[i].cost : 0;
             }
             if (!ok) continue;
@@ -607,10 +731,10 @@ int gol_batch_upload(gol_batch* b) {
             double chain = 0;
             for (size_t i = 0; i < b->grids.size(); ++i) {
                 const auto& e = b->grids[i];
-                if (ch[i].crit > GOL_BATCH_REPLAN * work_time && !e.force_band)
+                if (ch[i].crit > GOL_BATCH_REPLAN * work_time && !forced_band(e))
                     golb200::choose_batch_plan(e.W, e.Y, std::max<uint64_t>(e.gens, 1),
                                                e.force_wpl ? e.force_wpl : wpl,
-                                               e.force_k ? e.force_k : k, e.force_band, &ch[i],
+                                               e.force_k ? e.force_k : k, forced_band(e), &ch[i],
                                                par, 1.0);
                 if (e.gens) chain = std::max(chain, ch[i].crit);
             }
@@ -640,13 +764,15 @@ int gol_batch_upload(gol_batch* b) {
         }
         if (first_pass >= 2 * parallel || tallest <= 16) break;
         for (auto& e : b->grids) {
-            if (e.gens == 0 || e.force_band || e.choice.band != tallest) continue;
+            if (e.gens == 0 || forced_band(e) || e.choice.band != tallest) continue;
             golb200::GridChoice c2;
             if (golb200::choose_batch_plan(e.W, e.Y, std::max<uint64_t>(e.gens, 1), e.choice.wpl,
                                            e.choice.k, std::max(16, tallest / 2), &c2))
                 e.choice = c2;
         }
     }
+    size_t trk_words = 0, pstat_words = 0;
+    b->track_any = false;
     for (auto& e : b->grids) {
         if (e.gens == 0) e.choice.passes = 0;
         // Every buffer starts on a 256-byte boundary: lanes move up to 16
@@ -660,8 +786,23 @@ int gol_batch_upload(gol_batch* b) {
         g.done_base = groups;
         groups += g.ngroups * g.nslices;
         max_passes = std::max(max_passes, g.passes);
+        // Change tracking: on or off as set, else (auto) the last retune's
+        // choice, else on for grids of at least kTrackMinPasses passes.
+        e.tracked = g.passes > 0 &&
+                    (e.track_mode == GOL_TRACK_ON ||
+                     (e.track_mode == GOL_TRACK_AUTO &&
+                      (e.auto_track >= 0 ? e.auto_track == 1 : g.passes >= kTrackMinPasses)));
+        if (e.tracked) {
+            e.trk_offset = trk_words;
+            trk_words += golb200::batch_trk_words(g.ngroups, g.nslices);
+            e.pstat_offset = pstat_words;
+            pstat_words += 2 * (size_t)g.passes;
+            b->track_any = true;
+        }
         hg.push_back(g);
     }
+    b->trk_words = trk_words;
+    b->pstat_words = pstat_words;
     std::vector<BatchItem> items(golb200::count_batch_items(hg.data(), hg.size()));
     golb200::order_batch_items(hg.data(), hg.size(), items.data());
     b->nitems = (int)items.size();
@@ -676,7 +817,10 @@ int gol_batch_upload(gol_batch* b) {
     if (ce == cudaSuccess) ce = cudaMalloc(&b->d_done, std::max(groups, 1) * sizeof(int));
     if (ce == cudaSuccess) ce = cudaMalloc(&b->d_ticket, sizeof(int));
     if (ce == cudaSuccess) ce = cudaMalloc(&b->d_status, sizeof(int));
-    if (ce == cudaSuccess) ce = cudaMalloc(&b->d_census, 2 * sizeof(unsigned long long));
+    if (ce == cudaSuccess) ce = cudaMalloc(&b->d_census, 4 * sizeof(unsigned long long));
+    if (ce == cudaSuccess) ce = cudaMalloc(&b->d_trk, std::max<size_t>(trk_words, 1) * sizeof(uint32_t));
+    if (ce == cudaSuccess) ce = cudaMalloc(&b->d_pstat, std::max<size_t>(pstat_words, 1) * sizeof(int));
+    if (ce == cudaSuccess) ce = cudaMalloc(&b->d_gstat, std::max<size_t>(2 * hg.size(), 1) * sizeof(uint32_t));
     if (ce != cudaSuccess) {
         batch_free_device(b);
         return ce == cudaErrorMemoryAllocation ? b->fail(GOL_E_NOMEM, "device allocation failed")
@@ -688,6 +832,11 @@ int gol_batch_upload(gol_batch* b) {
         auto& e = b->grids[gi];
         hg[gi].buf[0] = b->arena + e.offset;
         hg[gi].buf[1] = b->arena + e.offset + e.stride;
+        hg[gi].gstat = b->d_gstat + 2 * gi;
+        if (e.tracked) {
+            hg[gi].trk = b->d_trk + e.trk_offset;
+            hg[gi].pstat = b->d_pstat + e.pstat_offset;
+        }
         if (e.W == 0 || e.Y == 0) continue;
         ce = cudaMemcpy2DAsync(hg[gi].buf[0], (size_t)e.pitch * sizeof(uint32_t), e.words.data(),
                                (size_t)e.W * sizeof(uint32_t), (size_t)e.W * sizeof(uint32_t), e.Y,
@@ -741,11 +890,19 @@ int gol_batch_run(gol_batch* b) {
         if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_done, 0, std::max(b->ngroups_total, 1) * sizeof(int), cs);
         if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_ticket, 0, sizeof(int), cs);
         if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_status, 0, sizeof(int), cs);
-        if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_census, 0, 2 * sizeof(unsigned long long), cs);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_census, 0, 4 * sizeof(unsigned long long), cs);
+        // change tracking: every flag "changed" (the first pass computes
+        // everything), no still pass, counters zero
+        if (ce == cudaSuccess && b->trk_words)
+            ce = cudaMemsetAsync(b->d_trk, 0xff, b->trk_words * sizeof(uint32_t), cs);
+        if (ce == cudaSuccess && b->pstat_words)
+            ce = cudaMemsetAsync(b->d_pstat, 0, b->pstat_words * sizeof(int), cs);
+        if (ce == cudaSuccess)
+            ce = cudaMemsetAsync(b->d_gstat, 0, std::max<size_t>(2 * b->grids.size(), 1) * sizeof(uint32_t), cs);
         if (ce == cudaSuccess)
             ce = golb200::launch_batch_kernel(b->d_grids, b->d_items, b->nitems, b->d_ticket,
                                               b->d_done, b->d_status, b->num_sms, cs, b->d_census,
-                                              b->wpl_only);
+                                              b->wpl_only, 0, b->track_any);
         cudaGraph_t g = nullptr;
         cudaError_t ce2 = cudaStreamEndCapture(cs, &g);
         if (ce == cudaSuccess) ce = ce2;
@@ -888,6 +1045,72 @@ int gol_batch_census(gol_batch* b, uint64_t* wait_cycles, uint64_t* work_cycles)
     if (ce != cudaSuccess) return b->cuda_fail(ce, "batch census");
     if (wait_cycles) *wait_cycles = c[0];
     if (work_cycles) *work_cycles = c[1];
+    return GOL_OK;
+}
+
+int gol_batch_set_tracking(gol_batch* b, int32_t grid_id, int32_t mode) {
+    if (!b || grid_id < 0 || grid_id >= (int)b->grids.size()) return GOL_E_INVALID;
+    if (mode != GOL_TRACK_AUTO && mode != GOL_TRACK_OFF && mode != GOL_TRACK_ON)
+        return b->fail(GOL_E_INVALID, "tracking mode must be GOL_TRACK_AUTO, _OFF or _ON");
+    b->grids[grid_id].track_mode = mode;
+    b->uploaded = false;
+    return GOL_OK;
+}
+
+// The autotuner's second look: each grid in auto mode keeps change tracking
+// if the last run skipped a useful share of its items (at least
+// kRetuneMinSkip; below that the comparisons cost more than they save),
+// and a grid that skipped most of its items gets the finest tiles
+// (kRetuneFineRows-row bands). The next run re-plans and re-uploads.
+int gol_batch_retune(gol_batch* b) {
+    if (!b) return GOL_E_INVALID;
+    if (!b->uploaded || !b->ran) return b->fail(GOL_E_STATE, "retune needs a batched run first");
+    std::vector<uint32_t> st(2 * b->grids.size());
+    cudaError_t ce = cudaStreamSynchronize(b->stream);
+    if (ce == cudaSuccess && !st.empty())
+        ce = cudaMemcpy(st.data(), b->d_gstat, st.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return b->cuda_fail(ce, "batch retune");
+    for (size_t i = 0; i < b->grids.size(); ++i) {
+        auto& e = b->grids[i];
+        if (e.track_mode != GOL_TRACK_AUTO || !e.tracked) continue;
+        const double total = (double)st[2 * i] + st[2 * i + 1];
+        if (total <= 0) continue;
+        const double skip = st[2 * i + 1] / total;
+        e.auto_track = skip >= kRetuneMinSkip ? 1 : 0;
+        e.tile_rows_hint = (e.auto_track == 1 && skip >= kRetuneFineSkip) ? kRetuneFineRows : 0;
+    }
+    b->uploaded = false;
+    return GOL_OK;
+}
+
+int gol_batch_tiles(gol_batch* b, uint64_t* computed, uint64_t* skipped) {
+    if (!b || !b->d_census) return GOL_E_INVALID;
+    unsigned long long c[4] = {0, 0, 0, 0};
+    cudaError_t ce = cudaStreamSynchronize(b->stream);
+    if (ce == cudaSuccess) ce = cudaMemcpy(c, b->d_census, sizeof(c), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return b->cuda_fail(ce, "batch census");
+    if (computed) *computed = c[2];
+    if (skipped) *skipped = c[3];
+    return GOL_OK;
+}
+
+int gol_batch_grid_stats(gol_batch* b, int32_t grid_id, uint32_t* tracked, uint32_t* computed,
+                         uint32_t* skipped, uint32_t* still_pass) {
+    if (!b || grid_id < 0 || grid_id >= (int)b->grids.size()) return GOL_E_INVALID;
+    if (!b->uploaded || !b->ran) return b->fail(GOL_E_STATE, "no batched run yet");
+    const auto& e = b->grids[grid_id];
+    uint32_t st[2] = {0, 0}, still = 0xffffffffu;
+    cudaError_t ce = cudaStreamSynchronize(b->stream);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpy(st, b->d_gstat + 2 * (size_t)grid_id, sizeof(st), cudaMemcpyDeviceToHost);
+    if (ce == cudaSuccess && e.tracked)
+        ce = cudaMemcpy(&still, b->d_trk + e.trk_offset + 2 * (size_t)e.choice.ngroups * e.choice.nslices,
+                        sizeof(still), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return b->cuda_fail(ce, "batch grid stats");
+    if (tracked) *tracked = e.tracked ? 1u : 0u;
+    if (computed) *computed = st[0];
+    if (skipped) *skipped = st[1];
+    if (still_pass) *still_pass = still;
     return GOL_OK;
 }
 

@@ -110,7 +110,23 @@ struct BatchGrid {
     int halo;              // halo words each side of a slice (0 when unsliced)
     int done_base;         // offset of this grid's (group, slice) counters
     int parity0;           // buffer holding the grid at the start of the launch
+    // Change tracking (trk null: every item is computed). An item is a tile:
+    // it is recomputed only if it or one of its 3x3 neighbour items changed
+    // in the previous pass.
+    uint32_t* trk;         // [2][ngroups * nslices] change flags by absolute pass
+                           // parity (parity0 + pass) & 1, nonzero = changed; then one
+                           // word: the pass from which nothing changes (0xFFFFFFFF: none)
+    int* pstat;            // per pass of this launch: [items done, items changed]
+    uint32_t* gstat;       // items computed, items skipped (accumulated)
+    int* rflag;            // set to 1 once the grid is known to be still (may be null)
+    int pass0;             // passes this grid ran in earlier launches (the still pass
+                           // in trk counts from the grid's first launch)
 };
+
+// Words of a grid's change-tracking region (trk).
+inline size_t batch_trk_words(int ngroups, int nslices) {
+    return 2 * (size_t)ngroups * nslices + 1;
+}
 
 struct BatchItem {
     int grid, group, slice, pass;
@@ -137,8 +153,8 @@ size_t order_batch_items(const BatchGrid* grids, size_t ngrids, BatchItem* out);
 size_t count_batch_items(const BatchGrid* grids, size_t ngrids);
 
 // Resident one-warp CTAs per SM of the batch kernel built for one lane
-// width (1, 2, 4) or for any (0).
-int batch_kernel_ctas_per_sm(int wpl_only = 0);
+// width (1, 2, 4) or for any (0), without or with change tracking.
+int batch_kernel_ctas_per_sm(int wpl_only = 0, bool track = false);
 
 // The lane width every grid with work shares, or 0 when they differ.
 int batch_uniform_wpl(const BatchGrid* grids, size_t ngrids);
@@ -150,10 +166,12 @@ void batch_grid_from_choice(const GridChoice& ch, int W, int Y, BatchGrid* g);
 // order); done[] and *ticket, *status must be zero. All CTAs fit at once.
 // wpl_only: the lane width all grids share (batch_uniform_wpl), or 0.
 // spin_limit: polls before a dependency wait gives up (0 = the default guard).
+// track: some grid has change tracking (the kernel variant that compares
+// every stored word with its input).
 cudaError_t launch_batch_kernel(const BatchGrid* d_grids, const BatchItem* d_items, int nitems,
                                 int* d_ticket, int* d_done, int* d_status, int num_sms,
                                 cudaStream_t stream, unsigned long long* d_census = nullptr,
-                                int wpl_only = 0, long long spin_limit = 0);
+                                int wpl_only = 0, long long spin_limit = 0, bool track = false);
 
 cudaError_t launch_pack_cells(const uint8_t* cells, uint32_t* words, size_t x, size_t y,
                               cudaStream_t stream);

@@ -34,7 +34,10 @@
 namespace golb200 {
 
 constexpr int kStreamMaxThreads = 256;
-constexpr int kStreamAhead = 6;   // rows in flight per thread (multiple of 3)
+#ifndef GOL_STREAM_AHEAD
+#define GOL_STREAM_AHEAD 6
+#endif
+constexpr int kStreamAhead = GOL_STREAM_AHEAD;   // rows in flight per thread (multiple of 3)
 
 template <int WPL>
 __device__ __forceinline__ void stream_load(const uint32_t* p, bool v, uint32_t (&w)[WPL]) {

@@ -33,6 +33,8 @@
 namespace {
 
 constexpr int kRoundsInFlight = 3;
+constexpr uint64_t kServeTrackMinPasses = 8;   // auto: requests this long track changes
+constexpr double kServeRefCells = 1024.0 * 1024.0;
 
 struct Request {
     uint64_t id = 0;
@@ -45,6 +47,9 @@ struct Request {
     uint64_t input_seed = 0;
     double input_density = 0;
     size_t offset = 0, stride = 0;
+    size_t slot_words = 0;      // 2 * stride + the change-tracking region, rounded up
+    bool tracked = false;       // skips still tiles (its flags live in its slot)
+    bool early = false;         // finished before its last planned round: it became still
     int parity = 0;             // buffer holding the state after the rounds queued so far
     golb200::GridChoice plan{};
     int state = 0;              // 0 queued, 1 admitted, 2 finished (after its last round), 3 fetched
@@ -59,7 +64,11 @@ struct RoundBuffers {
     int* d_ticket = nullptr;
     int* d_status = nullptr;
     int* h_status = nullptr;                 // pinned copy, written by the round's stream
-    size_t cap_grids = 0, cap_items = 0, cap_done = 0;
+    int* d_pstat = nullptr;                  // per pass of each tracked request
+    int* d_still = nullptr;                  // per request of the round: it is still
+    int* h_still = nullptr;                  // pinned copy
+    size_t cap_grids = 0, cap_items = 0, cap_done = 0, cap_pstat = 0, cap_still = 0;
+    std::vector<uint64_t> ids;               // request of each grid of the round
     golb200::BatchGrid* h_grids = nullptr;   // pinned staging
     golb200::BatchItem* h_items = nullptr;
     cudaEvent_t done_event = nullptr;
@@ -80,6 +89,10 @@ struct gol_server {
     size_t arena_words = 0;
     std::map<size_t, size_t> free_blocks;   // offset -> length (words)
     uint64_t quantum = 128;
+    int policy = GOL_SERVE_FIFO;
+    int track_mode = GOL_TRACK_AUTO;
+    unsigned long long* d_census = nullptr;   // wait / work cycles, items computed / skipped
+    uint64_t early_finished = 0;
     uint64_t next_id = 1;
     std::unordered_map<uint64_t, Request> reqs;
     std::deque<uint64_t> queue;             // waiting for memory
@@ -134,7 +147,8 @@ void arena_free(gol_server* s, size_t off, size_t words) {
     }
 }
 
-int ensure_round_capacity(gol_server* s, RoundBuffers& r, size_t grids, size_t items, size_t done) {
+int ensure_round_capacity(gol_server* s, RoundBuffers& r, size_t grids, size_t items, size_t done,
+                          size_t pstat) {
     cudaError_t ce = cudaSuccess;
     auto grow = [&](size_t need, size_t& cap, auto** dptr, auto** hptr) {
         if (need <= cap || ce != cudaSuccess) return;
@@ -149,6 +163,8 @@ int ensure_round_capacity(gol_server* s, RoundBuffers& r, size_t grids, size_t i
     grow(std::max<size_t>(grids, 1), r.cap_grids, &r.d_grids, &r.h_grids);
     grow(std::max<size_t>(items, 1), r.cap_items, &r.d_items, &r.h_items);
     grow(std::max<size_t>(done, 1), r.cap_done, &r.d_done, static_cast<int**>(nullptr));
+    grow(std::max<size_t>(pstat, 1), r.cap_pstat, &r.d_pstat, static_cast<int**>(nullptr));
+    grow(std::max<size_t>(grids, 1), r.cap_still, &r.d_still, &r.h_still);
     if (ce == cudaSuccess && !r.d_ticket) ce = cudaMalloc(&r.d_ticket, sizeof(int));
     if (ce == cudaSuccess && !r.d_status) ce = cudaMalloc(&r.d_status, sizeof(int));
     if (ce == cudaSuccess && !r.h_status) ce = cudaMallocHost(&r.h_status, sizeof(int));
@@ -173,6 +189,30 @@ int retire_round(gol_server* s, RoundBuffers& r) {
         }
     }
     r.finishing.clear();
+    // A request found still in this round (a whole k-generation pass changed
+    // nothing, so its state repeats every k generations and both of its
+    // buffers hold it): if k divides its generation count it is done now,
+    // whatever rounds are still queued for it (their passes end at once). If
+    // not, only the remainder (fewer than k generations) is left to plan;
+    // rounds already queued for it end at once until that last short pass.
+    for (size_t i = 0; i < r.ids.size(); ++i) {
+        if (!r.h_still[i]) continue;
+        auto it = s->reqs.find(r.ids[i]);
+        if (it == s->reqs.end() || it->second.state != 1) continue;
+        Request& q = it->second;
+        const uint64_t k = (uint64_t)q.plan.k;
+        auto run = std::find(s->running.begin(), s->running.end(), r.ids[i]);
+        if (q.gens % k == 0) {
+            q.state = 2;
+            q.early = true;
+            s->finished.push_back(r.ids[i]);
+            if (run != s->running.end()) s->running.erase(run);
+            ++s->early_finished;
+        } else if (run != s->running.end()) {
+            q.planned = std::max(q.planned, q.gens - q.gens % k);
+        }
+    }
+    r.ids.clear();
     return GOL_OK;
 }
 
@@ -226,7 +266,11 @@ int gol_serve_create(gol_server** out, int32_t device, uint64_t arena_bytes, uin
         s->arena_words = arena_bytes / sizeof(uint32_t) / 64 * 64;
         ce = cudaMalloc(&s->arena, std::max<size_t>(s->arena_words, 64) * sizeof(uint32_t));
     }
+    if (ce == cudaSuccess) ce = cudaMalloc(&s->d_census, 4 * sizeof(unsigned long long));
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(s->d_census, 0, 4 * sizeof(unsigned long long), s->stream);
     if (ce != cudaSuccess) {
+        if (s->arena) cudaFree(s->arena);
+        if (s->d_census) cudaFree(s->d_census);
         if (s->own_stream) cudaStreamDestroy(s->stream);
         if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
         delete s;
@@ -240,10 +284,44 @@ int gol_serve_create(gol_server** out, int32_t device, uint64_t arena_bytes, uin
 
 // Every request runs 2 words per lane (1 for an odd word count) at depth
 // 4 with its own band height, so a round's launch holds one pipeline family
-// (mixed families on one SM compete for the instruction cache).
-static bool plan_request(Request& r, uint64_t generations) {
-    return golb200::choose_batch_plan(r.W, r.Y, std::max<uint64_t>(generations, 1), r.W % 2 ? 1 : 2,
-                                      golb200::kBatchMaxK, 0, &r.plan);
+// (mixed families on one SM compete for the instruction cache). Its slot in
+// the arena: the two grid buffers, two counters (items computed / skipped)
+// and, when it tracks changes, its change flags and still pass (the
+// batch kernel's tracking region), kept for the request's whole life.
+static bool plan_request(gol_server* s, Request& r, uint64_t generations) {
+    if (!golb200::choose_batch_plan(r.W, r.Y, std::max<uint64_t>(generations, 1), r.W % 2 ? 1 : 2,
+                                    golb200::kBatchMaxK, 0, &r.plan))
+        return false;
+    const uint64_t passes = (generations + r.plan.k - 1) / r.plan.k;
+    r.tracked = s->track_mode == GOL_TRACK_ON ||
+                (s->track_mode == GOL_TRACK_AUTO && passes >= kServeTrackMinPasses);
+    r.stride = ((size_t)r.W * r.Y + 63) / 64 * 64;
+    const size_t extra = 2 + (r.tracked ? golb200::batch_trk_words(r.plan.ngroups, r.plan.nslices) : 0);
+    r.slot_words = 2 * r.stride + (extra + 63) / 64 * 64;
+    return true;
+}
+
+static uint32_t* slot_gstat(gol_server* s, const Request& r) { return s->arena + r.offset + 2 * r.stride; }
+static uint32_t* slot_trk(gol_server* s, const Request& r) { return slot_gstat(s, r) + 2; }
+
+// Generations a request advances in one round: the quantum, or under the
+// shortest-work-first policy the quantum scaled up for grids smaller than
+// kServeRefCells cells (so small requests finish in few rounds while a
+// round's work stays bounded by the large ones' quantum).
+// Every round but a request's last advances a multiple of its depth k, so
+// its change flags (which speak of k-generation passes) stay valid from
+// round to round; only the last round may end with a shorter pass.
+static uint64_t round_generations(const gol_server* s, const Request& r) {
+    const uint64_t left = r.gens - r.planned;
+    const uint64_t k = (uint64_t)r.plan.k;
+    uint64_t q = s->quantum;
+    if (s->policy == GOL_SERVE_SRPT) {
+        const double cells = (double)r.x * (double)r.y;
+        const double scale = std::max(1.0, kServeRefCells / std::max(cells, 1.0));
+        q = (uint64_t)std::min<double>((double)s->quantum * scale, 1e12);
+    }
+    q = std::max(k, q / k * k);
+    return left <= q ? left : q;
 }
 
 int gol_serve_submit(gol_server* s, const uint8_t* cells, uint64_t x, uint64_t y,
@@ -258,9 +336,8 @@ int gol_serve_submit(gol_server* s, const uint8_t* cells, uint64_t x, uint64_t y
     r.W = (int)(x / 32);
     r.Y = (int)y;
     r.gens = generations;
-    r.stride = ((size_t)r.W * r.Y + 63) / 64 * 64;
-    if (2 * r.stride > s->arena_words) return s->fail(GOL_E_NOMEM, "request larger than the device arena");
-    if (!plan_request(r, generations)) return s->fail(GOL_E_UNSUPPORTED, "no plan for this request");
+    if (!plan_request(s, r, generations)) return s->fail(GOL_E_UNSUPPORTED, "no plan for this request");
+    if (r.slot_words > s->arena_words) return s->fail(GOL_E_NOMEM, "request larger than the device arena");
     r.words.resize((size_t)r.W * r.Y);
     golb200::host_pack_u8(cells, x, y, r.words.data());
     if (id) *id = r.id;
@@ -287,9 +364,8 @@ int gol_serve_submit_random(gol_server* s, uint64_t x, uint64_t y, uint64_t gene
     r.device_input = true;
     r.input_seed = seed;
     r.input_density = density;
-    r.stride = ((size_t)r.W * r.Y + 63) / 64 * 64;
-    if (2 * r.stride > s->arena_words) return s->fail(GOL_E_NOMEM, "request larger than the device arena");
-    if (!plan_request(r, generations)) return s->fail(GOL_E_UNSUPPORTED, "no plan for this request");
+    if (!plan_request(s, r, generations)) return s->fail(GOL_E_UNSUPPORTED, "no plan for this request");
+    if (r.slot_words > s->arena_words) return s->fail(GOL_E_NOMEM, "request larger than the device arena");
     if (id) *id = r.id;
     s->queue.push_back(r.id);
     s->reqs.emplace(r.id, std::move(r));
@@ -307,12 +383,18 @@ int gol_serve_step(gol_server* s) {
     int rc = harvest(s, false);
     if (rc) return rc;
 
-    // Admission: arrival order; a request that does not fit lets later,
-    // smaller ones through (its memory is reserved for it first next time).
+    // Admission: arrival order (FIFO) or least work first (SRPT: cells x
+    // generations); a request that does not fit lets later ones through.
+    if (s->policy == GOL_SERVE_SRPT && s->queue.size() > 1)
+        std::stable_sort(s->queue.begin(), s->queue.end(), [s](uint64_t a, uint64_t b) {
+            const Request& ra = s->reqs[a];
+            const Request& rb = s->reqs[b];
+            return (double)ra.x * ra.y * ra.gens < (double)rb.x * rb.y * rb.gens;
+        });
     for (auto it = s->queue.begin(); it != s->queue.end();) {
         Request& r = s->reqs[*it];
         size_t off = 0;
-        if (!arena_alloc(s, 2 * r.stride, &off)) {
+        if (!arena_alloc(s, r.slot_words, &off)) {
             ++it;
             continue;
         }
@@ -326,6 +408,13 @@ int gol_serve_step(gol_server* s) {
             ce = cudaMemcpyAsync(s->arena + off, r.words.data(), r.words.size() * sizeof(uint32_t),
                                  cudaMemcpyHostToDevice, s->stream);
         }
+        // counters zero; change flags "changed" (the first pass computes
+        // every tile) and no still pass
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(slot_gstat(s, r), 0, 2 * sizeof(uint32_t), s->stream);
+        if (ce == cudaSuccess && r.tracked)
+            ce = cudaMemsetAsync(slot_trk(s, r), 0xff,
+                                 golb200::batch_trk_words(r.plan.ngroups, r.plan.nslices) * sizeof(uint32_t),
+                                 s->stream);
         if (ce != cudaSuccess) return s->cuda_fail(ce, "request upload");
         std::vector<uint32_t>().swap(r.words);   // a pageable source is staged before the call returns
         if (r.gens == 0) {               // nothing to run: finished at once
@@ -344,14 +433,18 @@ int gol_serve_step(gol_server* s) {
         rc = harvest(s, true);
         if (rc) return rc;
     }
-    // Plan this round: every running request advances min(quantum, left).
+    // Plan this round: every running request advances its round's
+    // generations (round_generations).
     std::vector<golb200::BatchGrid> grids;
     int done = 0, max_passes = 0;
+    size_t pstat = 0;
+    bool track_any = false;
+    std::vector<size_t> pstat_off;   // per grid: its pass counters in rb.d_pstat (tracked grids)
     std::vector<uint64_t> still;
+    rb.ids.clear();
     for (uint64_t id : s->running) {
         Request& r = s->reqs[id];
-        const uint64_t left = r.gens - r.planned;
-        const uint64_t g = std::min<uint64_t>(left, s->quantum);
+        const uint64_t g = round_generations(s, r);
         golb200::GridChoice ch = r.plan;
         ch.passes = (int)((g + ch.k - 1) / ch.k);
         ch.last_k = g % ch.k ? (int)(g % ch.k) : ch.k;
@@ -360,9 +453,18 @@ int gol_serve_step(gol_server* s) {
         bg.buf[0] = s->arena + r.offset;
         bg.buf[1] = s->arena + r.offset + r.stride;
         bg.parity0 = r.parity;
+        bg.pass0 = (int)std::min<uint64_t>(r.planned / (uint64_t)ch.k, 0x3fffffff);
         bg.done_base = done;
         done += bg.ngroups * bg.nslices;
         max_passes = std::max(max_passes, bg.passes);
+        bg.gstat = slot_gstat(s, r);
+        pstat_off.push_back(pstat);
+        if (r.tracked) {   // flags and still pass stay in the slot between rounds
+            bg.trk = slot_trk(s, r);
+            pstat += 2 * (size_t)bg.passes;
+            track_any = true;
+        }
+        rb.ids.push_back(id);
         grids.push_back(bg);
         r.planned += g;
         r.parity = (r.parity + ch.passes) & 1;
@@ -375,7 +477,11 @@ int gol_serve_step(gol_server* s) {
     }
     s->running.swap(still);
     const size_t nitems = golb200::count_batch_items(grids.data(), grids.size());
-    if ((rc = ensure_round_capacity(s, rb, grids.size(), nitems, (size_t)done))) return rc;
+    if ((rc = ensure_round_capacity(s, rb, grids.size(), nitems, (size_t)done, pstat))) return rc;
+    for (size_t i = 0; i < grids.size(); ++i) {
+        grids[i].rflag = rb.d_still + i;
+        if (grids[i].trk) grids[i].pstat = rb.d_pstat + pstat_off[i];
+    }
     golb200::order_batch_items(grids.data(), grids.size(), rb.h_items);
     (void)max_passes;
     std::memcpy(rb.h_grids, grids.data(), grids.size() * sizeof(golb200::BatchGrid));
@@ -387,12 +493,18 @@ int gol_serve_step(gol_server* s) {
     if (ce == cudaSuccess) ce = cudaMemsetAsync(rb.d_done, 0, (size_t)std::max(done, 1) * sizeof(int), s->stream);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(rb.d_ticket, 0, sizeof(int), s->stream);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(rb.d_status, 0, sizeof(int), s->stream);
+    if (ce == cudaSuccess && pstat) ce = cudaMemsetAsync(rb.d_pstat, 0, pstat * sizeof(int), s->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(rb.d_still, 0, grids.size() * sizeof(int), s->stream);
     if (ce == cudaSuccess)
         ce = golb200::launch_batch_kernel(rb.d_grids, rb.d_items, (int)nitems, rb.d_ticket, rb.d_done,
-                                          rb.d_status, s->num_sms, s->stream, nullptr,
-                                          golb200::batch_uniform_wpl(grids.data(), grids.size()));
+                                          rb.d_status, s->num_sms, s->stream, s->d_census,
+                                          golb200::batch_uniform_wpl(grids.data(), grids.size()), 0,
+                                          track_any);
     if (ce == cudaSuccess)
         ce = cudaMemcpyAsync(rb.h_status, rb.d_status, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(rb.h_still, rb.d_still, grids.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                             s->stream);
     if (ce == cudaSuccess) ce = cudaEventRecord(rb.done_event, s->stream);
     if (ce != cudaSuccess) return s->cuda_fail(ce, "round launch");
     rb.in_flight = true;
@@ -425,9 +537,10 @@ int gol_serve_fetch(gol_server* s, uint64_t id, uint8_t* cells) {
     if (it == s->reqs.end()) return s->fail(GOL_E_INVALID, "unknown request");
     Request& r = it->second;
     if (r.state != 2) return s->fail(GOL_E_STATE, "request not finished");
-    // Its last round has completed and no later round touches its slot, so
-    // the copy runs on its own stream, beside the rounds still queued. A
-    // request with no generations never ran: wait for its upload instead.
+    // Its last round has completed and no later round writes its grid (a
+    // request finished early is still: rounds still queued for it end at
+    // once), so the copy runs on its own stream, beside the rounds still
+    // queued. A request with no generations never ran: wait for its upload.
     cudaError_t ce = cudaSuccess;
     if (r.gens == 0) ce = cudaStreamSynchronize(s->stream);
     std::vector<uint32_t> words((size_t)r.W * r.Y);
@@ -437,7 +550,7 @@ int gol_serve_fetch(gol_server* s, uint64_t id, uint8_t* cells) {
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->copy_stream);
     if (ce != cudaSuccess) return s->cuda_fail(ce, "result copy");
     golb200::host_unpack_u8(words.data(), r.x, r.y, cells);
-    arena_free(s, r.offset, 2 * r.stride);
+    arena_free(s, r.offset, r.slot_words);
     s->reqs.erase(it);
     return GOL_OK;
 }
@@ -456,7 +569,7 @@ int gol_serve_fetch_words(gol_server* s, uint64_t id, void* words) {
                              (size_t)r.W * r.Y * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->copy_stream);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->copy_stream);
     if (ce != cudaSuccess) return s->cuda_fail(ce, "result copy");
-    arena_free(s, r.offset, 2 * r.stride);
+    arena_free(s, r.offset, r.slot_words);
     s->reqs.erase(it);
     return GOL_OK;
 }
@@ -467,7 +580,7 @@ int gol_serve_release(gol_server* s, uint64_t id) {
     auto it = s->reqs.find(id);
     if (it == s->reqs.end()) return s->fail(GOL_E_INVALID, "unknown request");
     if (it->second.state != 2) return s->fail(GOL_E_STATE, "request not finished");
-    arena_free(s, it->second.offset, 2 * it->second.stride);
+    arena_free(s, it->second.offset, it->second.slot_words);
     s->reqs.erase(it);
     return GOL_OK;
 }
@@ -496,6 +609,33 @@ int gol_serve_drain(gol_server* s) {
     return GOL_OK;
 }
 
+int gol_serve_set_policy(gol_server* s, int32_t policy) {
+    if (!s) return GOL_E_INVALID;
+    if (policy != GOL_SERVE_FIFO && policy != GOL_SERVE_SRPT)
+        return s->fail(GOL_E_INVALID, "policy must be GOL_SERVE_FIFO or GOL_SERVE_SRPT");
+    s->policy = policy;
+    return GOL_OK;
+}
+
+int gol_serve_set_tracking(gol_server* s, int32_t mode) {
+    if (!s) return GOL_E_INVALID;
+    if (mode != GOL_TRACK_AUTO && mode != GOL_TRACK_OFF && mode != GOL_TRACK_ON)
+        return s->fail(GOL_E_INVALID, "tracking mode must be GOL_TRACK_AUTO, _OFF or _ON");
+    s->track_mode = mode;
+    return GOL_OK;
+}
+
+int gol_serve_tiles(gol_server* s, uint64_t* computed, uint64_t* skipped, uint64_t* early_finished) {
+    if (!s) return GOL_E_INVALID;
+    unsigned long long c[4] = {0, 0, 0, 0};
+    cudaError_t ce = cudaMemcpy(c, s->d_census, sizeof(c), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return s->cuda_fail(ce, "serving census");
+    if (computed) *computed = c[2];
+    if (skipped) *skipped = c[3];
+    if (early_finished) *early_finished = s->early_finished;
+    return GOL_OK;
+}
+
 const char* gol_serve_last_error(const gol_server* s) { return s ? s->err.c_str() : "null server"; }
 
 void* gol_serve_stream(gol_server* s) { return s ? static_cast<void*>(s->stream) : nullptr; }
@@ -512,9 +652,13 @@ void gol_serve_destroy(gol_server* s) {
         if (r.h_grids) cudaFreeHost(r.h_grids);
         if (r.h_status) cudaFreeHost(r.h_status);
         if (r.h_items) cudaFreeHost(r.h_items);
+        if (r.d_pstat) cudaFree(r.d_pstat);
+        if (r.d_still) cudaFree(r.d_still);
+        if (r.h_still) cudaFreeHost(r.h_still);
         if (r.done_event) cudaEventDestroy(r.done_event);
     }
     if (s->arena) cudaFree(s->arena);
+    if (s->d_census) cudaFree(s->d_census);
     if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;

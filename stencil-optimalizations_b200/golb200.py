@@ -155,6 +155,10 @@ def lib():
     L.gol_batch_fetch.argtypes = [_vp, ctypes.c_int32, _vp]
     L.gol_batch_info.argtypes = [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u64)]
     L.gol_batch_census.argtypes = [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]
+    L.gol_batch_set_tracking.argtypes = [_vp, ctypes.c_int32, ctypes.c_int32]
+    L.gol_batch_retune.argtypes = [_vp]
+    L.gol_batch_tiles.argtypes = [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]
+    L.gol_batch_grid_stats.argtypes = [_vp, ctypes.c_int32] + [ctypes.POINTER(_u32)] * 4
     L.gol_batch_stream.argtypes = [_vp]
     L.gol_batch_stream.restype = _vp
     L.gol_batch_last_error.argtypes = [_vp]
@@ -174,6 +178,9 @@ def lib():
     L.gol_serve_release.argtypes = [_vp, _u64]
     L.gol_serve_stats.argtypes = [_vp] + [ctypes.POINTER(_u64)] * 5
     L.gol_serve_drain.argtypes = [_vp]
+    L.gol_serve_set_policy.argtypes = [_vp, ctypes.c_int32]
+    L.gol_serve_set_tracking.argtypes = [_vp, ctypes.c_int32]
+    L.gol_serve_tiles.argtypes = [_vp] + [ctypes.POINTER(_u64)] * 3
     L.gol_serve_last_error.argtypes = [_vp]
     L.gol_serve_last_error.restype = ctypes.c_char_p
     L.gol_serve_stream.argtypes = [_vp]
@@ -665,6 +672,31 @@ class GolBatch:
         self._check(lib().gol_batch_census(self._b, ctypes.byref(w), ctypes.byref(c)), "batch_census")
         return {"wait_cycles": w.value, "work_cycles": c.value}
 
+    TRACK = {"auto": 0, "off": 1, "on": 2}
+
+    def set_tracking(self, gid: int, mode: str = "auto") -> None:
+        """Change tracking of one grid: "auto" (the autotuner's choice),
+        "off" (every item computed) or "on"."""
+        self._check(lib().gol_batch_set_tracking(self._b, gid, self.TRACK[mode]),
+                    "batch_set_tracking")
+
+    def retune(self) -> None:
+        """Per-grid tracking and tile choice from the last run's census."""
+        self._check(lib().gol_batch_retune(self._b), "batch_retune")
+
+    def tiles(self) -> dict:
+        """Work items of the last run computed and skipped."""
+        c, k = _u64(), _u64()
+        self._check(lib().gol_batch_tiles(self._b, ctypes.byref(c), ctypes.byref(k)), "batch_tiles")
+        return {"computed": c.value, "skipped": k.value}
+
+    def grid_stats(self, gid: int) -> dict:
+        t, c, k, st = _u32(), _u32(), _u32(), _u32()
+        self._check(lib().gol_batch_grid_stats(self._b, gid, ctypes.byref(t), ctypes.byref(c),
+                                               ctypes.byref(k), ctypes.byref(st)), "batch_grid_stats")
+        return {"tracked": bool(t.value), "computed": c.value, "skipped": k.value,
+                "still_pass": None if st.value == 0xFFFFFFFF else st.value}
+
     def stream_ptr(self) -> int:
         return int(lib().gol_batch_stream(self._b) or 0)
 
@@ -762,6 +794,22 @@ class GolServer:
 
     def drain(self) -> None:
         self._check(lib().gol_serve_drain(self._s), "serve_drain")
+
+    POLICIES = {"fifo": 0, "srpt": 1}
+
+    def set_policy(self, policy: str) -> None:
+        """"fifo" (arrival order, fixed quantum) or "srpt" (least work first,
+        small grids get more generations per round)."""
+        self._check(lib().gol_serve_set_policy(self._s, self.POLICIES[policy]), "serve_set_policy")
+
+    def set_tracking(self, mode: str) -> None:
+        self._check(lib().gol_serve_set_tracking(self._s, GolBatch.TRACK[mode]), "serve_set_tracking")
+
+    def tiles(self) -> dict:
+        c, k, e = _u64(), _u64(), _u64()
+        self._check(lib().gol_serve_tiles(self._s, ctypes.byref(c), ctypes.byref(k), ctypes.byref(e)),
+                    "serve_tiles")
+        return {"computed": c.value, "skipped": k.value, "early_finished": e.value}
 
     def close(self) -> None:
         if self._s:

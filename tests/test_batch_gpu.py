@@ -122,3 +122,97 @@ def test_dependency_wait_gives_up_with_a_status():
         b.run()
         b.sync()
         assert np.array_equal(b.fetch(gid), oracle.life_cells(c, 17))
+
+
+# --- change tracking inside the batch -------------------------------------
+
+GLIDER = np.array([[0, 1, 0], [0, 0, 1], [1, 1, 1]], dtype=np.uint8)
+
+
+def settling_workload():
+    """Grids that settle or stay sparse: dead grids with a few patches of
+    Bernoulli(0.35) soup, a lone glider crossing item boundaries (also in an
+    x-sliced grid), blinkers, an all-dead grid and one dense soup."""
+    work = []
+    for i, (x, y) in enumerate([(1024, 512), (2048, 256), (512, 1024), (4096, 128)]):
+        work.append((golb200.load_sparse_patches(x, y, 50 + i, 64, 0.05, 0.35), 300 + 97 * i))
+    g = np.zeros((256, 5120), np.uint8)             # 160 words: x-sliced
+    g[10:13, 900:903] = GLIDER
+    g[100:103, 2000:2003] = GLIDER
+    work.append((g, 400))
+    g = np.zeros((300, 96), np.uint8)               # narrow: segmented warps
+    g[5:8, 40:43] = GLIDER
+    work.append((g, 257))
+    g = np.zeros((128, 256), np.uint8)
+    g[60, 100:103] = 1                              # a blinker (period 2)
+    work.append((g, 101))
+    work.append((np.zeros((64, 640), np.uint8), 50))
+    work.append((oracle.random_ones_zeros(768, 96, 9), 333))
+    return work
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4])
+def test_batch_tracking_settling_vs_oracle(k):
+    work = settling_workload()
+    with golb200.GolBatch() as b:
+        ids = []
+        for c, n in work:
+            gid = b.add(c, n)
+            b.set_plan(gid, 0, k, 0)
+            b.set_tracking(gid, "on")
+            ids.append(gid)
+        b.run()
+        b.sync()
+        for gid, (c, n) in zip(ids, work):
+            assert np.array_equal(b.fetch(gid), oracle.life_cells(c, n)), (gid, c.shape, n, k)
+        t = b.tiles()
+        assert t["skipped"] > 0 and t["computed"] > 0
+        stats = [b.grid_stats(g) for g in ids]
+        assert all(s["tracked"] for s in stats)
+        # all dead: pass 0 computes every item and changes nothing, so the
+        # grid is still from pass 1 and every later item is skipped
+        assert stats[7]["still_pass"] == 1
+        passes = -(-50 // b.plan(ids[7])["temporal_steps"])
+        assert stats[7]["skipped"] == stats[7]["computed"] * (passes - 1)
+        # a run again from the same inputs gives the same grids
+        b.run()
+        b.sync()
+        for gid, (c, n) in zip(ids, work):
+            assert np.array_equal(b.fetch(gid), oracle.life_cells(c, n)), (gid, "rerun", k)
+
+
+def test_batch_tracked_and_dense_grids_in_one_launch():
+    work = settling_workload()
+    with golb200.GolBatch() as b:
+        ids = []
+        for i, (c, n) in enumerate(work):
+            gid = b.add(c, n)
+            b.set_tracking(gid, "on" if i % 2 else "off")
+            ids.append(gid)
+        b.run()
+        b.sync()
+        for gid, (c, n) in zip(ids, work):
+            assert np.array_equal(b.fetch(gid), oracle.life_cells(c, n)), (gid, c.shape, n)
+            assert b.grid_stats(gid)["tracked"] == bool(gid % 2)
+            if not gid % 2:
+                assert b.grid_stats(gid)["skipped"] == 0
+
+
+def test_batch_retune_keeps_results():
+    """The autotuner's second look (per-grid tracking and tile rows from the
+    first run's census) re-plans the batch; results stay bit-exact."""
+    work = settling_workload()
+    with golb200.GolBatch() as b:
+        ids = [b.add(c, n) for c, n in work]
+        b.run()
+        b.sync()
+        first = [b.fetch(g) for g in ids]
+        b.retune()
+        b.run()
+        b.sync()
+        for gid, (c, n) in zip(ids, work):
+            got = b.fetch(gid)
+            assert np.array_equal(got, first[gid])
+            assert np.array_equal(got, oracle.life_cells(c, n)), (gid, c.shape, n)
+        # the dense soup keeps computing most items; the dead grid is still at once
+        assert b.grid_stats(7)["still_pass"] in (1, None)

@@ -79,3 +79,81 @@ def test_poisson_stream_small():
                          gens=(16, 512), quantum=64, arena_bytes=512 << 20)
     assert r["requests"] > 50
     assert r["latency_p99_ms"] >= r["latency_p50_ms"] > 0
+
+
+def settling_requests():
+    """Inputs that settle: sparse soup patches in dead grids, a lone blinker
+    (period 2, so a 4-generation pass leaves it as it was and its tiles look
+    still), an all-dead grid and a block (a still life from the start), plus
+    one dense soup."""
+    reqs = []
+    for i, (x, y) in enumerate([(1024, 512), (512, 768), (2048, 256)]):
+        reqs.append((golb200.load_sparse_patches(x, y, 70 + i, 64, 0.05, 0.35), 600 + 131 * i))
+    g = np.zeros((128, 256), np.uint8)
+    g[60, 100:103] = 1
+    reqs.append((g, 257))
+    reqs.append((np.zeros((96, 640), np.uint8), 900))
+    g = np.zeros((64, 128), np.uint8)
+    g[10:12, 20:22] = 1
+    reqs.append((g, 1000))
+    reqs.append((oracle.random_ones_zeros(320, 200, 17), 450))
+    return reqs
+
+
+@pytest.mark.parametrize("tracking,policy", [("on", "fifo"), ("on", "srpt"), ("off", "srpt"),
+                                             ("auto", "fifo")])
+def test_tracking_and_policies_same_alone_and_in_the_mix(tracking, policy):
+    reqs = settling_requests()
+    mixed = {}
+    with golb200.GolServer(arena_bytes=256 << 20, quantum=64) as s:
+        s.set_tracking(tracking)
+        s.set_policy(policy)
+        ids = {}
+        for i, (c, n) in enumerate(reqs):
+            ids[s.submit(c, n)] = i
+            if i % 3 == 2:
+                s.step()
+        while len(mixed) < len(ids):
+            s.step()
+            for rid in s.finished():
+                mixed[ids[rid]] = s.fetch(rid)
+        t = s.tiles()
+    for i, (c, n) in enumerate(reqs):
+        want = oracle.life_cells(c, n)
+        assert np.array_equal(mixed[i], want), (i, tracking, policy)
+        with golb200.GolServer(arena_bytes=64 << 20, quantum=64) as a:
+            a.set_tracking(tracking)
+            a.set_policy(policy)
+            rid = a.submit(c, n)
+            while True:
+                a.step()
+                if rid in a.finished():
+                    assert np.array_equal(a.fetch(rid), want), (i, "alone", tracking, policy)
+                    break
+    if tracking == "on":
+        # the dead grid and the block are still after their first pass and
+        # finish early; tiles of the settled patches are skipped
+        assert t["early_finished"] >= 2
+        assert t["skipped"] > 0
+    if tracking == "off":
+        assert t["skipped"] == 0 and t["early_finished"] == 0
+
+
+def test_still_request_finishes_before_its_generations():
+    """A still life asked for 10^6 generations finishes after its first
+    round: the first pass changes nothing, so nothing later can."""
+    g = np.zeros((64, 256), np.uint8)
+    g[10:12, 20:22] = 1                      # block
+    g[40:43, 50:53] = np.array([[0, 1, 0], [1, 0, 1], [0, 1, 0]], np.uint8)   # tub
+    with golb200.GolServer(arena_bytes=64 << 20, quantum=64) as s:
+        s.set_tracking("on")
+        rid = s.submit(g, 10**6)
+        rounds = 0
+        while True:
+            s.step()
+            rounds += 1
+            if rid in s.finished():
+                break
+            assert rounds < 200
+        assert np.array_equal(s.fetch(rid), g)
+        assert s.tiles()["early_finished"] == 1
