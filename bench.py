@@ -75,7 +75,8 @@ def parse_args():
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the sparse, batched and serving measurements")
-    ap.add_argument("--only", choices=["sparse", "published", "batched", "serving", "hbm"],
+    ap.add_argument("--only", choices=["sparse", "published", "batched", "batched_settling",
+                                       "serving", "hbm"],
                     help="measure just that configuration and print it")
     return ap.parse_args()
 
@@ -565,8 +566,14 @@ def bench_batched(stream, device, n: int = 512, seed: int = SEED) -> dict:
     b.upload()
     info = b.info()
     b.run()
+    b.sync()                                        # first run: the census the autotuner reads
+    first_tiles = b.tiles()
+    b.retune()                                      # per-grid tracking / tile choice
+    b.run()
     b.sync()                                        # warm-up (and graph capture)
     batched = [_events_ms(stream, b.run, b.sync) for _ in range(3)]
+    tiles = b.tiles()
+    tracked = sum(1 for i in range(n) if b.grid_stats(i)["tracked"])
     results = [oracle.pack_rows(b.fetch(i), 64) for i in range(n)]
     b.run_plain(4)
     b.sync()
@@ -591,6 +598,8 @@ def bench_batched(stream, device, n: int = 512, seed: int = SEED) -> dict:
                         f"generations log-uniform [64, 4096], seed {seed}",
             "cell_updates": cu, "work_items": info["items"], "unit": UNIT,
             "value_batched": vb, "ms_batched": min(batched),
+            "autotuner": {"first_run_items": first_tiles, "grids_tracked_after_retune": tracked,
+                          "timed_run_items": tiles},
             "value_plain_per_grid": vp, "ms_plain": min(plain), "speedup": vb / vp,
             "value_plain_graphs_multistream": vg, "ms_plain_graphs_multistream": ms_graphs,
             "speedup_vs_graphs_multistream": vb / vg,
@@ -601,16 +610,112 @@ def bench_batched(stream, device, n: int = 512, seed: int = SEED) -> dict:
             "batched_all_equal_oracle": all(ok), "grids_checked_vs_oracle": len(ok)}
 
 
+def _check_serving_samples(samples) -> dict:
+    """Every sampled request's result against the oracle (its input remade
+    on the host with the same hash as the device generator)."""
+    import concurrent.futures as cf
+
+    import golb200
+    import oracle
+
+    def one(item):
+        d, out = item
+        cells = golb200.load_hash_bernoulli(d["x"], d["y"], d["cell_seed"], d["density"])
+        want = oracle.life_rows(oracle.pack_rows(cells, 32), d["x"], d["gens"], 32,
+                                threads=1 if d["x"] * d["y"] < (1 << 21) else 8)
+        got = out if out.dtype == np.uint32 else oracle.pack_rows(out, 32)
+        return bool(np.array_equal(got.view(np.uint32), want))
+    with cf.ThreadPoolExecutor(max_workers=max(1, (os.cpu_count() or 2) // 2)) as pool:
+        ok = list(pool.map(one, samples))
+    return {"sampled": len(ok), "all_equal_oracle": all(ok)}
+
+
+def bench_batched_settling(stream, device, n: int = 512, seed: int = SEED) -> dict:
+    """The batched workload's grids (same sizes and generation counts) with
+    settling inputs: dead grids with patches of Bernoulli(0.35) soup in 5 %
+    of their 64 x 64 slots (at least one). Batched with change tracking
+    (autotuned: a first run, gol_batch_retune, then timed runs) against the
+    same batch with tracking off; every grid checked against the oracle."""
+    import concurrent.futures as cf
+
+    import golb200
+    import oracle
+    work = golb200.workload_uneven(seed, n, 256, 4096, 64, (0.2, 0.5), (64, 4096))
+
+    def cells_of(d):
+        slots = (d["x"] // 64) * (d["y"] // 64)
+        return golb200.load_sparse_patches(d["x"], d["y"], d["cell_seed"], 64,
+                                           max(0.05, 1.0 / slots + 1e-9), 0.35)
+    with cf.ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as pool:
+        inputs = list(pool.map(lambda d: oracle.pack_rows(cells_of(d), 64), work))
+    out = {"workload": f"{n} grids as the batched workload (seed {seed}), dead with Bernoulli(0.35) "
+                       "patches in 5 % of 64x64 slots (at least one)", "unit": UNIT}
+    results = {}
+    for mode in ("on", "off"):
+        b = golb200.GolBatch(device=device, stream=stream.cuda_stream)
+        for d, w in zip(work, inputs):
+            gid = b.add(oracle.unpack_rows(w, d["x"], 64), d["gens"])
+            if mode == "off":
+                b.set_tracking(gid, "off")
+        b.upload()
+        info = b.info()
+        b.run()
+        b.sync()
+        if mode == "on":
+            b.retune()
+            b.run()
+            b.sync()
+        ms = min(_events_ms(stream, b.run, b.sync) for _ in range(3))
+        out[f"value_tracking_{mode}"] = info["cell_updates"] / (ms * 1e-3) / 1e9
+        out[f"ms_tracking_{mode}"] = ms
+        out[f"items_tracking_{mode}"] = b.tiles()
+        if mode == "on":
+            out["grids_still_before_their_end"] = sum(
+                1 for i in range(n) if b.grid_stats(i)["still_pass"] is not None)
+        results[mode] = [oracle.pack_rows(b.fetch(i), 64) for i in range(n)]
+        b.close()
+    out["speedup_tracking"] = out["value_tracking_on"] / out["value_tracking_off"]
+    out["cell_updates"] = info["cell_updates"]
+
+    def check(i):
+        d = work[i]
+        want = oracle.life_rows(inputs[i], d["x"], d["gens"], 64,
+                                threads=1 if inputs[i].size < (1 << 16) else 4)
+        return bool(np.array_equal(results["on"][i], want) and np.array_equal(results["off"][i], want))
+    with cf.ThreadPoolExecutor(max_workers=max(1, (os.cpu_count() or 2) // 2)) as pool:
+        ok = list(pool.map(check, range(n)))
+    out["all_equal_oracle"] = all(ok)
+    return out
+
+
 def bench_serving(device) -> dict:
     """Poisson stream, mean 2000 requests/s, sides log-uniform [128, 8192]
     (multiples of 64), density U[0.1, 0.5], generations log-uniform
-    [16, 8192], inputs generated on the device, results copied back."""
+    [16, 8192]. Four runs of the same 2-s stream: arrival-order (FIFO) and
+    least-work-first (SRPT) scheduling with inputs generated on the device and
+    packed results copied back, then both again with host I/O (host cells in
+    through gol_serve_submit, cells out through gol_serve_fetch). Change
+    tracking is on for long requests (auto). Every 64th request of the FIFO
+    runs is checked against the oracle."""
     import serve
-    r = serve.run_stream(rate=2000.0, seconds=2.0, seed=SEED, device=device)
-    r["workload"] = ("Poisson arrivals, mean 2000 req/s for 2 s, sides log-uniform [128, 8192] x64, "
-                     "density U[0.1, 0.5], generations log-uniform [16, 8192], seed 42")
-    r["unit_throughput"] = "cell-updates/s"
-    return r
+    out = {"workload": "Poisson arrivals, mean 2000 req/s for 2 s, sides log-uniform [128, 8192] "
+                       "x64, density U[0.1, 0.5], generations log-uniform [16, 8192], seed 42",
+           "unit_throughput": "cell-updates/s"}
+    for policy in ("fifo", "srpt"):
+        for host_io in (False, True):
+            r = serve.run_stream(rate=2000.0, seconds=2.0, seed=SEED, device=device, policy=policy,
+                                 host_io=host_io, check_every=64 if policy == "fifo" else 0)
+            samples = r.pop("samples")
+            if samples:
+                r["check"] = _check_serving_samples(samples)
+            r["p99_over_p50"] = r["latency_p99_ms"] / max(r["latency_p50_ms"], 1e-9)
+            out[f"{policy}{'_host_io' if host_io else ''}"] = r
+    # the headline figures: the FIFO run with device-side inputs
+    for k in ("requests", "cell_updates_per_s", "latency_p50_ms", "latency_p99_ms"):
+        out[k] = out["fifo"][k]
+    out["serving_sample_equal_oracle"] = all(out[k].get("check", {}).get("all_equal_oracle", True)
+                                             for k in ("fifo", "fifo_host_io"))
+    return out
 
 
 def run_extra(name: str) -> dict:
@@ -816,12 +921,13 @@ def run_ours(args, d: Dist) -> None:
     if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(cells)
 
-    sparse = published = batched = serving = hbm = None
+    sparse = published = batched = batched_settling = serving = hbm = None
     if d.rank == 0 and d.world == 1 and not args.no_extras:
         hbm = run_extra("hbm")
         sparse = run_extra("sparse")
         published = run_extra("published")
         batched = run_extra("batched")
+        batched_settling = run_extra("batched_settling")
         serving = run_extra("serving")
 
     if d.rank == 0:
@@ -847,6 +953,7 @@ def run_ours(args, d: Dist) -> None:
             "sparse_settling": sparse,
             "published_workloads": published,
             "batched_uneven": batched,
+            "batched_uneven_settling": batched_settling,
             "serving": serving,
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": grid_bytes, "d2h_bytes_per_step": grid_bytes,
@@ -875,7 +982,8 @@ def main():
               "published": lambda: bench_published(s, d.local_rank),
               "batched": lambda: bench_batched(s, d.local_rank),
               "serving": lambda: bench_serving(d.local_rank),
-              "hbm": lambda: bench_hbm(s, d.local_rank)}[args.only]
+              "hbm": lambda: bench_hbm(s, d.local_rank),
+              "batched_settling": lambda: bench_batched_settling(s, d.local_rank)}[args.only]
         print(json.dumps({args.only: fn()}), flush=True)
         return
     if d.world > 1:

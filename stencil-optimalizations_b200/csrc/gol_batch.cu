@@ -129,7 +129,7 @@ __device__ __forceinline__ uint32_t seg_group(const BatchGrid& G, int group, int
     const int f0 = 3 * K;
     const int f1 = min(G.band + 2 * K - 1, G.Y - y0_last + K - 1);
     const int fast_end = f1 > f0 ? f0 + (f1 - f0) / 3 * 3 : f0;
-    constexpr int TR = TRACK ? 1 : 0;
+    constexpr int TR = TRACK ? 3 : 0;   // old rows through the second ring
     if (fast_end > f0) {
         temporal_steps<WPL, K, false, false, TR, true, true>(s, c, 0, f0);
         temporal_steps<WPL, K, true, true, TR, true, true>(s, c, f0, fast_end);
@@ -179,11 +179,22 @@ __device__ __forceinline__ void release_max(int* p, int v) {
 // their dependencies or touching the grid, and both buffers hold the result.
 // census: [0] SM cycles waiting on dependencies, [1] working, [2] items
 // computed, [3] items skipped (tracked grids).
+// Resident one-warp CTAs per SM the registers are sized for. The tracked
+// variants of 1 and 2 words per lane are held near the untracked ones'
+// register counts (96 and 136), so tracking costs them little occupancy;
+// at 4 words per lane a cap spills heavily, so none is set.
 template <int WPL_ONLY, bool TRACK>
-__global__ void __launch_bounds__(32, GOL_BATCH_MIN_BLOCKS)
+constexpr int batch_min_blocks() {
+    return !TRACK ? GOL_BATCH_MIN_BLOCKS
+                  : (WPL_ONLY == 1 ? 19 : WPL_ONLY == 2 ? 15 : GOL_BATCH_MIN_BLOCKS);
+}
+
+template <int WPL_ONLY, bool TRACK>
+__global__ void __launch_bounds__(32, (batch_min_blocks<WPL_ONLY, TRACK>()))
 batch_kernel(const BatchGrid* __restrict__ grids, const BatchItem* __restrict__ items, int nitems,
              int* ticket, int* done, int* status, unsigned long long* census, long long spin_limit) {
-    __shared__ __align__(16) uint32_t ring[kRowRing * 32 * (WPL_ONLY ? WPL_ONLY : 4)];
+    // the row ring, and with TRACK the old-row ring right after it
+    __shared__ __align__(16) uint32_t ring[kRowRing * 32 * (WPL_ONLY ? WPL_ONLY : 4) * (TRACK ? 2 : 1)];
     constexpr int kEdgeWords = WPL_ONLY == 1 ? 1 : seg_edge_words(kBatchMaxK);   // 1: shuffles
     __shared__ uint32_t etab[kEdgeWords];
     const int lane = threadIdx.x & 31;

@@ -110,12 +110,11 @@ constexpr uint32_t kCensusCap = 1u << 20;   // passes recorded per run (4 MiB)
 
 int alloc_local(gol_engine* e) {
     golb200::LocalState& s = e->lst;
-    const size_t nt = (size_t)e->lplan.tiles_x * e->lplan.tiles_y;
     cudaError_t ce = cudaSuccess;
     if (!s.list) {
         for (auto& p : s.changed)
             if (ce == cudaSuccess) ce = cudaMalloc(&p, golb200::local_change_bytes(e->lplan));
-        if (ce == cudaSuccess) ce = cudaMalloc(&s.list, nt * sizeof(int));
+        if (ce == cudaSuccess) ce = cudaMalloc(&s.list, golb200::local_list_ints(e->lplan) * sizeof(int));
         if (ce == cudaSuccess) ce = cudaMalloc(&s.count, golb200::kLocalCountWords * sizeof(int));
         if (ce == cudaSuccess) ce = cudaMalloc(&s.census, kCensusCap * sizeof(uint32_t));
         if (ce == cudaSuccess) ce = cudaMalloc(&s.pass_no, sizeof(uint32_t));

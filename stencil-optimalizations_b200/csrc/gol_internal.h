@@ -41,9 +41,7 @@ cudaError_t launch_rows_pass(const uint32_t* src, uint32_t* dst, int W, int Y, i
 
 // Change-tracking tiles (GOL_ALG_LOCAL): tile = x-slice x row band.
 struct LocalPlan {
-    RowsPlan rows;     // slice/band geometry of one tile
-    int seg_lanes = 0; // lanes per tile (its words plus a halo lane each side)
-    int segs = 0;      // tiles carried by one warp at once
+    RowsPlan rows;     // slice/band geometry of one tile (one lane of words)
     int tiles_x = 0, tiles_y = 0;
     int ctas = 0;      // persistent CTAs of the tile kernel (capped at one wave)
     int num_sms = 0;
@@ -68,12 +66,19 @@ inline size_t local_change_bytes(const LocalPlan& lp) {
     return (size_t)lp.tiles_y * ((lp.tiles_x + 31) / 32) * sizeof(uint32_t);
 }
 
-constexpr int kLocalCountWords = 6;
+constexpr int kLocalCountWords = 8;
+
+// Entries of the lane list a pass's plan writes: one per active tile and
+// one halo lane at each end of every run of active tiles. At most 48 per 32
+// tiles of a tile row (16 runs of one tile).
+inline size_t local_list_ints(const LocalPlan& lp) {
+    return (size_t)lp.tiles_y * ((lp.tiles_x + 31) / 32) * 48 + 64;
+}
 
 struct LocalState {
     uint32_t* changed[2] = {nullptr, nullptr};  // change bits per tile, by pass parity
     int* list = nullptr;                        // active tiles of the current pass
-    int* count = nullptr;                       // kLocalCountWords plan words: list lengths
+    int* count = nullptr;                       // kLocalCountWords plan words: tile counts
                                                 // by pass parity, CTA ticket, dense choice
     uint32_t* census = nullptr;                 // active tiles per pass
     uint32_t census_cap = 0;

@@ -14,13 +14,17 @@
 // cells around each cell). Per pass:
 //   plan   one thread per 32 tiles of a tile row dilates the previous
 //          pass's change bits over the 3x3 neighbourhood, active tiles are
-//          appended to a list (warp scan + one atomic per warp), this pass's
+//          appended to a list as runs (warp scan + one atomic per warp), this pass's
 //          bits are cleared, and the last CTA appends the list length to a
 //          census;
-//   tiles  persistent one-warp CTAs walk the list, several tiles per warp
-//          (one per 3-lane segment: the segmented-warp form of the K-stage
-//          pipeline), compare each tile's result with its input and set the
-//          tile's change bit when any of its cells differs after the pass.
+//   tiles  persistent one-warp CTAs walk the list in windows of 32 lanes:
+//          a run of horizontally adjacent active tiles takes one lane per
+//          tile plus a halo lane at each end (neighbouring tiles share their
+//          halos: about 1 + 2/run lanes per tile instead of 3), each lane
+//          streams its tile's band through the K stages (the segmented-warp
+//          form of the pipeline), compares its result with its input and
+//          sets the tile's change bit when any of its cells differs after
+//          the pass.
 // No copies for skipped tiles: a tile skipped at pass p did not change at
 // pass p-1 (it is in its own neighbourhood), so the buffer pass p writes —
 // the one pass p-1 read — already holds its current state.
@@ -37,14 +41,6 @@
 
 #include "gol_internal.h"
 #include "gol_rows_temporal.cuh"
-
-#ifndef GOL_TILE_LANES
-// Change-tracking tile width in lanes: its words plus a halo lane each side.
-// On the sparse 16384^2 workload (k = 6, 6-row tiles, one change bit per
-// tile) 3, 4 and 5 lanes ran at 85, 81 and 71 T cell-updates/s: one word
-// (32 cells) per tile skips the most.
-#define GOL_TILE_LANES 3
-#endif
 
 #ifndef GOL_LOCAL_CARVEOUT
 // Shared-memory carveout (percent of the maximum) preferred by all three
@@ -74,25 +70,35 @@ constexpr int kPlanThreads = 256;
 // ty * change_words(tiles_x) + tx / 32.
 __host__ __device__ inline int change_words(int tiles_x) { return (tiles_x + 31) / 32; }
 
-// The plan's device words (PlanCounts): list lengths by pass parity, the
+// The plan's device words (PlanCounts): active tiles by pass parity, the
 // last CTA's ticket, whether the last planned pass had at least dense_min
-// active tiles, and whether each parity's pass runs dense.
-enum PlanCounts { kListLen0 = 0, kTicket = 2, kDenseHint = 3, kDense0 = 4 };
-static_assert(kDense0 + 2 <= kLocalCountWords, "plan words");
+// active tiles, whether each parity's pass runs dense, and the lane list's
+// length by pass parity.
+enum PlanCounts { kTiles0 = 0, kTicket = 2, kDenseHint = 3, kDense0 = 4, kLanes0 = 6 };
+static_assert(kLanes0 + 2 <= kLocalCountWords, "plan words");
+
+// The lane list: a pass's active tiles in runs of horizontally adjacent
+// tiles of one tile row, each run with a halo lane before and after it. An
+// entry is tile * 4 + role: the tile of a tile lane, or the first / last
+// tile of the run for its left / right halo lane.
+enum LaneRole { kRoleTile = 0, kRoleLeft = 1, kRoleRight = 2 };
 
 // One thread per flag word (32 tiles of a tile row). A tile is active if it
 // or one of its 8 neighbours changed in the previous pass: the OR of the
 // three flag rows around it, each shifted one bit left and right (with the
-// carry bits of the neighbouring words). Active tiles are appended to
-// `list` in order a warp at a time (scan of the per-thread counts, one
-// atomic per warp, so a warp of the tile kernel gets neighbouring tiles).
-// counts[parity] is this pass's list length (zero on entry); counts[parity
-// ^ 1] is zeroed for the next pass; the last CTA decides the pass's form
-// and records the census (tiles computed: all of them in a dense pass).
-// A pass runs dense when it has at least dense_min active tiles, or when
-// the previous one had: then the list is not written at all (the count
-// still is), at the price of one dense pass too many when activity drops.
-// This pass's flags are cleared on the way.
+// carry bits of the neighbouring words). The active tiles are appended to
+// the lane list in order, a warp at a time (a scan of the per-thread lane
+// counts, one atomic per warp): each run of adjacent active tiles as its
+// tiles with a halo lane before and after, so that neighbouring tiles share
+// halo lanes. A run continues across flag words of one tile row within a
+// warp; at a warp's edge it is cut in two (each part with its halos).
+// counts[kTiles0 + parity] / [kLanes0 + parity] are this pass's tile and
+// lane counts (zero on entry); the other parity's are zeroed for the next
+// pass; the last CTA decides the pass's form and records the census (tiles
+// computed: all of them in a dense pass). A pass runs dense when it has at
+// least dense_min active tiles, or when the previous one had: then the list
+// is not written at all (the counts still are), at the price of one dense
+// pass too many when activity drops. This pass's flags are cleared on the way.
 __global__ void __launch_bounds__(kPlanThreads)
 plan_tiles_kernel(const uint32_t* __restrict__ prev, uint32_t* __restrict__ clear, int tiles_x,
                   int tiles_y, int* __restrict__ list, int* counts, int parity,
@@ -103,7 +109,10 @@ plan_tiles_kernel(const uint32_t* __restrict__ prev, uint32_t* __restrict__ clea
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     const bool skip_list = counts[kDenseHint] != 0;
-    if (blockIdx.x == 0 && threadIdx.x == 0) counts[parity ^ 1] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        counts[kTiles0 + (parity ^ 1)] = 0;
+        counts[kLanes0 + (parity ^ 1)] = 0;
+    }
     uint32_t act = 0u;
     int ty = 0, w = 0;
     if (t < nw) {
@@ -122,8 +131,19 @@ plan_tiles_kernel(const uint32_t* __restrict__ prev, uint32_t* __restrict__ clea
         if (valid < 32) act &= (1u << valid) - 1u;
         clear[t] = 0u;
     }
+    // Runs: a run continues from the previous word (same tile row, same
+    // warp) when that word's last tile and this word's first are active.
+    const uint32_t prev_act = __shfl_up_sync(0xffffffffu, act, 1);
+    const uint32_t next_act = __shfl_down_sync(0xffffffffu, act, 1);
+    const bool cin = lane > 0 && w > 0 && (prev_act >> 31);
+    const bool cout = lane < 31 && w + 1 < wx && (next_act & 1u);
+    const uint32_t starts = act & ~((act << 1) | (cin ? 1u : 0u));
+    const uint32_t ends = act & ~((act >> 1) | (cout ? 0x80000000u : 0u));
     const int n = __popc(act);
-    int incl = n;
+    const int nl = n + __popc(starts) + __popc(ends);
+    // scan of (lanes << 16 | tiles): both at most 48 * 32 per warp
+    const int packed = (nl << 16) | n;
+    int incl = packed;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const int v = __shfl_up_sync(0xffffffffu, incl, o);
@@ -131,17 +151,20 @@ plan_tiles_kernel(const uint32_t* __restrict__ prev, uint32_t* __restrict__ clea
     }
     const int wtotal = __shfl_sync(0xffffffffu, incl, 31);
     int base = 0;
-    if (lane == 31 && wtotal) base = atomicAdd(counts + parity, wtotal);
-    base = __shfl_sync(0xffffffffu, base, 31) + incl - n;
-    // Each lane writes its own tiles, all lanes at once. (A warp writing the
-    // lanes' runs one after another, coalesced, cost the plan kernel 1.2 us
-    // more per pass on the sparse 16384^2 workload; big lists, where it would
-    // pay, come only after dense-level passes, which skip the list.)
+    if (lane == 31 && wtotal) {
+        atomicAdd(counts + kTiles0 + parity, wtotal & 0xffff);
+        base = atomicAdd(counts + kLanes0 + parity, wtotal >> 16);
+    }
+    base = __shfl_sync(0xffffffffu, base, 31) + ((incl - packed) >> 16);
+    // Each lane writes its own runs, all lanes at once.
     if (!skip_list) {
         while (act) {
             const int b = __ffs((int)act) - 1;
             act &= act - 1u;
-            list[base++] = ty * tiles_x + 32 * w + b;
+            const int tile = ty * tiles_x + 32 * w + b;
+            if ((starts >> b) & 1u) list[base++] = tile * 4 + kRoleLeft;
+            list[base++] = tile * 4 + kRoleTile;
+            if ((ends >> b) & 1u) list[base++] = tile * 4 + kRoleRight;
         }
     }
 
@@ -151,7 +174,7 @@ plan_tiles_kernel(const uint32_t* __restrict__ prev, uint32_t* __restrict__ clea
         unsigned* ticket = reinterpret_cast<unsigned*>(counts + kTicket);
         if (atomicAdd(ticket, 1u) == gridDim.x - 1) {   // every CTA has appended
             __threadfence();
-            const int total = atomicAdd(counts + parity, 0);
+            const int total = atomicAdd(counts + kTiles0 + parity, 0);
             const bool dense = skip_list || total >= dense_min;
             counts[kDense0 + parity] = dense ? 1 : 0;
             counts[kDenseHint] = total >= dense_min ? 1 : 0;
@@ -166,8 +189,8 @@ plan_tiles_kernel(const uint32_t* __restrict__ prev, uint32_t* __restrict__ clea
 }
 
 struct TileList {
-    const int* list;        // active tile indices (band * tiles_x + slice)
-    const int* count;       // number of entries in `list`
+    const int* list;        // the lane list (entries tile * 4 + role)
+    const int* lanes;       // number of entries in `list`
     uint32_t* changed;      // change bits of this pass (cleared by the plan kernel)
     int tiles_x;
     const int* dense;       // nonzero: this pass runs dense (the tile kernel returns)
@@ -180,10 +203,17 @@ struct TileList {
 #define GOL_TILE_WARPS 1
 #endif
 constexpr int kTileWarps = GOL_TILE_WARPS;
+constexpr int kWindowOwn = 30;   // lanes of the lane list a warp stores per window
 
-// One warp, up to `segs` tiles at once (segment s takes list entry
-// base + s). Each segment streams its tile's band through the K stages with
-// change tracking; a ballot over the segment's lanes gives changed[tile].
+// One warp per window of 32 consecutive entries of the lane list: it owns
+// the middle 30 (window w owns entries [30w, 30w + 30)) and computes the two
+// outer ones only as context, so a run cut by a window edge still has a
+// correct neighbour word beyond each owned lane (an error entering at the
+// window's edge moves one cell per generation and stays in the outer lane
+// for K <= 32). Each lane streams its own tile's band through the K stages
+// (the segmented-warp pipeline, segments = runs: a run's halo lanes and the
+// window's edges see dead cells beyond them), compares every stored word
+// with its input, and a lane whose tile changed sets the tile's change bit.
 // When the dense form is enabled this kernel is launched after it, as a
 // programmatic dependent: the two never touch the same data in one pass
 // (one of them returns at once), so a tile pass starts without waiting,
@@ -191,12 +221,12 @@ constexpr int kTileWarps = GOL_TILE_WARPS;
 // work in the stream waits for this kernel only.
 template <int WPL, int K>
 __global__ void __launch_bounds__(32 * kTileWarps)
-seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
+seg_tiles_kernel(RowsLaunch a, TileList t) {
     __shared__ __align__(16) uint32_t rings[kTileWarps][kRowRing * 32 * WPL];
     constexpr int kEdgeWords = WPL == 1 ? 1 : seg_edge_words(K);   // one word per lane: shuffles
     __shared__ uint32_t etabs[kTileWarps][kEdgeWords];
     const int dense = *t.dense;
-    const int n = *t.count;   // both loads in flight together
+    const int nl = *t.lanes;   // both loads in flight together
     if (dense) {   // a dense pass
         asm volatile("griddepcontrol.wait;" ::: "memory");
         return;
@@ -207,16 +237,16 @@ seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
     uint32_t* etab = etabs[warp];
     const int gwarp = blockIdx.x * kTileWarps + warp;
     const int nwarps = gridDim.x * kTileWarps;
-    const int L = seg_lanes;
-    const int seg = lane / L, q = lane - seg * L;
-    for (int t = lane; t < kEdgeWords; t += 32) etab[t] = 0u;
+    for (int u = lane; u < kEdgeWords; u += 32) etab[u] = 0u;
     __syncwarp();
-    for (int first = gwarp * segs; first < n; first += nwarps * segs) {
-        const int idx = first + seg;
-        const bool has = seg < segs && idx < n;
-        const int tile = has ? t.list[idx] : 0;
+    for (int win = gwarp; win * kWindowOwn < nl; win += nwarps) {
+        const int g = win * kWindowOwn - 1 + lane;
+        const int d = (g >= 0 && g < nl) ? t.list[g] : -1;
+        const bool valid = d >= 0;
+        const int role = valid ? (d & 3) : kRoleTile;
+        const int tile = valid ? (d >> 2) : 0;
         const int ty = tile / t.tiles_x, tx = tile - ty * t.tiles_x;
-        const int xs = tx * a.slice;
+        const int col = tx + (role == kRoleLeft ? -1 : role == kRoleRight ? 1 : 0);
         TemporalCtx c;
         c.src = a.src;
         c.dst = a.dst;
@@ -227,16 +257,16 @@ seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
         c.y0 = ty * a.band;
         c.y1 = min(c.y0 + a.band, a.Y);
         c.lane = lane;
-        c.base = xs - a.halo + q * WPL;
-        c.lane_ok = has && c.y0 < a.Y && c.base >= 0 && c.base < a.W;
-        c.own = c.lane_ok && c.base >= xs && c.base < xs + a.slice;
+        c.base = col * WPL;
+        c.lane_ok = valid && c.y0 < a.Y && c.base >= 0 && c.base < a.W;
+        c.own = c.lane_ok && role == kRoleTile && lane >= 1 && lane <= kWindowOwn;
+        c.seg_first = !valid || role == kRoleLeft || lane == 0;
+        c.seg_last = !valid || role == kRoleRight || lane == 31;
         c.eb = etab + lane;
-        c.el = q == 0 ? etab : etab + lane;                      // segment ends: zero entries
-        c.er = q == L - 1 ? etab + kSegEdgeStride - 1 : etab + lane + 2;
+        c.el = c.seg_first ? etab : etab + lane;                      // run ends: zero entries
+        c.er = c.seg_last ? etab + kSegEdgeStride - 1 : etab + lane + 2;
         c.src_l = max(lane - 1, 0);
         c.src_r = min(lane + 1, 31);
-        c.seg_first = q == 0;
-        c.seg_last = q == L - 1;
         c.ring = ring + lane * WPL;
         c.ring_saddr = (uint32_t)__cvta_generic_to_shared(c.ring);
         c.ring_stride = ring_slot_words<WPL, true>();
@@ -247,10 +277,10 @@ seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
         for (int w = 0; w < WPL; ++w) {
             s.ld[0][w] = s.ld[1][w] = s.ld[2][w] = 0u;
 #pragma unroll
-            for (int g = 0; g < K; ++g) {
-                s.h0[g][0][w] = s.h0[g][1][w] = s.h0[g][2][w] = 0u;
-                s.h1[g][0][w] = s.h1[g][1][w] = s.h1[g][2][w] = 0u;
-                s.o[g][0][w] = s.o[g][1][w] = s.o[g][2][w] = 0u;
+            for (int gg = 0; gg < K; ++gg) {
+                s.h0[gg][0][w] = s.h0[gg][1][w] = s.h0[gg][2][w] = 0u;
+                s.h1[gg][0][w] = s.h1[gg][1][w] = s.h1[gg][2][w] = 0u;
+                s.o[gg][0][w] = s.o[gg][1][w] = s.o[gg][2][w] = 0u;
             }
         }
         for (int j = 0; j < kRowsInFlight; ++j) issue_row<WPL, K, 1, true>(c, j, j);
@@ -258,8 +288,8 @@ seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
         lds_words<WPL>(c.ring, s.ld[0]);
         s.diff = 0u;
 
-        // Steady state while every segment's rows stay inside the grid: the
-        // deepest band among the warp's tiles bounds the window.
+        // Steady state while every lane's rows stay inside the grid: the
+        // deepest band among the window's tiles bounds the window.
         const int y0_deep = __reduce_max_sync(0xffffffffu, c.lane_ok ? c.y0 : 0);
         const int nsteps = c.B + 3 * K;
         const int f0 = 3 * K;
@@ -273,12 +303,9 @@ seg_tiles_kernel(RowsLaunch a, TileList t, int seg_lanes, int segs) {
             temporal_steps<WPL, K, false, false, true, true>(s, c, 0, nsteps);
         }
         asm volatile("cp.async.wait_all;\n" ::: "memory");
-        const unsigned any = __ballot_sync(0xffffffffu, s.diff != 0u);
-        if (has && q == 0) {
-            const unsigned segmask = (L == 32 ? 0xffffffffu : ((1u << L) - 1u)) << (seg * L);
-            if (any & segmask)
-                atomicOr(t.changed + ty * change_words(t.tiles_x) + tx / 32, 1u << (tx % 32));
-        }
+        if (c.own && s.diff != 0u)
+            atomicOr(t.changed + ty * change_words(t.tiles_x) + tx / 32, 1u << (tx % 32));
+        __syncwarp();
     }
     asm volatile("griddepcontrol.wait;" ::: "memory");
 }
@@ -365,7 +392,7 @@ cudaError_t launch_tiles_one(const RowsLaunch& a, const TileList& t, const Local
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = lp.dense_min == INT_MAX ? 0 : 1;
-    return cudaLaunchKernelEx(&cfg, seg_tiles_kernel<WPL, K>, a, t, lp.seg_lanes, lp.segs);
+    return cudaLaunchKernelEx(&cfg, seg_tiles_kernel<WPL, K>, a, t);
 }
 
 template <int WPL, int K>
@@ -397,22 +424,17 @@ bool plan_local_tiles(int W, int Y, int k, int tile_rows, int wpl, int num_sms, 
     p.band = band;
     p.nbands = (Y + band - 1) / band;
     p.threads = 32;
-    constexpr int kTileLanes = GOL_TILE_LANES;           // lanes of words + a halo lane each side
-    if (W / wpl <= kTileLanes) {
-        p.slice = W;
-        p.halo = 0;
-        lp->seg_lanes = W / wpl;
-    } else {
-        p.slice = (kTileLanes - 2) * wpl;
-        p.halo = wpl;
-        lp->seg_lanes = kTileLanes;
-    }
-    lp->segs = 32 / lp->seg_lanes;
-    p.nslices = (W + p.slice - 1) / p.slice;
+    // A tile is one lane of words (32 cells at one word per lane); the lane
+    // list gives each run of active tiles a halo lane on either side.
+    p.slice = wpl;
+    p.halo = wpl;
+    p.nslices = W / wpl;
     lp->tiles_x = p.nslices;
     lp->tiles_y = p.nbands;
-    const int warps = (lp->tiles_x * lp->tiles_y + lp->segs - 1) / lp->segs;
-    lp->ctas = std::max(1, (std::min(warps, num_sms * 24) + kTileWarps - 1) / kTileWarps);
+    if ((long long)lp->tiles_x * lp->tiles_y >= (1LL << 29)) return false;   // entries: tile * 4
+    const long long lanes = (long long)lp->tiles_x * lp->tiles_y * 3 / 2;
+    const long long windows = (lanes + kWindowOwn - 1) / kWindowOwn;
+    lp->ctas = (int)std::max(1LL, (std::min<long long>(windows, num_sms * 24LL) + kTileWarps - 1) / kTileWarps);
     lp->num_sms = num_sms;
     // The dense form: the row-band plan at the kernel's lane width. Its
     // lanes start at multiples of that width and tiles are 1, 2 or 4 words
@@ -446,7 +468,8 @@ cudaError_t launch_local_pass(const uint32_t* src, uint32_t* dst, int W, int Y, 
         if (e != cudaSuccess) return e;
     }
     RowsLaunch a{src, dst, W, Y, p.band, p.slice, p.halo, W};
-    TileList t{st.list, st.count + parity, st.changed[parity], lp.tiles_x, st.count + kDense0 + parity};
+    TileList t{st.list, st.count + kLanes0 + parity, st.changed[parity], lp.tiles_x,
+               st.count + kDense0 + parity};
     switch (p.wpl) {
         case 4: return dispatch_tiles<4, 1>(k, a, t, lp, stream);
         case 2: return dispatch_tiles<2, 1>(k, a, t, lp, stream);

@@ -55,6 +55,71 @@ __device__ __forceinline__ void stream_load(const uint32_t* p, bool v, uint32_t 
 // indices share rows (and their halo rows meet in L2). a.halo is unused (the
 // row is never cut with halo lanes: lanes at a CTA boundary read their outer
 // words from memory).
+// One step of the stream: read-row i (grid row y0 - 1 + i) is in ring slot
+// J = i mod P. Its horizontal sums go to ring-of-3 slot i mod 3; then output
+// row i - 2 is formed from the sums of read-rows i-2, i-1, i and the centre
+// words of read-row i-1, still in slot (J - 1) mod P, which is then free and
+// takes read-row i - 1 + P (so P - 1 rows are in flight ahead). FAST: that
+// row exists and lies inside the grid (no bounds tests).
+template <int WPL, int P, int J, bool FAST>
+__device__ __forceinline__ void stream_step(const RowsLaunch& a, int i, int n, int y0, int base,
+                                            bool ok, bool load_l, bool load_r, int lane,
+                                            const uint32_t*& next, uint32_t (&v)[P][WPL],
+                                            uint32_t (&vl)[P], uint32_t (&vr)[P],
+                                            uint32_t (&h0)[3][WPL], uint32_t (&h1)[3][WPL]) {
+    constexpr int R = J % 3;                 // i mod 3 (i - J is a multiple of P, P of 3)
+    constexpr int JP = (J + P - 1) % P;      // slot of read-row i - 1
+    uint32_t lw = __shfl_up_sync(0xffffffffu, v[J][WPL - 1], 1);
+    uint32_t rw = __shfl_down_sync(0xffffffffu, v[J][0], 1);
+    if (lane == 0) lw = vl[J];
+    if (lane == 31) rw = vr[J];
+#pragma unroll
+    for (int w = 0; w < WPL; ++w) {
+        const uint32_t l = w == 0 ? lw : v[J][w - 1];
+        const uint32_t r = w == WPL - 1 ? rw : v[J][w + 1];
+        hsum(l, v[J][w], r, h0[R][w], h1[R][w]);
+    }
+    if (FAST || i >= 2) {                    // output row y0 + i - 2
+        constexpr int RM = (R + 1) % 3;      // (i - 2) mod 3
+        constexpr int RC = (R + 2) % 3;      // (i - 1) mod 3
+        uint32_t res[WPL];
+#pragma unroll
+        for (int w = 0; w < WPL; ++w)
+            res[w] = next_word(h0[RM][w], h1[RM][w], h0[RC][w], h1[RC][w], h0[R][w], h1[R][w],
+                               v[JP][w]);
+        if (ok) store_words<WPL>(a.dst + (size_t)(y0 + i - 2) * a.pitch + base, res);
+    }
+    // slot JP takes read-row i - 1 + P
+    if (FAST) {
+        if (ok) load_words<WPL>(next, v[JP]);
+        vl[JP] = load_l ? __ldg(next - 1) : 0u;
+        vr[JP] = load_r ? __ldg(next + WPL) : 0u;
+    } else {
+        const int ir = i - 1 + P;
+        const int y = y0 - 1 + ir;
+        const bool rv = ir < n && (unsigned)y < (unsigned)a.Y;
+        stream_load<WPL>(next, ok && rv, v[JP]);
+        vl[JP] = (load_l && rv) ? __ldg(next - 1) : 0u;
+        vr[JP] = (load_r && rv) ? __ldg(next + WPL) : 0u;
+    }
+    next += a.pitch;
+}
+
+template <int WPL, int P, bool FAST, int J = 0>
+__device__ __forceinline__ void stream_chunk(const RowsLaunch& a, int i0, int n, int y0, int base,
+                                             bool ok, bool load_l, bool load_r, int lane,
+                                             const uint32_t*& next, uint32_t (&v)[P][WPL],
+                                             uint32_t (&vl)[P], uint32_t (&vr)[P],
+                                             uint32_t (&h0)[3][WPL], uint32_t (&h1)[3][WPL]) {
+    if constexpr (J < P) {
+        if (!FAST && i0 + J >= n) return;   // n is uniform across the CTA
+        stream_step<WPL, P, J, FAST>(a, i0 + J, n, y0, base, ok, load_l, load_r, lane, next, v,
+                                     vl, vr, h0, h1);
+        stream_chunk<WPL, P, FAST, J + 1>(a, i0, n, y0, base, ok, load_l, load_r, lane, next, v,
+                                          vl, vr, h0, h1);
+    }
+}
+
 template <int WPL>
 __global__ void __launch_bounds__(kStreamMaxThreads)
 rows_stream_kernel(RowsLaunch a) {
@@ -71,62 +136,40 @@ rows_stream_kernel(RowsLaunch a) {
     const bool load_r = ok && lane == 31 && base + WPL < a.W;
     const int y0 = band * a.band;
     const int y1 = min(y0 + a.band, a.Y);
-    const int n = y1 - y0 + 2;    // rows y0 - 1 .. y1 are read
+    const int n = y1 - y0 + 2;    // read-rows 0 .. n-1: grid rows y0 - 1 .. y1
     const uint32_t* col = a.src + base;
 
     uint32_t v[P][WPL], vl[P], vr[P];   // rows in flight: words, outer left / right word
-
-    // Issues the load of read-row i (grid row y0 - 1 + i) into ring slot s.
-    auto issue = [&](int s, int i) {
-        const int y = y0 - 1 + i;
-        const bool rv = i < n && (unsigned)y < (unsigned)a.Y;
+    uint32_t h0[3][WPL], h1[3][WPL];    // horizontal sums by read-row mod 3
+#pragma unroll
+    for (int s = 0; s < P; ++s) {       // read-rows 0 .. P-2 into slots 0 .. P-2
+        const int y = y0 - 1 + s;
+        const bool rv = s < P - 1 && s < n && (unsigned)y < (unsigned)a.Y;
         const uint32_t* p = col + (size_t)(rv ? y : 0) * a.pitch;
         stream_load<WPL>(p, ok && rv, v[s]);
         vl[s] = (load_l && rv) ? __ldg(p - 1) : 0u;
         vr[s] = (load_r && rv) ? __ldg(p + WPL) : 0u;
-    };
-#pragma unroll
-    for (int s = 0; s < P; ++s) issue(s, s);
-
-    uint32_t h0[3][WPL], h1[3][WPL], c[3][WPL];   // by read-row mod 3
+    }
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
-        for (int w = 0; w < WPL; ++w) h0[r][w] = h1[r][w] = c[r][w] = 0u;
-
-    for (int i0 = 0; i0 < n; i0 += P) {   // n is uniform across the CTA
-#pragma unroll
-        for (int j = 0; j < P; ++j) {
-            const int i = i0 + j;
-            if (i >= n) break;
-            const int r = j % 3;   // == i % 3 (i0 is a multiple of P, P of 3)
-            // Neighbour words: the lane to the left's last word and the lane
-            // to the right's first word (zero past the grid), or from memory
-            // at the warp's ends.
-            uint32_t lw = __shfl_up_sync(0xffffffffu, v[j][WPL - 1], 1);
-            uint32_t rw = __shfl_down_sync(0xffffffffu, v[j][0], 1);
-            if (lane == 0) lw = vl[j];
-            if (lane == 31) rw = vr[j];
-#pragma unroll
-            for (int w = 0; w < WPL; ++w) {
-                const uint32_t l = w == 0 ? lw : v[j][w - 1];
-                const uint32_t rr = w == WPL - 1 ? rw : v[j][w + 1];
-                hsum(l, v[j][w], rr, h0[r][w], h1[r][w]);
-                c[r][w] = v[j][w];
-            }
-            issue(j, i + P);   // slot j is free again
-            if (i >= 2) {      // output row y0 + i - 2 from read-rows i-2, i-1, i
-                const int rm = (j + 1) % 3;   // (i - 2) mod 3
-                const int rc = (j + 2) % 3;   // (i - 1) mod 3
-                uint32_t res[WPL];
-#pragma unroll
-                for (int w = 0; w < WPL; ++w)
-                    res[w] = next_word(h0[rm][w], h1[rm][w], h0[rc][w], h1[rc][w], h0[r][w],
-                                       h1[r][w], c[rc][w]);
-                if (ok) store_words<WPL>(a.dst + (size_t)(y0 + i - 2) * a.pitch + base, res);
-            }
-        }
+        for (int w = 0; w < WPL; ++w) h0[r][w] = h1[r][w] = 0u;
+    // the next row to issue: read-row P - 1 (a pointer that may point
+    // outside the grid; it is dereferenced only for rows inside it)
+    const uint32_t* next = col + (long long)(y0 - 2 + P) * a.pitch;
+    int i0 = 0;
+    // Chunks whose steps all issue rows inside the grid, output rows >= 2
+    // in: read-rows up to i0 + 2P - 2 <= n - 2, and i0 >= P.
+    if (n >= 2 * P + 2) {
+        stream_chunk<WPL, P, false>(a, 0, n, y0, base, ok, load_l, load_r, lane, next, v, vl, vr,
+                                    h0, h1);
+        for (i0 = P; i0 + 2 * P <= n; i0 += P)
+            stream_chunk<WPL, P, true>(a, i0, n, y0, base, ok, load_l, load_r, lane, next, v, vl,
+                                       vr, h0, h1);
     }
+    for (; i0 < n; i0 += P)
+        stream_chunk<WPL, P, false>(a, i0, n, y0, base, ok, load_l, load_r, lane, next, v, vl, vr,
+                                    h0, h1);
 }
 
 } // namespace golb200

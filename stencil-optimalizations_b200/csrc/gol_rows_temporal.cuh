@@ -215,7 +215,8 @@ __host__ __device__ constexpr int ring_slot_words() { return (SEG ? 32 : kTempor
 // the pass. CTA-wide tracked passes (TRACK 2) stage that row like stage 0's
 // rows, in a second ring right after the first (same slot numbering, this
 // byte offset): the copy for step j's output row (y0 - 3K + j) travels with
-// stage 0's row of step j. (Tile warps, TRACK 1, load it when storing:
+// stage 0's row of step j; so do segmented warps with TRACK 3. (Tile
+// warps, TRACK 1, load it when storing:
 // their many resident warps hide the latency, and their shared memory
 // stays small.)
 template <int WPL, bool SEG>
@@ -231,7 +232,7 @@ __device__ __forceinline__ void issue_row_at(const TemporalCtx& c, int j, uint32
     const bool v = c.lane_ok && (unsigned)r < (unsigned)c.Y;
     const uint32_t* g = v ? c.src + (size_t)r * c.pitch + c.base : c.src;
     cp_async_words<WPL>(saddr, g, v);
-    if (TRACK == 2) {
+    if (TRACK >= 2) {
         const int ro = r - 2 * K;
         const bool vo = c.lane_ok && (unsigned)ro < (unsigned)c.Y;
         const uint32_t* go = vo ? c.src + (size_t)ro * c.pitch + c.base : c.src;
@@ -308,7 +309,9 @@ __device__ __forceinline__ void flush_tile_row(TemporalRegs<WPL, K>& s, const Te
 // work, so those warps shuffle instead (no table, no barrier).
 // PART = rows padded to whole lanes: the last lane of a row may hold words
 // past W, masked word by word (otherwise a lane is all in or all out).
-// TRACK: 0 none; 1 = OR of (new ^ old) over every stored word (s.diff);
+// TRACK: 0 none; 1 = OR of (new ^ old) over every stored word (s.diff), the
+// old word loaded from global memory when storing; 3 = the same with the old
+// row staged through the old-row ring (fewer registers in flight);
 // 2 = per-tile change bits, closed at each tile row's last row (CTA-wide
 // kernels only: every lane of a CTA is on the same row at a step).
 template <int WPL, int K, int PH, bool FAST, bool LMASK, int TRACK, bool SEG = false,
@@ -372,13 +375,13 @@ __device__ __forceinline__ void temporal_step(TemporalRegs<WPL, K>& s, const Tem
                     store_words<WPL>(c.dst + (size_t)row * c.pitch + c.base, res);
                     if (TRACK) {   // compare with the same row before the pass
                         uint32_t old[WPL];
-                        if (TRACK == 2)   // old-row ring slot i mod 6
+                        if (TRACK >= 2)   // old-row ring slot i mod 6
                             lds_words_at<WPL>(s.bank_cur + PH * SB + old_ring_offset<WPL, SEG>(), old);
                         else
                             load_words<WPL>(c.src + (size_t)row * c.pitch + c.base, old);
 #pragma unroll
                         for (int w = 0; w < WPL; ++w) {
-                            if (TRACK == 1)
+                            if (TRACK != 2)
                                 s.diff |= res[w] ^ old[w];
                             else
                                 s.diff |= (res[w] != old[w] ? 1u : 0u) << w;

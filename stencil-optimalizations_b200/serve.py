@@ -7,10 +7,13 @@ Each request draws its size, density, generation count and input seed from
 gol_workload_uneven (sides log-uniform, multiples of 64; density uniform;
 generations log-uniform) and its arrival time from gol_poisson_arrivals.
 Requests are submitted when their arrival time has come (inputs generated on
-the device at admission), the server is stepped continuously, and a request
-completes when its last round has finished on the GPU. The loop reports
-p50/p99 completion latency (arrival to completion, host clock) and the
-aggregate cell-updates/s over the run.
+the device at admission, or with --host-io made on the host and copied in,
+results copied back and unpacked), the server is stepped continuously, and a
+request completes when its last round has finished on the GPU (or earlier,
+once change tracking finds it still). --policy picks arrival order or
+least-work-first scheduling, --tracking the change-tracking mode. The loop
+reports p50/p99 completion latency (arrival to completion, host clock) and
+the aggregate cell-updates/s over the run.
 """
 from __future__ import annotations
 
@@ -32,8 +35,20 @@ import golb200  # noqa: E402
 def run_stream(rate: float = 2000.0, seconds: float = 2.0, seed: int = 42, min_side: int = 128,
                max_side: int = 8192, density=(0.1, 0.5), gens=(16, 8192), quantum: int = 128,
                arena_bytes: int = 0, device: int = 0, fetch: str = "words",
-               max_requests: int | None = None, server: golb200.GolServer | None = None) -> dict:
-    """Serves the seeded Poisson stream that arrives within `seconds`."""
+               max_requests: int | None = None, server: golb200.GolServer | None = None,
+               policy: str = "fifo", tracking: str = "auto", host_io: bool = False,
+               check_every: int = 0) -> dict:
+    """Serves the seeded Poisson stream that arrives within `seconds`.
+
+    host_io: every request's cells are made on the host (the same cells
+    gol_serve_submit_random would make on the device, by a pool of threads
+    working ahead of the arrivals, as clients would hold them) and submitted
+    through gol_serve_submit (host pack, copy to the device at admission);
+    every result is fetched as cells (copy back, host unpack). Otherwise
+    inputs are generated on the device and results fetched as packed words.
+    check_every > 0 keeps the fetched result of every check_every-th request
+    (submission order) in r["samples"] as (request, result)."""
+    from concurrent.futures import ThreadPoolExecutor
     n = int(rate * seconds * 1.2) + 16
     if max_requests:
         n = min(n, max_requests)
@@ -42,43 +57,80 @@ def run_stream(rate: float = 2000.0, seconds: float = 2.0, seed: int = 42, min_s
     keep = [i for i in range(n) if arrivals[i] <= seconds] if not max_requests else list(range(n))
     own = server is None
     srv = server or golb200.GolServer(device=device, arena_bytes=arena_bytes, quantum=quantum)
-    pending: dict[int, tuple[float, int]] = {}
+    srv.set_policy(policy)
+    srv.set_tracking(tracking)
+    pool = ThreadPoolExecutor(max_workers=max(1, (os.cpu_count() or 2) // 2)) if host_io else None
+    ahead: dict[int, object] = {}
+
+    def make_cells(d):
+        return golb200.load_hash_bernoulli(d["x"], d["y"], d["cell_seed"], d["density"])
+
+    def prefetch(upto: int) -> None:
+        for j in range(upto, min(len(keep), upto + 64)):
+            if j not in ahead:
+                ahead[j] = pool.submit(make_cells, work[keep[j]])
+
+    pending: dict[int, tuple[float, int, int]] = {}
     latencies: list[float] = []
+    samples: list[tuple[dict, np.ndarray]] = []
     cell_updates = 0
     submitted = 0
+    late = 0
+    if pool:
+        prefetch(0)
+        for f in list(ahead.values()):
+            f.result()
     t0 = time.perf_counter()
     try:
         while submitted < len(keep) or pending:
             now = time.perf_counter() - t0
             while submitted < len(keep) and arrivals[keep[submitted]] <= now:
                 d = work[keep[submitted]]
-                rid = srv.submit_random(d["x"], d["y"], d["gens"], d["cell_seed"], d["density"])
-                pending[rid] = (float(arrivals[keep[submitted]]), d["x"] * d["y"] * d["gens"])
+                if pool:
+                    prefetch(submitted)
+                    f = ahead.pop(submitted)
+                    late += 0 if f.done() else 1
+                    rid = srv.submit(f.result(), d["gens"])
+                else:
+                    rid = srv.submit_random(d["x"], d["y"], d["gens"], d["cell_seed"], d["density"])
+                pending[rid] = (float(arrivals[keep[submitted]]), d["x"] * d["y"] * d["gens"],
+                                submitted)
                 submitted += 1
             srv.step()
             done = srv.finished()
             t_done = time.perf_counter() - t0
             for rid in done:
-                arr, cu = pending.pop(rid)
+                arr, cu, idx = pending.pop(rid)
                 latencies.append(t_done - arr)
                 cell_updates += cu
-                if fetch == "words":
-                    srv.fetch_words(rid)
-                elif fetch == "cells":
-                    srv.fetch(rid)
+                keep_it = check_every > 0 and idx % check_every == 0
+                if host_io or fetch == "cells":
+                    out = srv.fetch(rid)
+                elif fetch == "words" or keep_it:
+                    out = srv.fetch_words(rid)
                 else:
                     srv.release(rid)
+                    out = None
+                if keep_it:
+                    samples.append((work[keep[idx]], out))
             if not done and submitted < len(keep) and not pending:
                 wait = arrivals[keep[submitted]] - (time.perf_counter() - t0)
                 if wait > 0:
                     time.sleep(min(wait, 0.001))
         wall = time.perf_counter() - t0
         stats = srv.stats()
+        tiles = srv.tiles()
     finally:
+        if pool:
+            pool.shutdown(wait=False, cancel_futures=True)
         if own:
             srv.close()
     lat = np.array(latencies) if latencies else np.zeros(1)
     return {
+        "policy": policy, "tracking": tracking, "host_io": host_io,
+        "inputs_generated_late": late, "tiles_computed": tiles["computed"],
+        "tiles_skipped": tiles["skipped"], "finished_early_still": tiles["early_finished"],
+        "samples": samples,
         "requests": len(latencies),
         "offered_rate_req_s": rate,
         "wall_s": wall,
@@ -98,8 +150,14 @@ def main() -> None:
     ap.add_argument("--seconds", type=float, default=2.0)
     ap.add_argument("--seed", type=int, default=42)
     ap.add_argument("--quantum", type=int, default=128)
+    ap.add_argument("--policy", choices=["fifo", "srpt"], default="fifo")
+    ap.add_argument("--tracking", choices=["auto", "on", "off"], default="auto")
+    ap.add_argument("--host-io", action="store_true")
     a = ap.parse_args()
-    print(json.dumps(run_stream(a.rate, a.seconds, a.seed, quantum=a.quantum)))
+    r = run_stream(a.rate, a.seconds, a.seed, quantum=a.quantum, policy=a.policy,
+                   tracking=a.tracking, host_io=a.host_io)
+    r.pop("samples")
+    print(json.dumps(r))
 
 
 if __name__ == "__main__":

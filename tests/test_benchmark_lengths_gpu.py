@@ -8,6 +8,7 @@ the full run the same way (experiment_manager.hpp:272-307).
   dense 8192^2, 32-bit rows, 4096 generations
   sparse 16384^2 (1 % of 64x64 slots Bernoulli(0.35)), 20000 generations, change tracking
   the 512 uneven grids of the batched workload after one batched launch
+  every 64th request of the serving stream
 """
 import os
 from concurrent.futures import ThreadPoolExecutor
@@ -75,3 +76,26 @@ def test_batched_workload_every_grid():
                              range(len(work))))
     bad = [i for i in range(len(work)) if not np.array_equal(got[i], want[i])]
     assert not bad, bad[:10]
+
+
+def test_serving_stream_sampled_requests():
+    """The benchmark's serving stream (Poisson 2000 req/s for 2 s, sides
+    128..8192, 16..8192 generations, change tracking on long requests):
+    every 64th request's result, fetched as cells, equals the oracle on the
+    same input made on the host."""
+    import serve
+    r = serve.run_stream(rate=2000.0, seconds=2.0, seed=42, fetch="cells", check_every=64)
+    assert r["requests"] > 3000
+    samples = r["samples"]
+    assert len(samples) > 40
+
+    def one(item):
+        d, out = item
+        cells = golb200.load_hash_bernoulli(d["x"], d["y"], d["cell_seed"], d["density"])
+        want = oracle.life_rows(oracle.pack_rows(cells, 32), d["x"], d["gens"], 32,
+                                threads=1 if d["x"] * d["y"] < (1 << 21) else 8)
+        return bool(np.array_equal(oracle.pack_rows(out, 32), want))
+    workers = max(1, (os.cpu_count() or 2) // 2)
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        ok = list(pool.map(one, samples))
+    assert all(ok), [i for i, v in enumerate(ok) if not v][:10]
