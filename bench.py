@@ -635,7 +635,8 @@ def bench_batched_settling(stream, device, n: int = 512, seed: int = SEED) -> di
     settling inputs: dead grids with patches of Bernoulli(0.35) soup in 5 %
     of their 64 x 64 slots (at least one). Batched with change tracking
     (autotuned: a first run, gol_batch_retune, then timed runs) against the
-    same batch with tracking off; every grid checked against the oracle."""
+    same batch with every grid tracked and with none; every grid of every
+    run checked against the oracle."""
     import concurrent.futures as cf
 
     import golb200
@@ -651,17 +652,18 @@ def bench_batched_settling(stream, device, n: int = 512, seed: int = SEED) -> di
     out = {"workload": f"{n} grids as the batched workload (seed {seed}), dead with Bernoulli(0.35) "
                        "patches in 5 % of 64x64 slots (at least one)", "unit": UNIT}
     results = {}
-    for mode in ("on", "off"):
+    # on: every grid tracked; off: none; auto: the autotuner (a first run,
+    # gol_batch_retune, then the timed runs)
+    for mode in ("on", "off", "auto"):
         b = golb200.GolBatch(device=device, stream=stream.cuda_stream)
         for d, w in zip(work, inputs):
             gid = b.add(oracle.unpack_rows(w, d["x"], 64), d["gens"])
-            if mode == "off":
-                b.set_tracking(gid, "off")
+            b.set_tracking(gid, mode)
         b.upload()
         info = b.info()
         b.run()
         b.sync()
-        if mode == "on":
+        if mode == "auto":
             b.retune()
             b.run()
             b.sync()
@@ -669,19 +671,21 @@ def bench_batched_settling(stream, device, n: int = 512, seed: int = SEED) -> di
         out[f"value_tracking_{mode}"] = info["cell_updates"] / (ms * 1e-3) / 1e9
         out[f"ms_tracking_{mode}"] = ms
         out[f"items_tracking_{mode}"] = b.tiles()
+        stats = [b.grid_stats(i) for i in range(n)]
+        out[f"grids_tracked_{mode}"] = sum(1 for st in stats if st["tracked"])
         if mode == "on":
-            out["grids_still_before_their_end"] = sum(
-                1 for i in range(n) if b.grid_stats(i)["still_pass"] is not None)
+            out["grids_still_before_their_end"] = sum(1 for st in stats if st["still_pass"] is not None)
         results[mode] = [oracle.pack_rows(b.fetch(i), 64) for i in range(n)]
         b.close()
-    out["speedup_tracking"] = out["value_tracking_on"] / out["value_tracking_off"]
+    out["speedup_tracking_on"] = out["value_tracking_on"] / out["value_tracking_off"]
+    out["speedup_autotuned"] = out["value_tracking_auto"] / out["value_tracking_off"]
     out["cell_updates"] = info["cell_updates"]
 
     def check(i):
         d = work[i]
         want = oracle.life_rows(inputs[i], d["x"], d["gens"], 64,
                                 threads=1 if inputs[i].size < (1 << 16) else 4)
-        return bool(np.array_equal(results["on"][i], want) and np.array_equal(results["off"][i], want))
+        return all(bool(np.array_equal(results[m][i], want)) for m in results)
     with cf.ThreadPoolExecutor(max_workers=max(1, (os.cpu_count() or 2) // 2)) as pool:
         ok = list(pool.map(check, range(n)))
     out["all_equal_oracle"] = all(ok)
@@ -691,20 +695,22 @@ def bench_batched_settling(stream, device, n: int = 512, seed: int = SEED) -> di
 def bench_serving(device) -> dict:
     """Poisson stream, mean 2000 requests/s, sides log-uniform [128, 8192]
     (multiples of 64), density U[0.1, 0.5], generations log-uniform
-    [16, 8192]. Four runs of the same 2-s stream: arrival-order (FIFO) and
-    least-work-first (SRPT) scheduling with inputs generated on the device and
-    packed results copied back, then both again with host I/O (host cells in
-    through gol_serve_submit, cells out through gol_serve_fetch). Change
-    tracking is on for long requests (auto). Every 64th request of the FIFO
-    runs is checked against the oracle."""
+    [16, 8192]. Arrival-order (FIFO) and least-work-first (SRPT) scheduling
+    on the 2-s stream with inputs generated on the device and packed results
+    copied back, then both with host I/O (host cells, made before the stream
+    starts, in through gol_serve_submit; cells out through gol_serve_fetch)
+    on the stream's first 0.5 s. Change tracking is on for long requests
+    (auto). Every 64th request of the FIFO runs is checked against the
+    oracle."""
     import serve
     out = {"workload": "Poisson arrivals, mean 2000 req/s for 2 s, sides log-uniform [128, 8192] "
                        "x64, density U[0.1, 0.5], generations log-uniform [16, 8192], seed 42",
            "unit_throughput": "cell-updates/s"}
     for policy in ("fifo", "srpt"):
         for host_io in (False, True):
-            r = serve.run_stream(rate=2000.0, seconds=2.0, seed=SEED, device=device, policy=policy,
-                                 host_io=host_io, check_every=64 if policy == "fifo" else 0)
+            r = serve.run_stream(rate=2000.0, seconds=0.5 if host_io else 2.0, seed=SEED,
+                                 device=device, policy=policy, host_io=host_io,
+                                 check_every=64 if policy == "fifo" else 0)
             samples = r.pop("samples")
             if samples:
                 r["check"] = _check_serving_samples(samples)

@@ -361,8 +361,10 @@ int gol_batch_census(gol_batch* b, uint64_t* wait_cycles, uint64_t* work_cycles)
  * once. GOL_TRACK_AUTO (default) tracks grids of at least 8 passes until
  * gol_batch_retune has seen a run; gol_batch_retune then keeps tracking per
  * grid where the run skipped at least 5 % of its items (finest tiles, 16-row
- * bands, from 50 %) and runs the others dense. Both take effect at the next
- * upload/run. */
+ * bands, from 50 %) and runs the others dense, and turns tracking off for
+ * the whole batch when the items it would skip do not pay for the tracked
+ * kernel's extra time on every item (about 25 %). Both take effect at the
+ * next upload/run. */
 enum gol_track_mode { GOL_TRACK_AUTO = 0, GOL_TRACK_OFF = 1, GOL_TRACK_ON = 2 };
 int gol_batch_set_tracking(gol_batch* b, int32_t grid_id, int32_t mode);
 int gol_batch_retune(gol_batch* b);
@@ -415,8 +417,8 @@ int gol_serve_drain(gol_server* s);
  * GOL_SERVE_FIFO (default) admits in arrival order and advances every
  * running request by `quantum` generations per round; GOL_SERVE_SRPT admits
  * the queued request with the least work (cells x generations) first and
- * scales a small grid's per-round generations up by 2^20 / its cells, so
- * small requests finish in few rounds. */
+ * scales a small grid's per-round generations up by 2^20 / its cells (at
+ * most 4 quanta), so small requests finish in fewer rounds. */
 enum gol_serve_policy { GOL_SERVE_FIFO = 0, GOL_SERVE_SRPT = 1 };
 int gol_serve_set_policy(gol_server* s, int32_t policy);
 /* Change tracking for requests submitted from then on (GOL_TRACK_AUTO: those

@@ -52,6 +52,15 @@
 #ifndef GOL_BATCH_MIN_BLOCKS
 #define GOL_BATCH_MIN_BLOCKS 1   // resident one-warp CTAs per SM the registers are sized for
 #endif
+#ifndef GOL_BATCH_TRACK_OLD
+// How tracked items read a row before the pass to compare: 3 = through a
+// second shared-memory ring beside the row ring, 1 = a global load when
+// storing.
+#define GOL_BATCH_TRACK_OLD 3
+#endif
+#ifndef GOL_BATCH_TRACK_CAP
+#define GOL_BATCH_TRACK_CAP 1   // hold tracked variants near the untracked registers
+#endif
 
 namespace golb200 {
 
@@ -129,7 +138,7 @@ __device__ __forceinline__ uint32_t seg_group(const BatchGrid& G, int group, int
     const int f0 = 3 * K;
     const int f1 = min(G.band + 2 * K - 1, G.Y - y0_last + K - 1);
     const int fast_end = f1 > f0 ? f0 + (f1 - f0) / 3 * 3 : f0;
-    constexpr int TR = TRACK ? 3 : 0;   // old rows through the second ring
+    constexpr int TR = TRACK ? GOL_BATCH_TRACK_OLD : 0;
     if (fast_end > f0) {
         temporal_steps<WPL, K, false, false, TR, true, true>(s, c, 0, f0);
         temporal_steps<WPL, K, true, true, TR, true, true>(s, c, f0, fast_end);
@@ -185,8 +194,9 @@ __device__ __forceinline__ void release_max(int* p, int v) {
 // at 4 words per lane a cap spills heavily, so none is set.
 template <int WPL_ONLY, bool TRACK>
 constexpr int batch_min_blocks() {
-    return !TRACK ? GOL_BATCH_MIN_BLOCKS
-                  : (WPL_ONLY == 1 ? 19 : WPL_ONLY == 2 ? 15 : GOL_BATCH_MIN_BLOCKS);
+    return !TRACK || !GOL_BATCH_TRACK_CAP
+               ? GOL_BATCH_MIN_BLOCKS
+               : (WPL_ONLY == 1 ? 19 : WPL_ONLY == 2 ? 15 : GOL_BATCH_MIN_BLOCKS);
 }
 
 template <int WPL_ONLY, bool TRACK>
@@ -194,7 +204,8 @@ __global__ void __launch_bounds__(32, (batch_min_blocks<WPL_ONLY, TRACK>()))
 batch_kernel(const BatchGrid* __restrict__ grids, const BatchItem* __restrict__ items, int nitems,
              int* ticket, int* done, int* status, unsigned long long* census, long long spin_limit) {
     // the row ring, and with TRACK the old-row ring right after it
-    __shared__ __align__(16) uint32_t ring[kRowRing * 32 * (WPL_ONLY ? WPL_ONLY : 4) * (TRACK ? 2 : 1)];
+    __shared__ __align__(16) uint32_t
+        ring[kRowRing * 32 * (WPL_ONLY ? WPL_ONLY : 4) * (TRACK && GOL_BATCH_TRACK_OLD == 3 ? 2 : 1)];
     constexpr int kEdgeWords = WPL_ONLY == 1 ? 1 : seg_edge_words(kBatchMaxK);   // 1: shuffles
     __shared__ uint32_t etab[kEdgeWords];
     const int lane = threadIdx.x & 31;
@@ -606,6 +617,10 @@ constexpr int kTrackMinPasses = 8;
 constexpr double kRetuneMinSkip = 0.05;    // skipped share below which a grid runs dense
 constexpr double kRetuneFineSkip = 0.5;    // skipped share from which it gets the finest tiles
 constexpr int kRetuneFineRows = 16;        // the planner's smallest band
+// Time of an item under the tracked kernel over the untracked one (the
+// settling variant of the 512-grid workload: 65.2 ms for 3.51 M computed
+// items against 52.5 ms for 3.56 M untracked ones).
+constexpr double kTrackItemCost = 1.25;
 
 int forced_band(const gol_batch::Entry& e) { return e.force_band ? e.force_band : e.tile_rows_hint; }
 
@@ -1081,15 +1096,32 @@ int gol_batch_retune(gol_batch* b) {
     if (ce == cudaSuccess && !st.empty())
         ce = cudaMemcpy(st.data(), b->d_gstat, st.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost);
     if (ce != cudaSuccess) return b->cuda_fail(ce, "batch retune");
+    // Per grid: keep tracking where it skipped enough of the grid's items.
+    // Then for the batch: a launch with any tracked grid runs the tracked
+    // kernel for every item, at kTrackItemCost times an untracked item's
+    // time, so tracking stays on only if the items it skips pay for that.
+    double with_tracking = 0, without = 0;
+    bool forced = false;
     for (size_t i = 0; i < b->grids.size(); ++i) {
         auto& e = b->grids[i];
-        if (e.track_mode != GOL_TRACK_AUTO || !e.tracked) continue;
-        const double total = (double)st[2 * i] + st[2 * i + 1];
-        if (total <= 0) continue;
+        const double computed = st[2 * i], total = (double)st[2 * i] + st[2 * i + 1];
+        without += total;
+        forced |= e.track_mode == GOL_TRACK_ON && e.choice.passes > 0;
+        if (e.track_mode != GOL_TRACK_AUTO || !e.tracked || total <= 0) {
+            with_tracking += kTrackItemCost * (e.tracked ? computed : total);
+            continue;
+        }
         const double skip = st[2 * i + 1] / total;
         e.auto_track = skip >= kRetuneMinSkip ? 1 : 0;
         e.tile_rows_hint = (e.auto_track == 1 && skip >= kRetuneFineSkip) ? kRetuneFineRows : 0;
+        with_tracking += kTrackItemCost * (e.auto_track ? computed : total);
     }
+    if (!forced && with_tracking >= without)
+        for (auto& e : b->grids)
+            if (e.track_mode == GOL_TRACK_AUTO) {
+                e.auto_track = 0;
+                e.tile_rows_hint = 0;
+            }
     b->uploaded = false;
     return GOL_OK;
 }

@@ -70,8 +70,8 @@ void parallel_rows(size_t y, size_t bytes_per_row, F&& body) {
     const size_t total = y * bytes_per_row;
     unsigned hw = std::thread::hardware_concurrency();
     size_t nt = std::max<size_t>(1, std::min<size_t>(hw ? hw : 1, 64));
-    // Below ~4 MiB threads cost more than they save.
-    nt = std::min(nt, std::max<size_t>(1, total >> 22));
+    // One thread per MiB: below that a thread costs more than it saves.
+    nt = std::min(nt, std::max<size_t>(1, total >> 20));
     nt = std::min(nt, std::max<size_t>(y, 1));
     if (nt <= 1) {
         body(0, y);

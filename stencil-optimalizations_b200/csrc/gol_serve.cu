@@ -35,6 +35,7 @@ namespace {
 constexpr int kRoundsInFlight = 3;
 constexpr uint64_t kServeTrackMinPasses = 8;   // auto: requests this long track changes
 constexpr double kServeRefCells = 1024.0 * 1024.0;
+constexpr double kServeMaxScale = 4.0;
 
 struct Request {
     uint64_t id = 0;
@@ -316,9 +317,12 @@ static uint64_t round_generations(const gol_server* s, const Request& r) {
     const uint64_t k = (uint64_t)r.plan.k;
     uint64_t q = s->quantum;
     if (s->policy == GOL_SERVE_SRPT) {
+        // at most kServeMaxScale quanta: a round lasts at least as long as
+        // its longest chain of dependent passes, so an unbounded scale for
+        // tiny grids (up to 64 quanta) made every round long
         const double cells = (double)r.x * (double)r.y;
-        const double scale = std::max(1.0, kServeRefCells / std::max(cells, 1.0));
-        q = (uint64_t)std::min<double>((double)s->quantum * scale, 1e12);
+        const double scale = std::min(kServeMaxScale, std::max(1.0, kServeRefCells / std::max(cells, 1.0)));
+        q = (uint64_t)((double)s->quantum * scale);
     }
     q = std::max(k, q / k * k);
     return left <= q ? left : q;

@@ -40,12 +40,12 @@ def run_stream(rate: float = 2000.0, seconds: float = 2.0, seed: int = 42, min_s
                check_every: int = 0) -> dict:
     """Serves the seeded Poisson stream that arrives within `seconds`.
 
-    host_io: every request's cells are made on the host (the same cells
-    gol_serve_submit_random would make on the device, by a pool of threads
-    working ahead of the arrivals, as clients would hold them) and submitted
-    through gol_serve_submit (host pack, copy to the device at admission);
-    every result is fetched as cells (copy back, host unpack). Otherwise
-    inputs are generated on the device and results fetched as packed words.
+    host_io: every request's cells are made on the host before the stream
+    starts (the same cells gol_serve_submit_random would make on the device,
+    held as clients would hold them) and submitted through gol_serve_submit
+    (host pack, copy to the device at admission); every result is fetched as
+    cells (copy back, host unpack). Otherwise inputs are generated on the
+    device and results fetched as packed words.
     check_every > 0 keeps the fetched result of every check_every-th request
     (submission order) in r["samples"] as (request, result)."""
     from concurrent.futures import ThreadPoolExecutor
@@ -59,38 +59,27 @@ def run_stream(rate: float = 2000.0, seconds: float = 2.0, seed: int = 42, min_s
     srv = server or golb200.GolServer(device=device, arena_bytes=arena_bytes, quantum=quantum)
     srv.set_policy(policy)
     srv.set_tracking(tracking)
-    pool = ThreadPoolExecutor(max_workers=max(1, (os.cpu_count() or 2) // 2)) if host_io else None
-    ahead: dict[int, object] = {}
-
-    def make_cells(d):
-        return golb200.load_hash_bernoulli(d["x"], d["y"], d["cell_seed"], d["density"])
-
-    def prefetch(upto: int) -> None:
-        for j in range(upto, min(len(keep), upto + 64)):
-            if j not in ahead:
-                ahead[j] = pool.submit(make_cells, work[keep[j]])
+    host_cells = []
+    if host_io:
+        with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as pool:
+            host_cells = list(pool.map(
+                lambda j: golb200.load_hash_bernoulli(work[j]["x"], work[j]["y"], work[j]["cell_seed"],
+                                                      work[j]["density"]), keep))
 
     pending: dict[int, tuple[float, int, int]] = {}
     latencies: list[float] = []
     samples: list[tuple[dict, np.ndarray]] = []
     cell_updates = 0
     submitted = 0
-    late = 0
-    if pool:
-        prefetch(0)
-        for f in list(ahead.values()):
-            f.result()
     t0 = time.perf_counter()
     try:
         while submitted < len(keep) or pending:
             now = time.perf_counter() - t0
             while submitted < len(keep) and arrivals[keep[submitted]] <= now:
                 d = work[keep[submitted]]
-                if pool:
-                    prefetch(submitted)
-                    f = ahead.pop(submitted)
-                    late += 0 if f.done() else 1
-                    rid = srv.submit(f.result(), d["gens"])
+                if host_io:
+                    rid = srv.submit(host_cells[submitted], d["gens"])
+                    host_cells[submitted] = None
                 else:
                     rid = srv.submit_random(d["x"], d["y"], d["gens"], d["cell_seed"], d["density"])
                 pending[rid] = (float(arrivals[keep[submitted]]), d["x"] * d["y"] * d["gens"],
@@ -121,14 +110,12 @@ def run_stream(rate: float = 2000.0, seconds: float = 2.0, seed: int = 42, min_s
         stats = srv.stats()
         tiles = srv.tiles()
     finally:
-        if pool:
-            pool.shutdown(wait=False, cancel_futures=True)
         if own:
             srv.close()
     lat = np.array(latencies) if latencies else np.zeros(1)
     return {
         "policy": policy, "tracking": tracking, "host_io": host_io,
-        "inputs_generated_late": late, "tiles_computed": tiles["computed"],
+        "tiles_computed": tiles["computed"],
         "tiles_skipped": tiles["skipped"], "finished_early_still": tiles["early_finished"],
         "samples": samples,
         "requests": len(latencies),
