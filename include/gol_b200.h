@@ -413,12 +413,10 @@ int gol_serve_stats(const gol_server* s, uint64_t* queued, uint64_t* running, ui
                     uint64_t* cell_updates, uint64_t* arena_free_bytes);
 /* Waits for every queued round. */
 int gol_serve_drain(gol_server* s);
-/* Scheduling policy, for requests submitted and rounds planned from then on:
- * GOL_SERVE_FIFO (default) admits in arrival order and advances every
- * running request by `quantum` generations per round; GOL_SERVE_SRPT admits
- * the queued request with the least work (cells x generations) first and
- * scales a small grid's per-round generations up by 2^20 / its cells (at
- * most 4 quanta), so small requests finish in fewer rounds. */
+/* Admission policy: GOL_SERVE_FIFO (default) admits queued requests in
+ * arrival order, GOL_SERVE_SRPT the one with the least work (cells x
+ * generations) first, when the arena cannot take them all. Either way every
+ * running request advances `quantum` generations per round. */
 enum gol_serve_policy { GOL_SERVE_FIFO = 0, GOL_SERVE_SRPT = 1 };
 int gol_serve_set_policy(gol_server* s, int32_t policy);
 /* Change tracking for requests submitted from then on (GOL_TRACK_AUTO: those

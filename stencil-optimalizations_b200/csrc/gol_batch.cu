@@ -59,7 +59,7 @@
 #define GOL_BATCH_TRACK_OLD 3
 #endif
 #ifndef GOL_BATCH_TRACK_CAP
-#define GOL_BATCH_TRACK_CAP 1   // hold tracked variants near the untracked registers
+#define GOL_BATCH_TRACK_CAP 0   // 1: hold tracked variants near the untracked registers
 #endif
 
 namespace golb200 {
@@ -125,7 +125,9 @@ __device__ __forceinline__ uint32_t seg_group(const BatchGrid& G, int group, int
             s.o[g][0][w] = s.o[g][1][w] = s.o[g][2][w] = 0u;
         }
     }
-    for (int j = 0; j < kRowsInFlight; ++j) issue_row<WPL, K>(c, j, j);
+    constexpr int TR = TRACK ? GOL_BATCH_TRACK_OLD : 0;
+    // (with TRACK the first rows' old-row copies travel with them too)
+    for (int j = 0; j < kRowsInFlight; ++j) issue_row<WPL, K, TR, true>(c, j, j);
     cp_async_wait<kRowsInFlight - 1>();
     lds_words<WPL>(c.ring, s.ld[0]);
     s.diff = 0u;
@@ -138,7 +140,6 @@ __device__ __forceinline__ uint32_t seg_group(const BatchGrid& G, int group, int
     const int f0 = 3 * K;
     const int f1 = min(G.band + 2 * K - 1, G.Y - y0_last + K - 1);
     const int fast_end = f1 > f0 ? f0 + (f1 - f0) / 3 * 3 : f0;
-    constexpr int TR = TRACK ? GOL_BATCH_TRACK_OLD : 0;
     if (fast_end > f0) {
         temporal_steps<WPL, K, false, false, TR, true, true>(s, c, 0, f0);
         temporal_steps<WPL, K, true, true, TR, true, true>(s, c, f0, fast_end);

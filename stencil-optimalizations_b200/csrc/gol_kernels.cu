@@ -11,7 +11,10 @@
 #define GOL_STREAM_THREADS 128   // CTA size of the one-generation streaming kernel
 #endif
 #ifndef GOL_STREAM_CTAS_PER_SM
-#define GOL_STREAM_CTAS_PER_SM 16   // default band: about this many CTAs per SM per pass
+// Default band of the streaming kernel: about this many CTAs per SM per pass
+// (at 32768^2: 9-row bands; 8-, 12- and 16-row bands ran at 5.40, 5.31 and
+// 5.15 TB/s algorithmic).
+#define GOL_STREAM_CTAS_PER_SM 48
 #endif
 
 namespace golb200 {
@@ -102,8 +105,8 @@ bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPla
         // One generation: lanes of wpl words across the row in CTAs of up to
         // GOL_STREAM_THREADS threads, each thread walking `band` rows. The
         // default band gives about GOL_STREAM_CTAS_PER_SM CTAs per SM (many
-        // resident warps, several waves), never below 8 rows (each band
-        // re-reads one halo row above and one below) nor above 64.
+        // waves of short-lived CTAs), never below 8 rows (each band re-reads
+        // one halo row above and one below, from L2) nor above 64.
         plan->threads = std::min(GOL_STREAM_THREADS, (lanes + 31) / 32 * 32);
         plan->nslices = (lanes + plan->threads - 1) / plan->threads;
         plan->slice = plan->threads * wpl;

@@ -34,8 +34,7 @@ namespace {
 
 constexpr int kRoundsInFlight = 3;
 constexpr uint64_t kServeTrackMinPasses = 8;   // auto: requests this long track changes
-constexpr double kServeRefCells = 1024.0 * 1024.0;
-constexpr double kServeMaxScale = 4.0;
+constexpr size_t kStageBytes = (size_t)256 << 20;   // pinned staging ring for host inputs
 
 struct Request {
     uint64_t id = 0;
@@ -85,6 +84,19 @@ struct gol_server {
     cudaStream_t stream = nullptr;         // uploads and rounds, in order
     bool own_stream = false;
     cudaStream_t copy_stream = nullptr;    // result copies, overlapping later rounds
+    // Host inputs reach the device through a pinned staging ring on their
+    // own stream (a copy from pageable memory would first wait for every
+    // round queued on the round stream); the round stream waits for each
+    // upload's event before the round that first uses it.
+    cudaStream_t upload_stream = nullptr;
+    uint8_t* stage = nullptr;
+    size_t stage_bytes = 0, stage_head = 0;
+    struct StageUse {
+        size_t pos, len;
+        cudaEvent_t done;
+    };
+    std::deque<StageUse> stage_uses;       // uploads whose staging bytes may still be read
+    std::vector<cudaEvent_t> free_events;
     int num_sms = 148;
     uint32_t* arena = nullptr;
     size_t arena_words = 0;
@@ -174,6 +186,52 @@ int ensure_round_capacity(gol_server* s, RoundBuffers& r, size_t grids, size_t i
     return GOL_OK;
 }
 
+// Copies a request's packed host input into its slot: through the pinned
+// staging ring on the upload stream, the round stream waiting for it (an
+// input larger than the ring goes straight from pageable memory).
+cudaError_t upload_words(gol_server* s, uint32_t* dst, const std::vector<uint32_t>& words) {
+    const size_t len = words.size() * sizeof(uint32_t);
+    if (len == 0) return cudaSuccess;
+    if (len > s->stage_bytes)
+        return cudaMemcpyAsync(dst, words.data(), len, cudaMemcpyHostToDevice, s->stream);
+    size_t pos = (s->stage_head + 255) / 256 * 256;
+    if (pos + len > s->stage_bytes) pos = 0;
+    // wait for the uploads still reading bytes we are about to overwrite
+    while (!s->stage_uses.empty()) {
+        const auto& u = s->stage_uses.front();
+        const bool overlap = u.pos < pos + len && pos < u.pos + u.len;
+        if (!overlap && cudaEventQuery(u.done) != cudaSuccess) break;
+        cudaError_t ce = cudaEventSynchronize(u.done);
+        if (ce != cudaSuccess) return ce;
+        s->free_events.push_back(u.done);
+        s->stage_uses.pop_front();
+    }
+    for (const auto& u : s->stage_uses)   // (an older one left overlapping: wait for it too)
+        if (u.pos < pos + len && pos < u.pos + u.len) {
+            cudaError_t ce = cudaEventSynchronize(u.done);
+            if (ce != cudaSuccess) return ce;
+        }
+    std::memcpy(s->stage + pos, words.data(), len);
+    cudaEvent_t ev = nullptr;
+    if (!s->free_events.empty()) {
+        ev = s->free_events.back();
+        s->free_events.pop_back();
+    } else {
+        cudaError_t ce = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (ce != cudaSuccess) return ce;
+    }
+    cudaError_t ce = cudaMemcpyAsync(dst, s->stage + pos, len, cudaMemcpyHostToDevice, s->upload_stream);
+    if (ce == cudaSuccess) ce = cudaEventRecord(ev, s->upload_stream);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(s->stream, ev, 0);
+    if (ce != cudaSuccess) {
+        s->free_events.push_back(ev);
+        return ce;
+    }
+    s->stage_uses.push_back({pos, len, ev});
+    s->stage_head = pos + len;
+    return cudaSuccess;
+}
+
 // Marks the requests of a completed round finished and checks its status.
 int retire_round(gol_server* s, RoundBuffers& r) {
     const int st = *r.h_status;           // copied before the round's event was recorded
@@ -256,6 +314,11 @@ int gol_serve_create(gol_server** out, int32_t device, uint64_t arena_bytes, uin
         }
     }
     if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&s->upload_stream, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) {
+        s->stage_bytes = kStageBytes;
+        ce = cudaMallocHost(&s->stage, s->stage_bytes);
+    }
     if (ce == cudaSuccess && arena_bytes == 0) {
         // Admission is bounded by the HBM free when the server starts:
         // half of it goes to resident grids.
@@ -274,6 +337,8 @@ int gol_serve_create(gol_server** out, int32_t device, uint64_t arena_bytes, uin
         if (s->d_census) cudaFree(s->d_census);
         if (s->own_stream) cudaStreamDestroy(s->stream);
         if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
+        if (s->upload_stream) cudaStreamDestroy(s->upload_stream);
+        if (s->stage) cudaFreeHost(s->stage);
         delete s;
         return ce == cudaErrorMemoryAllocation ? GOL_E_NOMEM : GOL_E_CUDA;
     }
@@ -309,22 +374,18 @@ static uint32_t* slot_trk(gol_server* s, const Request& r) { return slot_gstat(s
 // shortest-work-first policy the quantum scaled up for grids smaller than
 // kServeRefCells cells (so small requests finish in few rounds while a
 // round's work stays bounded by the large ones' quantum).
-// Every round but a request's last advances a multiple of its depth k, so
-// its change flags (which speak of k-generation passes) stay valid from
-// round to round; only the last round may end with a shorter pass.
+// Generations a request advances in one round: the quantum. Every round
+// but a request's last advances a multiple of its depth k, so its change
+// flags (which speak of k-generation passes) stay valid from round to
+// round; only the last round may end with a shorter pass. (Giving small
+// grids more generations per round, 2^20 / cells quanta, at most 64 or at
+// most 4, made rounds as long as those grids' chains of dependent passes:
+// on the 2000 req/s stream p50 rose from 9.7 to 36-57 ms and p99 from 94 to
+// 430-600 ms, so both policies use the quantum.)
 static uint64_t round_generations(const gol_server* s, const Request& r) {
     const uint64_t left = r.gens - r.planned;
     const uint64_t k = (uint64_t)r.plan.k;
-    uint64_t q = s->quantum;
-    if (s->policy == GOL_SERVE_SRPT) {
-        // at most kServeMaxScale quanta: a round lasts at least as long as
-        // its longest chain of dependent passes, so an unbounded scale for
-        // tiny grids (up to 64 quanta) made every round long
-        const double cells = (double)r.x * (double)r.y;
-        const double scale = std::min(kServeMaxScale, std::max(1.0, kServeRefCells / std::max(cells, 1.0)));
-        q = (uint64_t)((double)s->quantum * scale);
-    }
-    q = std::max(k, q / k * k);
+    const uint64_t q = std::max(k, s->quantum / k * k);
     return left <= q ? left : q;
 }
 
@@ -409,8 +470,7 @@ int gol_serve_step(gol_server* s) {
             ce = golb200::launch_hash_bernoulli(s->arena + off, r.x, r.y, r.input_seed,
                                                 r.input_density, s->stream);
         } else {
-            ce = cudaMemcpyAsync(s->arena + off, r.words.data(), r.words.size() * sizeof(uint32_t),
-                                 cudaMemcpyHostToDevice, s->stream);
+            ce = upload_words(s, s->arena + off, r.words);
         }
         // counters zero; change flags "changed" (the first pass computes
         // every tile) and no still pass
@@ -664,6 +724,11 @@ void gol_serve_destroy(gol_server* s) {
     if (s->arena) cudaFree(s->arena);
     if (s->d_census) cudaFree(s->d_census);
     if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
+    if (s->upload_stream) cudaStreamSynchronize(s->upload_stream);
+    for (auto& u : s->stage_uses) cudaEventDestroy(u.done);
+    for (auto ev : s->free_events) cudaEventDestroy(ev);
+    if (s->upload_stream) cudaStreamDestroy(s->upload_stream);
+    if (s->stage) cudaFreeHost(s->stage);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }

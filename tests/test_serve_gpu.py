@@ -132,12 +132,10 @@ def test_tracking_and_policies_same_alone_and_in_the_mix(tracking, policy):
                     break
     if tracking == "on":
         # tiles of the dead grid, the block and the settled patches are
-        # skipped; under FIFO's fixed 64-generation rounds the dead grid and
-        # the block are found still in their first round and finish early
-        # (SRPT gives these small grids all their generations in one round)
+        # skipped; the dead grid and the block are found still in their first
+        # 64-generation round and finish early
         assert t["skipped"] > 0
-        if policy == "fifo":
-            assert t["early_finished"] >= 2
+        assert t["early_finished"] >= 2
     if tracking == "off":
         assert t["skipped"] == 0 and t["early_finished"] == 0
 
