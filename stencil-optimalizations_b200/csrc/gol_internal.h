@@ -24,8 +24,6 @@ struct RowsPlan {
     int halo = 0;      // x-halo words each side of a slice (0 when unsliced)
     bool stream = false;   // k = 1 streaming kernel (gol_rows_stream.cuh): band = rows
                            // per thread, nslices = CTAs across the row, no halo
-    bool warp = false;     // narrow grids: one-warp CTAs, 30-lane x-slices with a
-                           // context lane each side (rows_warp_kernel)
 };
 
 // Picks words-per-lane and CTA shape for a W-word by Y-row grid and depth k.

@@ -10,13 +10,6 @@
 #ifndef GOL_STREAM_THREADS
 #define GOL_STREAM_THREADS 128   // CTA size of the one-generation streaming kernel
 #endif
-#ifndef GOL_WARP_PLAN
-#define GOL_WARP_PLAN 1   // narrow grids (CTAs of fewer than four warps) use one-warp slices
-#endif
-#ifndef GOL_WARP_CTAS_PER_SM
-#define GOL_WARP_CTAS_PER_SM 16   // default band of the one-warp plan: CTAs per SM per pass
-#endif
-
 #ifndef GOL_STREAM_CTAS_PER_SM
 // Default band of the streaming kernel: about this many CTAs per SM per pass
 // (at 32768^2: 9-row bands; 8-, 12- and 16-row bands ran at 5.40, 5.31 and
@@ -73,26 +66,11 @@ cudaError_t launch_stream(const RowsLaunch& a, const RowsPlan& p, cudaStream_t s
 }
 
 template <int WPL, int K>
-cudaError_t launch_warp(const RowsLaunch& a, const RowsPlan& p, cudaStream_t stream) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(p.nbands, p.nslices);
-    cfg.blockDim = dim3(32);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, rows_warp_kernel<WPL, K>, a);
-}
-
-template <int WPL, int K>
 cudaError_t dispatch_k(int k, const RowsLaunch& a, const RowsPlan& p, cudaStream_t stream) {
     if constexpr (K > kMaxKForWpl(WPL)) {
         return cudaErrorInvalidValue;
     } else {
-        if (k == K) return p.warp ? launch_warp<WPL, K>(a, p, stream) : launch_one<WPL, K>(a, p, stream);
+        if (k == K) return launch_one<WPL, K>(a, p, stream);
         return dispatch_k<WPL, K + 1>(k, a, p, stream);
     }
 }
@@ -137,26 +115,6 @@ bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPla
         if (band <= 0) {
             const long long ctas = (long long)GOL_STREAM_CTAS_PER_SM * num_sms;
             band = (int)std::min<long long>(64, std::max<long long>(8, ((long long)Y * plan->nslices + ctas - 1) / ctas));
-        }
-        band = std::min(band, std::max(Y, 1));
-        plan->band = band;
-        plan->nbands = (Y + band - 1) / band;
-        return true;
-    }
-    plan->warp = GOL_WARP_PLAN && allow_stream && lanes < 4 * 32 && lanes > kWarpSliceLanes;
-    if (plan->warp) {
-        // A narrow grid: CTAs spanning the row would have fewer than four
-        // warps; one-warp CTAs on 30-lane slices give many more CTAs with
-        // taller bands (fill and drain cost ~3k steps per band).
-        plan->slice = kWarpSliceLanes * wpl;
-        plan->nslices = (W + plan->slice - 1) / plan->slice;
-        plan->halo = wpl;
-        plan->threads = 32;
-        int band = band_rows;
-        if (band <= 0) {
-            const long long ctas = (long long)GOL_WARP_CTAS_PER_SM * num_sms;
-            band = (int)(((long long)Y * plan->nslices + ctas - 1) / ctas);
-            band = std::max(band, std::max(8, 4 * k));
         }
         band = std::min(band, std::max(Y, 1));
         plan->band = band;

@@ -543,85 +543,6 @@ rows_temporal_kernel(RowsLaunch a) {
     band_tile<WPL, K, 0>(a, blockIdx.x, blockIdx.y, smem);
 }
 
-// Narrow grids: one warp per CTA, one x-slice of 30 lanes of words (lanes 1
-// .. 30, stored) with a context lane each side (lanes 0 and 31: errors from
-// the unknown cells beyond them move one cell per generation and stay in
-// them for K <= 32), streaming one band. The warp is one segment of the
-// segmented-warp pipeline (shuffles at one word per lane, a per-warp edge
-// table otherwise; __syncwarp instead of a CTA barrier), so a narrow grid
-// gets many small CTAs with tall bands instead of few CTAs of one or two
-// warps. Grid: blockIdx.x = band, blockIdx.y = slice (a.slice = 30 * WPL).
-constexpr int kWarpSliceLanes = 30;
-
-template <int WPL, int K>
-__global__ void __launch_bounds__(32)
-rows_warp_kernel(RowsLaunch a) {
-    __shared__ __align__(16) uint32_t ring[kRowRing * 32 * WPL];
-    constexpr int kEdgeWords = WPL == 1 ? 1 : seg_edge_words(K);   // one word per lane: shuffles
-    __shared__ uint32_t etab[kEdgeWords];
-    pdl_trigger_and_wait();
-    const int lane = threadIdx.x & 31;
-    for (int u = lane; u < kEdgeWords; u += 32) etab[u] = 0u;
-    __syncwarp();
-    const int xs = blockIdx.y * a.slice;
-    TemporalCtx c;
-    c.src = a.src;
-    c.dst = a.dst;
-    c.W = a.W;
-    c.pitch = a.pitch;
-    c.Y = a.Y;
-    c.B = a.band;
-    c.y0 = blockIdx.x * a.band;
-    c.y1 = min(c.y0 + a.band, a.Y);
-    c.lane = lane;
-    c.base = xs + (lane - 1) * WPL;
-    c.lane_ok = c.base >= 0 && c.base < a.W;
-    c.own = c.lane_ok && lane >= 1 && lane <= kWarpSliceLanes;
-    c.seg_first = lane == 0;
-    c.seg_last = lane == 31;
-    c.eb = etab + lane;
-    c.el = c.seg_first ? etab : etab + lane;
-    c.er = c.seg_last ? etab + kSegEdgeStride - 1 : etab + lane + 2;
-    c.src_l = max(lane - 1, 0);
-    c.src_r = min(lane + 1, 31);
-    c.ring = ring + lane * WPL;
-    c.ring_saddr = (uint32_t)__cvta_generic_to_shared(c.ring);
-    c.ring_stride = ring_slot_words<WPL, true>();
-    set_word_masks<WPL>(c);
-
-    TemporalRegs<WPL, K> s;
-#pragma unroll
-    for (int w = 0; w < WPL; ++w) {
-        s.ld[0][w] = s.ld[1][w] = s.ld[2][w] = 0u;
-#pragma unroll
-        for (int g = 0; g < K; ++g) {
-            s.h0[g][0][w] = s.h0[g][1][w] = s.h0[g][2][w] = 0u;
-            s.h1[g][0][w] = s.h1[g][1][w] = s.h1[g][2][w] = 0u;
-            s.o[g][0][w] = s.o[g][1][w] = s.o[g][2][w] = 0u;
-        }
-    }
-    for (int j = 0; j < kRowsInFlight; ++j) issue_row<WPL, K, 0, true>(c, j, j);
-    cp_async_wait<kRowsInFlight - 1>();
-    lds_words<WPL>(c.ring, s.ld[0]);
-    s.diff = 0u;
-    const bool all_lanes_ok = xs - WPL >= 0 && xs + (32 - 1) * WPL <= a.W;
-    const int nsteps = c.B + 3 * K;
-    const int f0 = 3 * K;
-    const int f1 = min(c.B + 2 * K - 1, c.Y - c.y0 + K - 1);
-    const int fast_end = f1 > f0 ? f0 + (f1 - f0) / 3 * 3 : f0;
-    if (fast_end > f0) {
-        temporal_steps<WPL, K, false, false, 0, true>(s, c, 0, f0);
-        if (all_lanes_ok)
-            temporal_steps<WPL, K, true, false, 0, true>(s, c, f0, fast_end);
-        else
-            temporal_steps<WPL, K, true, true, 0, true>(s, c, f0, fast_end);
-        temporal_steps<WPL, K, false, false, 0, true>(s, c, fast_end, nsteps);
-    } else {
-        temporal_steps<WPL, K, false, false, 0, true>(s, c, 0, nsteps);
-    }
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-}
-
 // Shared memory a launch needs: the row ring (two with change tracking:
 // rows and old rows) and the edge table.
 __host__ __device__ inline size_t temporal_smem_bytes(int K, int threads, int wpl, bool track = false) {
