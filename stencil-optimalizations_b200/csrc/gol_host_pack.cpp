@@ -9,9 +9,15 @@
 // byte-to-bit multiply gather); unpacking expands eight cells per 64-bit
 // multiply and streams them out (it is bound by the memory writes); rows
 // are split across hardware threads.
+#include <unistd.h>
+
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
+#include <functional>
+#include <mutex>
 #include <random>
 #include <thread>
 #include <vector>
@@ -65,27 +71,94 @@ __attribute__((target("avx2"))) void pack_rows_avx2(const uint8_t* cells, size_t
 
 #endif
 
+// Worker threads kept for the life of the process (starting a thread per
+// call cost more than packing a few MiB), shared by every caller. A process
+// forked from one that started them has no workers (fork copies only the
+// calling thread), so there parallel_rows starts threads per call instead.
+class RowPool {
+  public:
+    static RowPool& get() {
+        static RowPool* pool = new RowPool();   // never destroyed: workers outlive statics
+        return *pool;
+    }
+    size_t workers() const { return threads_.size(); }
+    bool usable() const { return getpid() == pid_; }
+    void submit(std::function<void()> job) {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            jobs_.push_back(std::move(job));
+        }
+        cv_.notify_one();
+    }
+
+  private:
+    RowPool() : pid_(getpid()) {
+        const unsigned hw = std::thread::hardware_concurrency();
+        const size_t n = std::min<size_t>(hw > 1 ? hw - 1 : 0, 63);
+        for (size_t i = 0; i < n; ++i) threads_.emplace_back([this] { loop(); });
+        for (auto& t : threads_) t.detach();
+    }
+    void loop() {
+        for (;;) {
+            std::function<void()> job;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [this] { return !jobs_.empty(); });
+                job = std::move(jobs_.front());
+                jobs_.pop_front();
+            }
+            job();
+        }
+    }
+    pid_t pid_;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<std::function<void()>> jobs_;
+    std::vector<std::thread> threads_;
+};
+
 template <typename F>
 void parallel_rows(size_t y, size_t bytes_per_row, F&& body) {
     const size_t total = y * bytes_per_row;
     unsigned hw = std::thread::hardware_concurrency();
     size_t nt = std::max<size_t>(1, std::min<size_t>(hw ? hw : 1, 64));
-    // One thread per MiB: below that a thread costs more than it saves.
-    nt = std::min(nt, std::max<size_t>(1, total >> 20));
+    // One thread per 256 KiB: below that handing out the work costs more
+    // than it saves.
+    nt = std::min(nt, std::max<size_t>(1, total >> 18));
     nt = std::min(nt, std::max<size_t>(y, 1));
     if (nt <= 1) {
         body(0, y);
         return;
     }
-    std::vector<std::thread> ts;
     const size_t per = (y + nt - 1) / nt;
+    RowPool& pool = RowPool::get();
+    if (!pool.usable() || pool.workers() == 0) {
+        std::vector<std::thread> ts;
+        for (size_t t = 1; t < nt; ++t) {
+            const size_t y0 = t * per, y1 = std::min(y, y0 + per);
+            if (y0 >= y1) break;
+            ts.emplace_back([&body, y0, y1] { body(y0, y1); });
+        }
+        body(0, std::min(y, per));
+        for (auto& th : ts) th.join();
+        return;
+    }
+    std::mutex mu;
+    std::condition_variable cv;
+    size_t left = 0;
     for (size_t t = 1; t < nt; ++t) {
         const size_t y0 = t * per, y1 = std::min(y, y0 + per);
         if (y0 >= y1) break;
-        ts.emplace_back([&body, y0, y1] { body(y0, y1); });
+        ++left;
+        pool.submit([&, y0, y1] {
+            body(y0, y1);
+            std::lock_guard<std::mutex> lk(mu);
+            if (--left == 0) cv.notify_one();
+        });
     }
     body(0, std::min(y, per));
-    for (auto& th : ts) th.join();
+    std::unique_lock<std::mutex> lk(mu);
+    cv.wait(lk, [&] { return left == 0; });
 }
 
 } // namespace

@@ -97,3 +97,19 @@ def test_product_loader_matches_reference_generator(golden_cases):
             continue
         g = golb200.load_random_ones_zeros(case["x"], case["y"], case["seed"])
         assert f"{oracle.fnv1a64(g):016x}" == case["input_fnv1a64"], case["name"]
+
+
+@pytest.mark.parametrize("x,y", [(32, 1), (2048, 600), (4096, 1024), (16384, 700), (96, 3)])
+def test_host_pack_round_trip_without_a_device(x, y):
+    """set_and_format_input_data packs on the host (worker threads for
+    grids of more than 256 KiB of cells) and fetch_result unpacks: the
+    packed words are the reference's row layout and the round trip returns
+    the grid, all without a GPU."""
+    g = oracle.random_ones_zeros(x, y, x + y)
+    e = golb200.GolB200(grid_dimensions=(x, y), state_bits_count=32)
+    try:
+        e.set_and_format_input_data(g)
+        assert np.array_equal(e.fetch_words(32), oracle.pack_rows(g, 32))
+        assert np.array_equal(e.fetch_result(), g)
+    finally:
+        e.close()
