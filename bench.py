@@ -62,6 +62,15 @@ FLUSH_BYTES = 256 << 20
 ALG_INT_OPS_PER_CELL = 33.0 / 64.0
 
 
+def usable_cpus() -> int:
+    """Host threads this process may run on (its CPU affinity), not the
+    machine's total."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -251,7 +260,7 @@ def run_reference_arm(args, d: Dist) -> None:
         return
     import oracle
     make, kind, what = reference_engine()
-    cores = os.cpu_count() or 1
+    cores = usable_cpus() or 1
     size = args.size
     grid = oracle.random_ones_zeros(size, size, SEED)
     bands = np.array_split(np.arange(size), cores)
@@ -555,7 +564,7 @@ def bench_batched(stream, device, n: int = 512, seed: int = SEED) -> dict:
     work = golb200.workload_uneven(seed, n, 256, 4096, 64, (0.2, 0.5), (64, 4096))
     b = golb200.GolBatch(device=device, stream=stream.cuda_stream)
     inputs = []
-    with cf.ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as pool:
+    with cf.ThreadPoolExecutor(max_workers=min(32, usable_cpus() or 1)) as pool:
         for i in range(0, n, 32):
             chunk = work[i:i + 32]
             grids = list(pool.map(lambda d: golb200.load_bernoulli(d["x"], d["y"], d["cell_seed"],
@@ -588,7 +597,7 @@ def bench_batched(stream, device, n: int = 512, seed: int = SEED) -> dict:
         want = oracle.life_rows(inputs[i], d["x"], d["gens"], 64,
                                 threads=1 if inputs[i].size < (1 << 16) else 4)
         return bool(np.array_equal(results[i], want))
-    with cf.ThreadPoolExecutor(max_workers=max(1, (os.cpu_count() or 2) // 2)) as pool:
+    with cf.ThreadPoolExecutor(max_workers=max(1, (usable_cpus() or 2) // 2)) as pool:
         ok = list(pool.map(check, range(n)))
     cu = info["cell_updates"]
     vb = cu / (min(batched) * 1e-3) / 1e9
@@ -625,7 +634,7 @@ def _check_serving_samples(samples) -> dict:
                                 threads=1 if d["x"] * d["y"] < (1 << 21) else 8)
         got = out if out.dtype == np.uint32 else oracle.pack_rows(out, 32)
         return bool(np.array_equal(got.view(np.uint32), want))
-    with cf.ThreadPoolExecutor(max_workers=max(1, (os.cpu_count() or 2) // 2)) as pool:
+    with cf.ThreadPoolExecutor(max_workers=max(1, (usable_cpus() or 2) // 2)) as pool:
         ok = list(pool.map(one, samples))
     return {"sampled": len(ok), "all_equal_oracle": all(ok)}
 
@@ -647,7 +656,7 @@ def bench_batched_settling(stream, device, n: int = 512, seed: int = SEED) -> di
         slots = (d["x"] // 64) * (d["y"] // 64)
         return golb200.load_sparse_patches(d["x"], d["y"], d["cell_seed"], 64,
                                            max(0.05, 1.0 / slots + 1e-9), 0.35)
-    with cf.ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as pool:
+    with cf.ThreadPoolExecutor(max_workers=min(32, usable_cpus() or 1)) as pool:
         inputs = list(pool.map(lambda d: oracle.pack_rows(cells_of(d), 64), work))
     out = {"workload": f"{n} grids as the batched workload (seed {seed}), dead with Bernoulli(0.35) "
                        "patches in 5 % of 64x64 slots (at least one)", "unit": UNIT}
@@ -686,7 +695,7 @@ def bench_batched_settling(stream, device, n: int = 512, seed: int = SEED) -> di
         want = oracle.life_rows(inputs[i], d["x"], d["gens"], 64,
                                 threads=1 if inputs[i].size < (1 << 16) else 4)
         return all(bool(np.array_equal(results[m][i], want)) for m in results)
-    with cf.ThreadPoolExecutor(max_workers=max(1, (os.cpu_count() or 2) // 2)) as pool:
+    with cf.ThreadPoolExecutor(max_workers=max(1, (usable_cpus() or 2) // 2)) as pool:
         ok = list(pool.map(check, range(n)))
     out["all_equal_oracle"] = all(ok)
     return out

@@ -74,7 +74,7 @@ typedef struct gol_config {
     uint64_t x, y;                  /* grid_dimensions (cells)                   */
     uint32_t word_bits;             /* 32 or 64 (state width of the layout)      */
     uint32_t temporal_steps;        /* k generations per pass (0 = auto)         */
-    uint32_t thread_block_size;     /* rows per CTA band (0 = auto)              */
+    uint32_t thread_block_size;     /* rows per band (0 = auto; k = 1: per thread) */
     uint32_t tile_rows;             /* change-tracking tile height (0 = auto)    */
     uint64_t max_runtime_seconds;   /* 0 = unlimited                             */
     int32_t device;                 /* CUDA device ordinal                       */
@@ -252,8 +252,10 @@ int gol_local_stats(gol_engine* e, uint64_t* passes, uint64_t* tiles_per_pass,
 /* --- Stateless device entry points -------------------------------------- */
 
 /* One pass of k generations, d_src -> d_dst (device row grids, x/32 words
- * per row, 16-byte aligned, must not overlap). k in 1..16. band_rows = 0
- * picks a default. Asynchronous on `stream`. */
+ * per row, 16-byte aligned, must not overlap). k in 1..16. k = 1 runs the
+ * HBM-streaming one-generation kernel (band_rows: rows each thread walks),
+ * k >= 2 the K-stage row-band kernel (band_rows: output rows per CTA);
+ * band_rows = 0 picks a default. Asynchronous on `stream`. */
 int gol_rows_pass(const void* d_src, void* d_dst, uint64_t x, uint64_t y, uint32_t k,
                   uint32_t band_rows, void* stream);
 /* Same with the lane width forced (lane_words 1, 2 or 4; 0 = auto). */

@@ -1,3 +1,4 @@
+#define _GNU_SOURCE
 /*
  * ORACLE — test infrastructure, not product code.
  *
@@ -45,6 +46,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <pthread.h>
+#include <sched.h>
 #include <unistd.h>
 
 /* ---------------------------------------------------------------------- */
@@ -388,7 +390,14 @@ static void* gor_job_run(void* arg) {
     return NULL;
 }
 
+/* Threads this process may run on: its CPU affinity (a container may allow
+ * fewer CPUs than the machine has online). */
 int gor_max_threads(void) {
+    cpu_set_t set;
+    if (sched_getaffinity(0, sizeof(set), &set) == 0) {
+        const int n = CPU_COUNT(&set);
+        if (n > 0) return n;
+    }
     long n = sysconf(_SC_NPROCESSORS_ONLN);
     return n > 0 ? (int)n : 1;
 }

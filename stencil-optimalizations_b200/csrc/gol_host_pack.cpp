@@ -9,6 +9,7 @@
 // byte-to-bit multiply gather); unpacking expands eight cells per 64-bit
 // multiply and streams them out (it is bound by the memory writes); rows
 // are split across hardware threads.
+#include <sched.h>
 #include <unistd.h>
 
 #include <algorithm>
@@ -31,6 +32,18 @@
 #endif
 
 namespace golb200 {
+
+// Threads this process may run on: its CPU affinity (a container may allow
+// fewer CPUs than the machine has).
+unsigned usable_cpus() {
+    cpu_set_t set;
+    if (sched_getaffinity(0, sizeof(set), &set) == 0) {
+        const int n = CPU_COUNT(&set);
+        if (n > 0) return (unsigned)n;
+    }
+    const unsigned hw = std::thread::hardware_concurrency();
+    return hw ? hw : 1;
+}
 
 namespace {
 
@@ -93,7 +106,7 @@ class RowPool {
 
   private:
     RowPool() : pid_(getpid()) {
-        const unsigned hw = std::thread::hardware_concurrency();
+        const unsigned hw = usable_cpus();
         const size_t n = std::min<size_t>(hw > 1 ? hw - 1 : 0, 63);
         for (size_t i = 0; i < n; ++i) threads_.emplace_back([this] { loop(); });
         for (auto& t : threads_) t.detach();
@@ -120,8 +133,8 @@ class RowPool {
 template <typename F>
 void parallel_rows(size_t y, size_t bytes_per_row, F&& body) {
     const size_t total = y * bytes_per_row;
-    unsigned hw = std::thread::hardware_concurrency();
-    size_t nt = std::max<size_t>(1, std::min<size_t>(hw ? hw : 1, 64));
+    const unsigned hw = usable_cpus();
+    size_t nt = std::max<size_t>(1, std::min<size_t>(hw, 64));
     // One thread per 256 KiB: below that handing out the work costs more
     // than it saves.
     nt = std::min(nt, std::max<size_t>(1, total >> 18));

@@ -205,6 +205,9 @@ int host_sparse_patches(uint8_t* cells, size_t x, size_t y, uint64_t seed, size_
 
 int device_sm_count(int device);
 
+// Host threads this process may run on (its CPU affinity).
+unsigned usable_cpus();
+
 // Measured LOP3 throughput of the device (32-bit lane-ops per second).
 cudaError_t probe_lop3_rate(int device, cudaStream_t stream, double* lane_ops_per_s);
 

@@ -73,7 +73,7 @@ inline void set_word(void* w, uint32_t wb, size_t i, uint64_t v) {
 // Runs body(r0, r1) over word rows [0, n) split across host threads.
 template <typename F>
 void parallel_word_rows(size_t n, size_t cells_per_row, F&& body) {
-    unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    unsigned hw = std::max(1u, usable_cpus());
     size_t nt = std::min<size_t>(hw, std::max<size_t>(1, n * cells_per_row / (1u << 20)));
     nt = std::min(nt, n ? n : 1);
     if (nt <= 1) {

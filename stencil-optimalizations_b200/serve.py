@@ -32,6 +32,14 @@ import numpy as np  # noqa: E402
 import golb200  # noqa: E402
 
 
+def usable_cpus() -> int:
+    """Host threads this process may run on (its CPU affinity)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
 def run_stream(rate: float = 2000.0, seconds: float = 2.0, seed: int = 42, min_side: int = 128,
                max_side: int = 8192, density=(0.1, 0.5), gens=(16, 8192), quantum: int = 128,
                arena_bytes: int = 0, device: int = 0, fetch: str = "words",
@@ -61,7 +69,7 @@ def run_stream(rate: float = 2000.0, seconds: float = 2.0, seed: int = 42, min_s
     srv.set_tracking(tracking)
     host_cells = []
     if host_io:
-        with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as pool:
+        with ThreadPoolExecutor(max_workers=usable_cpus() or 1) as pool:
             host_cells = list(pool.map(
                 lambda j: golb200.load_hash_bernoulli(work[j]["x"], work[j]["y"], work[j]["cell_seed"],
                                                       work[j]["density"]), keep))

@@ -19,9 +19,16 @@ import pytest
 import golb200
 import oracle
 
-pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+pytestmark = [pytest.mark.gpu, pytest.mark.slow, pytest.mark.timeout(900)]
 
 GENS = 4096
+
+
+def usable_cpus() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
 
 
 def engine_words(cells, gens, word_bits, **kw):
@@ -70,7 +77,7 @@ def test_batched_workload_every_grid():
         b.run()
         b.sync()
         got = [oracle.pack_rows(b.fetch(i), 64) for i in range(len(work))]
-    workers = max(1, (os.cpu_count() or 1) // 2)
+    workers = max(1, (usable_cpus() or 1) // 2)
     with ThreadPoolExecutor(max_workers=workers) as pool:
         want = list(pool.map(lambda i: oracle_grid(inputs[i], work[i]["x"], work[i]["gens"]),
                              range(len(work))))
@@ -95,7 +102,7 @@ def test_serving_stream_sampled_requests():
         want = oracle.life_rows(oracle.pack_rows(cells, 32), d["x"], d["gens"], 32,
                                 threads=1 if d["x"] * d["y"] < (1 << 21) else 8)
         return bool(np.array_equal(oracle.pack_rows(out, 32), want))
-    workers = max(1, (os.cpu_count() or 2) // 2)
+    workers = max(1, (usable_cpus() or 2) // 2)
     with ThreadPoolExecutor(max_workers=workers) as pool:
         ok = list(pool.map(one, samples))
     assert all(ok), [i for i, v in enumerate(ok) if not v][:10]
