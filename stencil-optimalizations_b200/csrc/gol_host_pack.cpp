@@ -156,13 +156,16 @@ void parallel_rows(size_t y, size_t bytes_per_row, F&& body) {
         for (auto& th : ts) th.join();
         return;
     }
+    // The count of outstanding ranges is set before the first is handed
+    // out: workers decrement it (under mu) while later ranges are still
+    // being submitted.
+    size_t tasks = 0;
+    for (size_t t = 1; t < nt && t * per < y; ++t) ++tasks;
     std::mutex mu;
     std::condition_variable cv;
-    size_t left = 0;
-    for (size_t t = 1; t < nt; ++t) {
+    size_t left = tasks;
+    for (size_t t = 1; t <= tasks; ++t) {
         const size_t y0 = t * per, y1 = std::min(y, y0 + per);
-        if (y0 >= y1) break;
-        ++left;
         pool.submit([&, y0, y1] {
             body(y0, y1);
             std::lock_guard<std::mutex> lk(mu);
