@@ -950,6 +950,8 @@ def run_ours(args, d: Dist) -> None:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "dtype_note": "the kernels compute on 32-bit words; the 64-bit-row layout is the same "
+                          "bytes on the device",
             "data": "synthetic",
             "config": {
                 "workload": f"dense {size}x{size} Bernoulli(0.5) seed {SEED}, 64-bit rows, "
