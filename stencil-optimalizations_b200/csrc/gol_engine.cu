@@ -24,8 +24,6 @@ thread_local std::string g_create_error;
 // Passes per captured CUDA graph (even, so a chunk ends on the same buffer
 // parity it started from and one executable graph per parity suffices).
 constexpr int kGraphPasses = 16;
-// Row chunks of the host-device copies (see gol_engine::uploaded).
-constexpr int kCopyChunks = 8;
 
 } // namespace
 
@@ -48,15 +46,6 @@ struct gol_engine {
     bool own_stream = false;
     cudaStream_t capture_stream = nullptr;
     cudaGraphExec_t chunk[2] = {nullptr, nullptr};
-
-    // Host-device copies in row chunks, overlapped with the host packing
-    // and unpacking: set_input copies each packed chunk as soon as it is
-    // packed (when the device grids exist from an earlier round), finalize
-    // queues the result's chunks with an event each and fetch unpacks each
-    // chunk once its copy is done.
-    bool uploaded = false;                 // set_input already copied the grid to d[0]
-    cudaEvent_t d2h_done[kCopyChunks] = {};
-    bool d2h_pending = false;
 
     int k = 1;
     RowsPlan plan{};
@@ -183,65 +172,6 @@ int ensure_host(gol_engine* e) {
     }
     e->h_words = static_cast<uint32_t*>(p);
     e->h_bytes = bytes;
-    return GOL_OK;
-}
-
-// Waits for the result copies finalize queued (before h_words is reused).
-int wait_d2h(gol_engine* e) {
-    if (!e->d2h_pending) return GOL_OK;
-    e->d2h_pending = false;
-    cudaError_t ce = cudaSuccess;
-    for (auto ev : e->d2h_done)
-        if (ev && ce == cudaSuccess) ce = cudaEventSynchronize(ev);
-    return ce == cudaSuccess ? GOL_OK : e->cuda_fail(ce, "D2H copy");
-}
-
-int rows_per_chunk(const gol_engine* e) { return (e->Y + kCopyChunks - 1) / kCopyChunks; }
-
-// Packs the input into h_words (pack(row0, rows, words) packs that many
-// rows). When the device grids exist from an earlier round and h_words is
-// pinned, each chunk of rows is copied to d[0] as soon as it is packed, so
-// the copy overlaps the packing of the next chunk, and gol_init skips its
-// copy.
-template <typename Pack>
-int pack_input(gol_engine* e, Pack pack) {
-    int rc = wait_d2h(e);
-    if (rc) return rc;
-    e->uploaded = false;
-    const bool copy = e->d[0] && e->h_pinned && e->stream && e->W > 0 && e->Y > 0;
-    if (!copy) {
-        pack(0, e->Y, e->h_words);
-        return GOL_OK;
-    }
-    cudaError_t ce = cudaSetDevice(e->cfg.device);
-    const int per = rows_per_chunk(e);
-    for (int r0 = 0; r0 < e->Y && ce == cudaSuccess; r0 += per) {
-        const int rows = std::min(per, e->Y - r0);
-        uint32_t* h = e->h_words + (size_t)r0 * e->W;
-        pack(r0, rows, h);
-        ce = cudaMemcpyAsync(e->d[0] + (size_t)r0 * e->W, h, (size_t)rows * e->W * sizeof(uint32_t),
-                             cudaMemcpyHostToDevice, e->stream);
-    }
-    if (ce != cudaSuccess) return e->cuda_fail(ce, "H2D copy");
-    e->uploaded = true;
-    return GOL_OK;
-}
-
-// Unpacks h_words row chunk by row chunk, each once its copy has landed.
-template <typename Unpack>
-int unpack_result(gol_engine* e, Unpack unpack) {
-    if (!e->d2h_pending) {
-        unpack(0, e->Y);
-        return GOL_OK;
-    }
-    e->d2h_pending = false;
-    const int per = std::max(1, rows_per_chunk(e));
-    for (int c = 0; c < kCopyChunks; ++c) {
-        cudaError_t ce = cudaEventSynchronize(e->d2h_done[c]);
-        if (ce != cudaSuccess) return e->cuda_fail(ce, "D2H copy");
-        const int r0 = std::min(c * per, e->Y), rows = std::max(0, std::min(per, e->Y - r0));
-        if (rows > 0) unpack(r0, rows);
-    }
     return GOL_OK;
 }
 
@@ -386,10 +316,7 @@ int gol_set_input_u8(gol_engine* e, const uint8_t* cells, uint64_t x, uint64_t y
     int rc = check_shape(e, x, y);
     if (rc) return rc;
     if ((rc = ensure_host(e))) return rc;
-    if ((rc = pack_input(e, [&](int r0, int rows, uint32_t* w) {
-             golb200::host_pack_u8(cells + (size_t)r0 * x, x, (size_t)rows, w);
-         })))
-        return rc;
+    golb200::host_pack_u8(cells, x, y, e->h_words);
     e->has_host_grid = true;
     e->performed = 0;
     return GOL_OK;
@@ -402,10 +329,7 @@ int gol_set_input_i32(gol_engine* e, const int32_t* cells, uint64_t x, uint64_t 
     int rc = check_shape(e, x, y);
     if (rc) return rc;
     if ((rc = ensure_host(e))) return rc;
-    if ((rc = pack_input(e, [&](int r0, int rows, uint32_t* w) {
-             golb200::host_pack_i32(cells + (size_t)r0 * x, x, (size_t)rows, w);
-         })))
-        return rc;
+    golb200::host_pack_i32(cells, x, y, e->h_words);
     e->has_host_grid = true;
     e->performed = 0;
     return GOL_OK;
@@ -421,8 +345,6 @@ int gol_set_input_words(gol_engine* e, const void* words, uint64_t x, uint64_t y
     int rc = check_shape(e, x, y);
     if (rc) return rc;
     if ((rc = ensure_host(e))) return rc;
-    if ((rc = wait_d2h(e))) return rc;
-    e->uploaded = false;
     std::memcpy(e->h_words, words, e->h_bytes);   // same bytes for 32- and 64-bit rows
     e->has_host_grid = true;
     e->performed = 0;
@@ -439,8 +361,6 @@ int gol_set_input_layout(gol_engine* e, const void* words, int layout, uint32_t 
     if (e->initialized) return e->fail(GOL_E_STATE, "set_input while device data is live");
     int rc = ensure_host(e);
     if (rc) return rc;
-    if ((rc = wait_d2h(e))) return rc;
-    e->uploaded = false;
     golb200::host_layout_to_rows(words, e->x, e->y, layout, word_bits, xb, yb, e->h_words);
     e->has_host_grid = true;
     e->performed = 0;
@@ -495,9 +415,7 @@ int gol_init(gol_engine* e) {
         }
     }
     e->cur = 0;
-    if (!e->uploaded)
-        ce = cudaMemcpyAsync(e->d[0], e->h_words, bytes, cudaMemcpyHostToDevice, e->stream);
-    e->uploaded = false;
+    ce = cudaMemcpyAsync(e->d[0], e->h_words, bytes, cudaMemcpyHostToDevice, e->stream);
     if (ce != cudaSuccess) {
         release_device(e);
         return e->cuda_fail(ce, "H2D copy");
@@ -593,32 +511,17 @@ int gol_sync(gol_engine* e) {
     return GOL_OK;
 }
 
-// Queues the result's copy to the host in row chunks, an event after each,
-// and waits for the run and the first chunk (so a failure of the run is
-// reported here); the fetch calls wait for the rest, chunk by chunk.
 int gol_finalize(gol_engine* e) {
     if (!e) return GOL_E_INVALID;
     if (!e->initialized) return e->fail(GOL_E_STATE, "finalize before initialize");
-    cudaError_t ce = cudaSuccess;
-    for (auto& ev : e->d2h_done)
-        if (!ev && ce == cudaSuccess) ce = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
-    const int per = std::max(1, rows_per_chunk(e));
-    for (int c = 0; c < kCopyChunks && ce == cudaSuccess; ++c) {
-        const int r0 = std::min(c * per, e->Y), rows = std::max(0, std::min(per, e->Y - r0));
-        if (rows > 0)
-            ce = cudaMemcpyAsync(e->h_words + (size_t)r0 * e->W, e->d[e->cur] + (size_t)r0 * e->W,
-                                 (size_t)rows * e->W * sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                                 e->stream);
-        if (ce == cudaSuccess) ce = cudaEventRecord(e->d2h_done[c], e->stream);
-    }
-    if (ce == cudaSuccess) ce = cudaEventSynchronize(e->d2h_done[0]);
+    cudaError_t ce = cudaMemcpyAsync(e->h_words, e->d[e->cur], e->h_bytes, cudaMemcpyDeviceToHost,
+                                     e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
     e->initialized = false;
     if (ce != cudaSuccess) {
-        cudaStreamSynchronize(e->stream);
         release_device(e);
         return e->cuda_fail(ce, "D2H copy");
     }
-    e->d2h_pending = true;
     return GOL_OK;
 }
 
@@ -626,20 +529,16 @@ int gol_fetch_u8(gol_engine* e, uint8_t* cells) {
     if (!e) return GOL_E_INVALID;
     if (!e->has_host_grid || e->initialized) return e->fail(GOL_E_STATE, "fetch before finalize");
     if (!cells && e->x * e->y) return e->fail(GOL_E_INVALID, "null cells");
-    return unpack_result(e, [&](int r0, int rows) {
-        golb200::host_unpack_u8(e->h_words + (size_t)r0 * e->W, e->x, (size_t)rows,
-                                cells + (size_t)r0 * e->x);
-    });
+    golb200::host_unpack_u8(e->h_words, e->x, e->y, cells);
+    return GOL_OK;
 }
 
 int gol_fetch_i32(gol_engine* e, int32_t* cells) {
     if (!e) return GOL_E_INVALID;
     if (!e->has_host_grid || e->initialized) return e->fail(GOL_E_STATE, "fetch before finalize");
     if (!cells && e->x * e->y) return e->fail(GOL_E_INVALID, "null cells");
-    return unpack_result(e, [&](int r0, int rows) {
-        golb200::host_unpack_i32(e->h_words + (size_t)r0 * e->W, e->x, (size_t)rows,
-                                 cells + (size_t)r0 * e->x);
-    });
+    golb200::host_unpack_i32(e->h_words, e->x, e->y, cells);
+    return GOL_OK;
 }
 
 int gol_fetch_words(gol_engine* e, void* words, uint32_t word_bits) {
@@ -648,8 +547,6 @@ int gol_fetch_words(gol_engine* e, void* words, uint32_t word_bits) {
     if (e->x % word_bits) return e->fail(GOL_E_INVALID, "x must be a multiple of word_bits");
     if (!e->has_host_grid || e->initialized) return e->fail(GOL_E_STATE, "fetch before finalize");
     if (!words && e->h_bytes) return e->fail(GOL_E_INVALID, "null words");
-    int rc = wait_d2h(e);
-    if (rc) return rc;
     std::memcpy(words, e->h_words, e->h_bytes);
     return GOL_OK;
 }
@@ -662,8 +559,6 @@ int gol_fetch_layout(gol_engine* e, void* words, int layout, uint32_t word_bits)
     if (e->x % xb || e->y % yb) return e->fail(GOL_E_INVALID, "grid is not a whole number of layout words");
     if (!e->has_host_grid || e->initialized) return e->fail(GOL_E_STATE, "fetch before finalize");
     if (!words && e->h_bytes) return e->fail(GOL_E_INVALID, "null words");
-    int rc = wait_d2h(e);
-    if (rc) return rc;
     golb200::host_rows_to_layout(e->h_words, e->x, e->y, layout, word_bits, xb, yb, words);
     return GOL_OK;
 }
@@ -673,8 +568,6 @@ uint64_t gol_performed(const gol_engine* e) { return e ? e->performed : 0; }
 void gol_destroy(gol_engine* e) {
     if (!e) return;
     if (e->stream) cudaStreamSynchronize(e->stream);
-    for (auto& ev : e->d2h_done)
-        if (ev) cudaEventDestroy(ev);
     release_device(e);
     release_host(e);
     if (e->capture_stream) cudaStreamDestroy(e->capture_stream);
