@@ -163,6 +163,21 @@ __device__ __forceinline__ uint32_t seg_dispatch(int k, const BatchGrid& G, int 
     }
 }
 
+// Loads a descriptor field anew after an item's pipeline (an opaque load
+// the compiler cannot merge with the one before it), so the tracking fields
+// are not held in registers through the pipeline.
+template <typename T>
+__device__ __forceinline__ T* ld_ptr_again(T* const* p) {
+    unsigned long long v;
+    asm volatile("ld.global.nc.u64 %0, [%1];" : "=l"(v) : "l"(p));
+    return reinterpret_cast<T*>(v);
+}
+__device__ __forceinline__ int ld_int_again(const int* p) {
+    int v;
+    asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
 __device__ __forceinline__ void release_max(int* p, int v) {
     // Monotone release: an item of a still grid may finish before the item
     // of the previous pass on the same counter (it does not wait for it).
@@ -304,27 +319,30 @@ batch_kernel(const BatchGrid* __restrict__ grids, const BatchItem* __restrict__ 
             }
             changed = TRACK && __any_sync(0xffffffffu, diff != 0u);
         }
-        if (TRACK && G.trk && lane == 0)   // this pass's flag, read by the next pass
-            *(volatile uint32_t*)(G.trk + (odd ? nper : 0) + cell) =
-                (changed || k != G.k) ? 1u : 0u;
+        const BatchGrid* gp = grids + it.grid;
+        uint32_t* trk = TRACK ? ld_ptr_again(&gp->trk) : nullptr;
+        if (TRACK && trk && lane == 0)   // this pass's flag, read by the next pass
+            *(volatile uint32_t*)(trk + (odd ? nper : 0) + cell) = (changed || k != G.k) ? 1u : 0u;
         __threadfence();
         __syncwarp();
         if (lane == 0) {
-            if (TRACK && G.trk)
+            if (TRACK && trk)
                 release_max(mine, it.pass + 1);
             else
                 st_release(mine, it.pass + 1);
-            atomicAdd(G.gstat + (compute ? 0 : 1), 1u);
-            if (TRACK && G.trk) {
+            atomicAdd(ld_ptr_again(&gp->gstat) + (compute ? 0 : 1), 1u);
+            if (TRACK && trk) {
                 // Last item of this pass: if none changed, the grid is still
                 // from the next pass on.
-                if (changed || k != G.k) atomicAdd(G.pstat + 2 * it.pass + 1, 1);
+                int* pstat = ld_ptr_again(&gp->pstat);
+                if (changed || k != G.k) atomicAdd(pstat + 2 * it.pass + 1, 1);
                 __threadfence();
-                if (atomicAdd(G.pstat + 2 * it.pass, 1) == nper - 1) {
+                if (atomicAdd(pstat + 2 * it.pass, 1) == nper - 1) {
                     __threadfence();
-                    if (atomicAdd(G.pstat + 2 * it.pass + 1, 0) == 0) {
-                        atomicMin(G.trk + 2 * nper, (unsigned)(G.pass0 + it.pass + 1));
-                        if (G.rflag) *(volatile int*)G.rflag = 1;
+                    if (atomicAdd(pstat + 2 * it.pass + 1, 0) == 0) {
+                        atomicMin(trk + 2 * nper, (unsigned)(ld_int_again(&gp->pass0) + it.pass + 1));
+                        int* rflag = ld_ptr_again(&gp->rflag);
+                        if (rflag) *(volatile int*)rflag = 1;
                     }
                 }
             }
