@@ -63,7 +63,11 @@ enum gol_status {
 enum gol_algorithm {
     GOL_ALG_AUTO = 0,        /* temporal rows, depth picked by the engine       */
     GOL_ALG_ROWS = 1,        /* temporal rows with temporal_steps = k           */
-    GOL_ALG_LOCAL = 2        /* change-tracking tiles (skips stable tiles)      */
+    GOL_ALG_LOCAL = 2,       /* change-tracking tiles (skips stable tiles)      */
+    GOL_ALG_RESIDENT = 3     /* the whole run in one cooperative launch, bands
+                                kept in shared memory (grids that fit in the
+                                SMs' shared memory, e.g. 8192 x 8192); the run
+                                budget is checked only before the launch      */
 };
 
 /* Mirrors the ExperimentParams fields the hot path reads

@@ -50,6 +50,12 @@ struct gol_engine {
     int k = 1;
     RowsPlan plan{};
 
+    // shared-memory-resident run (GOL_ALG_RESIDENT)
+    bool resident = false;
+    golb200::ResidentPlan rplan{};
+    uint32_t* r_pub = nullptr;
+    int* r_ints = nullptr;                 // epoch counters, then the status word
+
     // change tracking (GOL_ALG_LOCAL)
     bool local = false;
     golb200::LocalPlan lplan{};
@@ -99,6 +105,10 @@ void release_local(gol_engine* e) {
 void release_device(gol_engine* e) {
     release_graphs(e);
     release_local(e);
+    if (e->r_pub) cudaFree(e->r_pub);
+    if (e->r_ints) cudaFree(e->r_ints);
+    e->r_pub = nullptr;
+    e->r_ints = nullptr;
     for (auto& p : e->d) {
         if (p) cudaFree(p);
         p = nullptr;
@@ -291,7 +301,7 @@ int gol_create(gol_engine** out, const gol_config* cfg) {
         g_create_error = "lane_words must be 0, 1, 2 or 4";
         return GOL_E_INVALID;
     }
-    if (cfg->algorithm > GOL_ALG_LOCAL) {
+    if (cfg->algorithm > GOL_ALG_RESIDENT) {
         g_create_error = "unknown algorithm";
         return GOL_E_INVALID;
     }
@@ -394,6 +404,11 @@ int gol_init(gol_engine* e) {
                             (int)e->cfg.lane_words, sms, &e->plan))
         return e->fail(GOL_E_UNSUPPORTED, "no kernel plan for this width and depth");
     e->local = e->cfg.algorithm == GOL_ALG_LOCAL;
+    e->resident = e->cfg.algorithm == GOL_ALG_RESIDENT;
+    if (e->resident &&
+        !golb200::plan_resident(e->W, e->Y, (int)e->cfg.temporal_steps, e->cfg.device, &e->rplan))
+        return e->fail(GOL_E_UNSUPPORTED,
+                       "grid does not fit in the SMs' shared memory for a resident run");
     if (e->local && !golb200::plan_local_tiles(e->W, e->Y, k, (int)e->cfg.tile_rows,
                                                (int)e->cfg.lane_words, sms,
                                                (int)std::min<uint32_t>(e->cfg.dense_pct, 101u),
@@ -424,6 +439,14 @@ int gol_init(gol_engine* e) {
         int rc = alloc_local(e);
         if (rc) return rc;
     }
+    if (e->resident && !e->r_pub) {
+        ce = cudaMalloc(&e->r_pub, std::max<size_t>(e->rplan.pub_words, 1) * sizeof(uint32_t));
+        if (ce == cudaSuccess) ce = cudaMalloc(&e->r_ints, (e->rplan.nbands + 1) * sizeof(int));
+        if (ce != cudaSuccess) {
+            release_device(e);
+            return e->cuda_fail(ce, "resident-run scratch");
+        }
+    }
     e->initialized = true;
     e->performed = 0;
     return GOL_OK;
@@ -444,6 +467,16 @@ int gol_run(gol_engine* e, uint64_t n) {
         auto s = std::chrono::duration_cast<std::chrono::seconds>(std::chrono::steady_clock::now() - t0);
         return (uint64_t)s.count() >= budget;
     };
+    if (e->resident) {   // every generation in one cooperative launch
+        if (time_is_up()) return GOL_OK;
+        cudaError_t ce = golb200::launch_resident(e->d[e->cur], e->d[e->cur ^ 1], e->W, e->Y,
+                                                  (long long)n, e->rplan, e->r_pub, e->r_ints,
+                                                  e->r_ints + e->rplan.nbands, e->stream);
+        if (ce != cudaSuccess) return e->cuda_fail(ce, "resident run launch");
+        e->cur ^= 1;
+        e->performed = n;
+        return GOL_OK;
+    }
     const int k = e->k;
     uint64_t passes = n / (uint64_t)k;
     const int rem = (int)(n % (uint64_t)k);
@@ -503,12 +536,22 @@ int gol_run(gol_engine* e, uint64_t n) {
     return GOL_OK;
 }
 
+// A resident run records GOL_E_TIMEOUT in its status word when a CTA gave
+// up waiting for a neighbour (bounded polls); reported after a sync.
+static int resident_status(gol_engine* e) {
+    if (!e->resident || !e->r_ints) return GOL_OK;
+    int st = 0;
+    cudaError_t ce = cudaMemcpy(&st, e->r_ints + e->rplan.nbands, sizeof(int), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "resident status");
+    return st ? e->fail(st, "a resident-run CTA gave up waiting for a neighbour") : GOL_OK;
+}
+
 int gol_sync(gol_engine* e) {
     if (!e) return GOL_E_INVALID;
     if (!e->stream) return GOL_OK;
     cudaError_t ce = cudaStreamSynchronize(e->stream);
     if (ce != cudaSuccess) return e->cuda_fail(ce, "stream synchronize");
-    return GOL_OK;
+    return resident_status(e);
 }
 
 int gol_finalize(gol_engine* e) {
@@ -522,7 +565,7 @@ int gol_finalize(gol_engine* e) {
         release_device(e);
         return e->cuda_fail(ce, "D2H copy");
     }
-    return GOL_OK;
+    return resident_status(e);
 }
 
 int gol_fetch_u8(gol_engine* e, uint8_t* cells) {

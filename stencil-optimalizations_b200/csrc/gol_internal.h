@@ -34,6 +34,25 @@ struct RowsPlan {
 bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPlan* plan,
                bool allow_stream = true);
 
+// Shared-memory-resident run (gol_rows_resident.cuh): every generation of
+// a grid whose bands fit in the SMs' shared memory, in one cooperative
+// launch of one CTA per band.
+struct ResidentPlan {
+    int wpl = 0, lanes = 0, groups = 0;   // lanes of wpl words across a row, row groups
+    int K = 0;                            // generations per epoch (halo rows)
+    int band = 0, nbands = 0;             // largest band, CTAs
+    size_t smem = 0;                      // dynamic shared memory per CTA
+    size_t pub_words = 0;                 // words of the publication slots
+};
+// False when the grid does not fit (or k_epoch is out of range). k_epoch = 0
+// picks the default.
+bool plan_resident(int W, int Y, int k_epoch, int device, ResidentPlan* p);
+// gens generations src -> dst. pub (p.pub_words), epoch_done (p.nbands ints)
+// and status are device scratch; epoch_done and status are cleared here.
+cudaError_t launch_resident(const uint32_t* src, uint32_t* dst, int W, int Y, long long gens,
+                            const ResidentPlan& p, uint32_t* pub, int* epoch_done, int* status,
+                            cudaStream_t stream, long long spin_limit = 0);
+
 // One pass of k generations (1 <= k <= kMaxKForWpl(plan.wpl)). pitch: words
 // from one row to the next (0 = W).
 cudaError_t launch_rows_pass(const uint32_t* src, uint32_t* dst, int W, int Y, int k,

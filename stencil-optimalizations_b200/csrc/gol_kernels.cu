@@ -2,7 +2,9 @@
 // kernel, plus device-side pack/unpack between uint8 cells and row words.
 #include <algorithm>
 
+#include "gol_b200.h"
 #include "gol_internal.h"
+#include "gol_rows_resident.cuh"
 #include "gol_rows_stream.cuh"
 #include "gol_rows_temporal.cuh"
 #include "gol_word_ops.cuh"
@@ -152,6 +154,75 @@ bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPla
     plan->band = band;
     plan->nbands = (Y + band - 1) / band;
     return true;
+}
+
+#ifndef GOL_RESIDENT_K
+#define GOL_RESIDENT_K 8   // generations per epoch of the resident run
+#endif
+#ifndef GOL_RESIDENT_WPL
+#define GOL_RESIDENT_WPL 2
+#endif
+#ifndef GOL_RESIDENT_THREADS
+#define GOL_RESIDENT_THREADS 512   // threads per CTA (lanes across a row x row groups)
+#endif
+
+bool plan_resident(int W, int Y, int k_epoch, int device, ResidentPlan* p) {
+    const int K = k_epoch > 0 ? k_epoch : GOL_RESIDENT_K;
+    if (K < 1 || K > 64 || W <= 0 || Y <= 0) return false;
+    int wpl = GOL_RESIDENT_WPL;
+    while (wpl > 1 && W % wpl) wpl /= 2;
+    const int lanes = ((W + wpl - 1) / wpl + 31) / 32 * 32;
+    if (lanes > kResidentMaxThreads) return false;
+    const int groups = std::max(1, std::min(GOL_RESIDENT_THREADS, kResidentMaxThreads) / lanes);
+    int sms = 0, smem_max = 0, coop = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess || !coop)
+        return false;
+    // Every band at least K rows (a band's halo comes from its neighbours
+    // only), at most one CTA per SM; the largest band's two buffers must fit.
+    const int nbands = std::min(sms, Y / K);
+    if (nbands < 1) return false;
+    const int band = (Y + nbands - 1) / nbands;
+    const size_t smem = resident_smem_bytes(band, K, lanes, wpl);
+    if (smem + 1024 > (size_t)smem_max) return false;
+    p->wpl = wpl;
+    p->lanes = lanes;
+    p->groups = groups;
+    p->K = K;
+    p->band = band;
+    p->nbands = nbands;
+    p->smem = smem;
+    p->pub_words = (size_t)nbands * 4 * K * W;
+    return true;
+}
+
+template <int WPL>
+static cudaError_t launch_resident_wpl(const ResidentLaunch& a, const ResidentPlan& p,
+                                       cudaStream_t stream) {
+    cudaError_t e = cudaFuncSetAttribute(rows_resident_kernel<WPL>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+    if (e != cudaSuccess) return e;
+    ResidentLaunch arg = a;
+    void* args[] = {&arg};
+    return cudaLaunchCooperativeKernel((const void*)rows_resident_kernel<WPL>, dim3(p.nbands),
+                                       dim3(p.lanes * p.groups), args, p.smem, stream);
+}
+
+cudaError_t launch_resident(const uint32_t* src, uint32_t* dst, int W, int Y, long long gens,
+                            const ResidentPlan& p, uint32_t* pub, int* epoch_done, int* status,
+                            cudaStream_t stream, long long spin_limit) {
+    cudaError_t e = cudaMemsetAsync(epoch_done, 0, (size_t)p.nbands * sizeof(int), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, sizeof(int), stream);
+    if (e != cudaSuccess) return e;
+    ResidentLaunch a{src, dst, pub, epoch_done, status, W, Y, p.band, p.K, p.lanes, p.groups, gens,
+                     spin_limit > 0 ? spin_limit : (1ll << 24)};
+    switch (p.wpl) {
+        case 4: return launch_resident_wpl<4>(a, p, stream);
+        case 2: return launch_resident_wpl<2>(a, p, stream);
+        case 1: return launch_resident_wpl<1>(a, p, stream);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_rows_pass(const uint32_t* src, uint32_t* dst, int W, int Y, int k,

@@ -47,7 +47,7 @@ def layout_block(layout: str, word_bits: int) -> tuple:
         return {16: (4, 4), 32: (8, 4), 64: (8, 8)}[word_bits]
     raise ValueError(f"unknown layout {layout!r}")
 
-ALGORITHMS = {"auto": 0, "rows": 1, "local": 2}
+ALGORITHMS = {"auto": 0, "rows": 1, "local": 2, "resident": 3}
 
 
 class GolConfig(ctypes.Structure):

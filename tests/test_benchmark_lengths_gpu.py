@@ -42,13 +42,14 @@ def engine_words(cells, gens, word_bits, **kw):
         return alg.fetch_words(word_bits)
 
 
-@pytest.mark.parametrize("size,word_bits,k", [(16384, 64, 4), (16384, 64, 8), (8192, 32, 0),
-                                              (8192, 32, 8)])
-def test_dense_configs_at_full_length(size, word_bits, k):
+@pytest.mark.parametrize("size,word_bits,k,alg", [(16384, 64, 4, "auto"), (16384, 64, 8, "auto"),
+                                                  (8192, 32, 0, "auto"), (8192, 32, 8, "auto"),
+                                                  (8192, 32, 0, "resident")])
+def test_dense_configs_at_full_length(size, word_bits, k, alg):
     cells = oracle.random_ones_zeros(size, size, 42)
-    got = engine_words(cells, GENS, word_bits, temporal_steps=k)
+    got = engine_words(cells, GENS, word_bits, temporal_steps=k, algorithm=alg)
     want = oracle.life_rows(oracle.pack_rows(cells, word_bits), size, GENS, word_bits)
-    assert np.array_equal(got, want), (size, word_bits, k)
+    assert np.array_equal(got, want), (size, word_bits, k, alg)
 
 
 def test_sparse_change_tracking_at_full_length():

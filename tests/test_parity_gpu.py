@@ -108,6 +108,36 @@ def test_streaming_kernel_stateless_pass():
         assert np.array_equal(got, oracle.pack_rows(oracle.life_cells(g, 9), 32)), (x, y, wpl)
 
 
+@pytest.mark.parametrize("x,y,gens,k", [(8192, 8192, 300, 0), (4096, 1000, 77, 8), (96, 40, 33, 4),
+                                         (32 * 37, 300, 100, 5), (2048, 64, 0, 8), (1024, 500, 1, 8),
+                                         (64, 148 * 9 + 5, 50, 3), (32 * 255, 700, 64, 16)])
+def test_resident_run(x, y, gens, k):
+    """GOL_ALG_RESIDENT: the whole run in one cooperative launch, each CTA's
+    band in shared memory, halos exchanged every k generations; odd widths
+    (one word per lane), bands of unequal height, generation counts that k
+    does not divide, zero and one generation."""
+    g = oracle.random_ones_zeros(x, y, x + y + gens)
+    out = run_engine(g, gens, k=k, word_bits=32, algorithm="resident")
+    assert np.array_equal(out, oracle.life_cells(g, gens)), (x, y, gens, k)
+
+
+def test_resident_run_reused_and_rejected_when_too_large():
+    g = oracle.random_ones_zeros(2048, 2048, 5)
+    ref = oracle.life_cells(g, 40)
+    with golb200.GolB200(grid_dimensions=(2048, 2048), algorithm="resident") as alg:
+        for _ in range(2):
+            alg.set_and_format_input_data(g)
+            alg.initialize_data_structures()
+            alg.run(40)
+            alg.finalize_data_structures()
+            assert np.array_equal(alg.fetch_result(), ref)
+    # 16384^2 is 32 MiB of cells: more than the SMs' shared memory holds
+    with golb200.GolB200(grid_dimensions=(16384, 16384), algorithm="resident") as alg:
+        alg.set_and_format_input_data(np.zeros((16384, 16384), np.uint8))
+        with pytest.raises(RuntimeError, match="shared memory"):
+            alg.initialize_data_structures()
+
+
 def test_word_bits_32_and_64_agree():
     g = oracle.random_ones_zeros(512, 100, 77)
     a = run_engine(g, 37, word_bits=32)
