@@ -157,7 +157,7 @@ bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPla
 }
 
 #ifndef GOL_RESIDENT_K
-#define GOL_RESIDENT_K 8   // generations per epoch of the resident run
+#define GOL_RESIDENT_K 6   // generations per epoch of the resident run
 #endif
 #ifndef GOL_RESIDENT_WPL
 #define GOL_RESIDENT_WPL 2

@@ -6,20 +6,33 @@
 // CTA c keeps rows [y0, y1) of the grid (its band) in two shared-memory
 // buffers and advances them K generations per epoch. An epoch needs K rows
 // above and K below the band (cells within K of the band's edge depend on
-// them): at the start of every epoch each CTA publishes its top and bottom K
-// rows to global memory, releases an epoch counter, waits for its two
-// neighbours' counters (bounded polls: GOL_E_TIMEOUT in *status and the CTA
-// stops), and copies their rows into its halo. Generation g of the epoch
-// computes the rows still covered by valid neighbours (the band plus K - g
-// rows each side), rows outside the grid stay dead. The publication slots
-// alternate by epoch parity: a CTA rewrites a slot only after both
-// neighbours have published the next epoch, i.e. after they read it.
+// them), which the neighbouring CTAs publish through global memory.
 //
-// Within a generation a thread owns WPL words of a column and walks a range
-// of rows (the CTA's threads are lanes across the row times row groups),
-// keeping the horizontal sums of three rows in registers like the streaming
-// kernel; words beyond its lane come from its warp neighbours by shuffle or
-// from shared memory at the warp's edges. One barrier per generation.
+// The exchange is overlapped with the band's interior. The first ni
+// generations of an epoch (ni = kResidentInterior, at most K) are first
+// computed on the rows at least g away from the band's edges (they depend on
+// the band only) while the neighbours' rows arrive. Then the CTA waits for
+// them (bounded polls: GOL_E_TIMEOUT in *status and the CTA stops), copies
+// them into its halo and completes generations g = 1..ni near the two edges:
+// rows [K - kk + g, K + g) and the mirror rows at the bottom. Those read
+// generation g - 1 rows that the interior pass of generation g + 1 (same
+// buffer) left alone, since the interior shrinks by one row per side per
+// generation. Generations ni+1..K are then computed whole (the band and the
+// K - g halo rows each side that the halo still determines). Rows outside
+// the grid are never computed and stay dead (zero).
+//
+// Epoch e publishes the band's top and bottom K rows into slot e & 1 and
+// releases an epoch counter; a CTA rewrites a slot two epochs later, after
+// both neighbours have published the epoch in between, i.e. after they read
+// it.
+//
+// Within a pass a thread owns WPL words of a column (the CTA's threads are
+// lanes across the row times row groups) and walks a range of rows with
+// the horizontal sums of three rows in registers. Shared-memory rows carry
+// four zero words of padding each side, so the words just outside a lane's
+// span are plain loads from the row (cheaper on the integer pipe, the
+// bound here, than shuffles and selects). Columns at or past W exist only
+// in the last warps of a row, which alone run the masked variant.
 //
 // All CTAs must be resident at once (they wait on each other): the launch
 // is cooperative, one CTA per SM at most.
@@ -32,11 +45,21 @@
 
 namespace golb200 {
 
-constexpr int kResidentMaxThreads = 512;
+#ifndef GOL_RESIDENT_MAX_THREADS
+#define GOL_RESIDENT_MAX_THREADS 512
+#endif
+constexpr int kResidentMaxThreads = GOL_RESIDENT_MAX_THREADS;
+constexpr int kResidentPad = 4;   // zero words each side of a shared-memory row
+#ifndef GOL_RESIDENT_INTERIOR
+#define GOL_RESIDENT_INTERIOR 1
+#endif
+// Generations of an epoch computed on the interior alone, before the wait
+// for the neighbours' rows.
+constexpr int kResidentInterior = GOL_RESIDENT_INTERIOR;
 
 struct ResidentLaunch {
     const uint32_t* src;   // the grid at generation 0 (W words per row, Y rows)
-    uint32_t* dst;         // the grid after `gens` generations (may alias src)
+    uint32_t* dst;         // the grid after `gens` generations (not src)
     uint32_t* pub;         // [nbands][2 parities][2 sides][K rows][W words]
     int* epoch_done;       // [nbands], zero at launch: epochs published
     int* status;           // GOL_E_TIMEOUT if a wait gave up
@@ -59,10 +82,14 @@ __device__ __forceinline__ void st_release_gpu(int* p, int v) {
     asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Shared memory of one CTA: two buffers of (band + 2K) rows of the row's
-// lanes * WPL words.
+// Words per shared-memory row: the lanes' words plus the padding.
+__host__ __device__ inline int resident_stride(int lanes, int wpl) {
+    return lanes * wpl + 2 * kResidentPad;
+}
+
+// Shared memory of one CTA: two buffers of (band + 2K) rows.
 __host__ __device__ inline size_t resident_smem_bytes(int band, int K, int lanes, int wpl) {
-    return 2ull * (size_t)(band + 2 * K) * (size_t)lanes * wpl * sizeof(uint32_t);
+    return 2ull * (size_t)(band + 2 * K) * (size_t)resident_stride(lanes, wpl) * sizeof(uint32_t);
 }
 
 template <int WPL>
@@ -89,64 +116,94 @@ __device__ __forceinline__ void sts_words_gen(uint32_t* p, const uint32_t (&v)[W
     }
 }
 
-// Horizontal sums of shared-memory row `row` (this lane's WPL words): the
-// words just outside the lane come from its warp neighbours, or from shared
-// memory at the warp's ends; outside the grid they are zero.
+// Horizontal sums of the shared-memory row at p (this lane's words). The
+// words just outside the lane's span are plain loads from the row (its
+// neighbours' words, or the zero padding at the row's ends): no shuffles,
+// selects or divergent loads.
 template <int WPL>
-__device__ __forceinline__ void resident_hsum(const uint32_t* buf, int row, int pitch, int lane,
-                                              int col, int W, uint32_t (&c)[WPL],
+__device__ __forceinline__ void resident_hsum(const uint32_t* p, uint32_t (&c)[WPL],
                                               uint32_t (&h0)[WPL], uint32_t (&h1)[WPL]) {
-    const uint32_t* r = buf + (size_t)row * pitch;
-    lds_words_gen<WPL>(r + col, c);
-    uint32_t lw = __shfl_up_sync(0xffffffffu, c[WPL - 1], 1);
-    uint32_t rw = __shfl_down_sync(0xffffffffu, c[0], 1);
-    if (lane == 0) lw = col > 0 ? r[col - 1] : 0u;
-    if (lane == 31) rw = col + WPL < pitch ? r[col + WPL] : 0u;
-    (void)W;
+    lds_words_gen<WPL>(p, c);
+    const uint32_t lw = p[-1];
+    const uint32_t rw = p[WPL];
 #pragma unroll
     for (int w = 0; w < WPL; ++w) {
         const uint32_t l = w == 0 ? lw : c[w - 1];
-        const uint32_t rr = w == WPL - 1 ? rw : c[w + 1];
-        hsum(l, c[w], rr, h0[w], h1[w]);
+        const uint32_t r = w == WPL - 1 ? rw : c[w + 1];
+        hsum(l, c[w], r, h0[w], h1[w]);
     }
 }
 
-// One output row of a generation: rows of the ring slots M (above), C
-// (the row itself) and P (below, just loaded).
-template <int WPL, int M, int C, int P>
-__device__ __forceinline__ void resident_row(uint32_t (&h0)[3][WPL], uint32_t (&h1)[3][WPL],
-                                             uint32_t (&cw)[3][WPL], uint32_t* D, int r, int pitch,
-                                             int col, int W, bool in) {
+// One output row from the ring slots M (above), C (the row) and P (below).
+template <int WPL, bool RAG, int M, int C, int P>
+__device__ __forceinline__ void resident_row(const uint32_t (&h0)[3][WPL],
+                                             const uint32_t (&h1)[3][WPL],
+                                             const uint32_t (&cw)[3][WPL], uint32_t* d,
+                                             const uint32_t (&cm)[WPL]) {
     uint32_t res[WPL];
 #pragma unroll
     for (int w = 0; w < WPL; ++w) {
-        const uint32_t v = next_word(h0[M][w], h1[M][w], h0[C][w], h1[C][w], h0[P][w], h1[P][w],
-                                     cw[C][w]);
-        res[w] = (in && col + w < W) ? v : 0u;
+        res[w] = next_word(h0[M][w], h1[M][w], h0[C][w], h1[C][w], h0[P][w], h1[P][w], cw[C][w]);
+        if constexpr (RAG) res[w] &= cm[w];
     }
-    sts_words_gen<WPL>(D + (size_t)r * pitch + col, res);
+    sts_words_gen<WPL>(d, res);
 }
 
-// Rows [r0, r1) of one generation, S -> D: the three-row ring of sums in
-// registers, slots named at compile time (the loop is unrolled by three).
-template <int WPL>
+// Rows [r0, r1) of one generation, S -> D (S and D point at this lane's
+// first word of row 0). The loop body covers three rows so the ring slots
+// are compile-time register names; it has no early exits, so the loads of
+// its three rows can be issued together.
+template <int WPL, bool RAG>
 __device__ __forceinline__ void resident_rows(const uint32_t* S, uint32_t* D, int r0, int r1,
-                                              int pitch, int lane, int col, int W, int Y, int gy0) {
+                                              int stride, const uint32_t (&cm)[WPL]) {
+    if (r0 >= r1) return;
     uint32_t h0[3][WPL], h1[3][WPL], cw[3][WPL];
-    resident_hsum<WPL>(S, r0 - 1, pitch, lane, col, W, cw[0], h0[0], h1[0]);
-    resident_hsum<WPL>(S, r0, pitch, lane, col, W, cw[1], h0[1], h1[1]);
-    for (int r = r0; r < r1; r += 3) {
-        resident_hsum<WPL>(S, r + 1, pitch, lane, col, W, cw[2], h0[2], h1[2]);
-        resident_row<WPL, 0, 1, 2>(h0, h1, cw, D, r, pitch, col, W, (unsigned)(gy0 + r) < (unsigned)Y);
-        if (r + 1 >= r1) break;
-        resident_hsum<WPL>(S, r + 2, pitch, lane, col, W, cw[0], h0[0], h1[0]);
-        resident_row<WPL, 1, 2, 0>(h0, h1, cw, D, r + 1, pitch, col, W,
-                                   (unsigned)(gy0 + r + 1) < (unsigned)Y);
-        if (r + 2 >= r1) break;
-        resident_hsum<WPL>(S, r + 3, pitch, lane, col, W, cw[1], h0[1], h1[1]);
-        resident_row<WPL, 2, 0, 1>(h0, h1, cw, D, r + 2, pitch, col, W,
-                                   (unsigned)(gy0 + r + 2) < (unsigned)Y);
+    const uint32_t* s = S + (size_t)(r0 - 1) * stride;
+    uint32_t* d = D + (size_t)r0 * stride;
+    resident_hsum<WPL>(s, cw[0], h0[0], h1[0]);
+    s += stride;
+    resident_hsum<WPL>(s, cw[1], h0[1], h1[1]);
+    s += stride;
+    int n = r1 - r0;
+    for (; n >= 3; n -= 3) {   // slot 0: row r - 1, slot 1: row r
+        resident_hsum<WPL>(s, cw[2], h0[2], h1[2]);
+        resident_row<WPL, RAG, 0, 1, 2>(h0, h1, cw, d, cm);
+        resident_hsum<WPL>(s + stride, cw[0], h0[0], h1[0]);
+        resident_row<WPL, RAG, 1, 2, 0>(h0, h1, cw, d + stride, cm);
+        resident_hsum<WPL>(s + 2 * stride, cw[1], h0[1], h1[1]);
+        resident_row<WPL, RAG, 2, 0, 1>(h0, h1, cw, d + 2 * stride, cm);
+        s += 3 * stride;
+        d += 3 * stride;
     }
+    if (n >= 1) {
+        resident_hsum<WPL>(s, cw[2], h0[2], h1[2]);
+        resident_row<WPL, RAG, 0, 1, 2>(h0, h1, cw, d, cm);
+    }
+    if (n == 2) {
+        resident_hsum<WPL>(s + stride, cw[0], h0[0], h1[0]);
+        resident_row<WPL, RAG, 1, 2, 0>(h0, h1, cw, d + stride, cm);
+    }
+}
+
+// Rows [lo, hi) split over groups [g0, g0 + ng) (this thread's group is g).
+template <int WPL, bool RAG>
+__device__ __forceinline__ void resident_range(const uint32_t* S, uint32_t* D, int lo, int hi,
+                                               int g, int g0, int ng, int stride,
+                                               const uint32_t (&cm)[WPL]) {
+    if (g < g0 || g >= g0 + ng || hi <= lo) return;
+    const int per = (hi - lo + ng - 1) / ng;
+    const int r0 = lo + (g - g0) * per;
+    resident_rows<WPL, RAG>(S, D, r0, min(hi, r0 + per), stride, cm);
+}
+
+template <int WPL>
+__device__ __forceinline__ void resident_pass(const uint32_t* S, uint32_t* D, int lo, int hi,
+                                              int g, int g0, int ng, int stride,
+                                              const uint32_t (&cm)[WPL], bool rag) {
+    if (rag)   // the same for every lane of a warp
+        resident_range<WPL, true>(S, D, lo, hi, g, g0, ng, stride, cm);
+    else
+        resident_range<WPL, false>(S, D, lo, hi, g, g0, ng, stride, cm);
 }
 
 template <int WPL>
@@ -154,32 +211,42 @@ __global__ void __launch_bounds__(kResidentMaxThreads, 1) rows_resident_kernel(R
     extern __shared__ __align__(16) uint32_t smem[];
     __shared__ int stop;
     const int K = a.K;
-    const int pitch = a.lanes * WPL;            // words per shared-memory row (zero past W)
+    const int stride = resident_stride(a.lanes, WPL);
     const int rows = a.band + 2 * K;            // shared-memory rows: K halo each side
     uint32_t* const buf0 = smem;
-    uint32_t* const buf1 = smem + (size_t)rows * pitch;
+    uint32_t* const buf1 = smem + (size_t)rows * stride;
     const int lane_in_row = threadIdx.x % a.lanes;
     const int group = threadIdx.x / a.lanes;
-    const int lane = threadIdx.x & 31;
     const int col = lane_in_row * WPL;
+    // Warps whose span reaches column W mask their results past it.
+    const bool rag = (lane_in_row | 31) * WPL + WPL > a.W;
+    uint32_t cm[WPL];
+#pragma unroll
+    for (int w = 0; w < WPL; ++w) cm[w] = col + w < a.W ? 0xffffffffu : 0u;
     const int cta = blockIdx.x;
     const int nbands = gridDim.x;
+    const bool top = cta == 0, bottom = cta == nbands - 1;
     // Bands split the rows evenly (sizes differ by at most one row, and the
     // planner makes every band at least K rows).
     const int y0 = (int)((long long)cta * a.Y / nbands);
     const int B = (int)((long long)(cta + 1) * a.Y / nbands) - y0;
     const size_t side_words = (size_t)K * a.W;
+    const int ng_top = a.groups > 1 ? a.groups / 2 : 1;
+    const int g_bot = a.groups > 1 ? ng_top : 0;
+    const int ng_bot = a.groups > 1 ? a.groups - ng_top : 1;
 
-    // Band rows into buffer 0 (shared row K + i = grid row y0 + i); halos and
-    // columns past W zero.
-    for (int i = threadIdx.x; i < rows * pitch; i += blockDim.x) {
-        const int r = i / pitch, c = i - r * pitch;
-        buf0[i] = (r >= K && r < K + B && c < a.W) ? a.src[(size_t)(y0 - K + r) * a.W + c] : 0u;
+    // Band rows into buffer 0 (shared row K + i = grid row y0 + i);
+    // everything else zero.
+    for (int i = threadIdx.x; i < rows * stride; i += blockDim.x) {
+        const int r = i / stride, c = i - r * stride - kResidentPad;
+        buf0[i] = (r >= K && r < K + B && c >= 0 && c < a.W)
+                      ? a.src[(size_t)(y0 - K + r) * a.W + c] : 0u;
         buf1[i] = 0u;
     }
     if (threadIdx.x == 0) stop = 0;
     __syncthreads();
 
+    const uint32_t* const lane0 = reinterpret_cast<const uint32_t*>(smem) + kResidentPad + col;
     int cur = 0;
     long long left = a.gens;
     for (int e = 0; left > 0; ++e) {
@@ -189,13 +256,22 @@ __global__ void __launch_bounds__(kResidentMaxThreads, 1) rows_resident_kernel(R
         uint32_t* mine = a.pub + ((size_t)cta * 4 + (e & 1) * 2) * side_words;
         for (int i = threadIdx.x; i < K * a.W; i += blockDim.x) {
             const int r = i / a.W, c = i - r * a.W;
-            mine[i] = A[(size_t)(K + r) * pitch + c];                       // top
-            mine[side_words + i] = A[(size_t)(K + B - K + r) * pitch + c];   // bottom
+            if (!top) mine[i] = A[(size_t)(K + r) * stride + kResidentPad + c];
+            if (!bottom) mine[side_words + i] = A[(size_t)(B + r) * stride + kResidentPad + c];
         }
-        __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) st_release_gpu(a.epoch_done + cta, e + 1);
-        // Wait for the neighbours' publications of this epoch (bounded).
+        // The interior: generation g's rows at least g from the band's edges,
+        // for the first ni generations (enough to cover the exchange).
+        const int ni = min(kk, kResidentInterior);
+        for (int g = 1; g <= ni; ++g) {
+            const int sb = (cur + g - 1) & 1;
+            const uint32_t* S = lane0 + (sb ? (size_t)rows * stride : 0);
+            uint32_t* D = const_cast<uint32_t*>(lane0) + (sb ? 0 : (size_t)rows * stride);
+            resident_pass<WPL>(S, D, K + g, K + B - g, group, 0, a.groups, stride, cm, rag);
+            __syncthreads();
+        }
+        // Wait for the neighbours' rows of this epoch (bounded).
         if (threadIdx.x < 2) {
             const int nb = threadIdx.x == 0 ? cta - 1 : cta + 1;
             if (nb >= 0 && nb < nbands) {
@@ -206,45 +282,54 @@ __global__ void __launch_bounds__(kResidentMaxThreads, 1) rows_resident_kernel(R
                         atomicExch(&stop, 1);
                         break;
                     }
-                    __nanosleep(128);
+                    __nanosleep(64);
                 }
             }
         }
         __syncthreads();
         if (stop) return;   // the same for every thread of the CTA
-        // Every thread acquires the counters whose data it reads next.
-        if (cta > 0) (void)ld_acquire_gpu(a.epoch_done + cta - 1);
-        if (cta + 1 < nbands) (void)ld_acquire_gpu(a.epoch_done + cta + 1);
         // Halo rows: the upper neighbour's bottom rows, the lower one's top
-        // rows (zero beyond the grid).
+        // rows. At the grid's edges they stay zero (never written).
         for (int i = threadIdx.x; i < K * a.W; i += blockDim.x) {
             const int r = i / a.W, c = i - r * a.W;
-            uint32_t up = 0u, dn = 0u;
-            if (cta > 0) up = a.pub[((size_t)(cta - 1) * 4 + (e & 1) * 2 + 1) * side_words + i];
-            if (cta + 1 < nbands) dn = a.pub[((size_t)(cta + 1) * 4 + (e & 1) * 2) * side_words + i];
-            A[(size_t)r * pitch + c] = up;
-            A[(size_t)(K + B + r) * pitch + c] = dn;
+            if (!top)
+                A[(size_t)r * stride + kResidentPad + c] =
+                    a.pub[((size_t)(cta - 1) * 4 + (e & 1) * 2 + 1) * side_words + i];
+            if (!bottom)
+                A[(size_t)(K + B + r) * stride + kResidentPad + c] =
+                    a.pub[((size_t)(cta + 1) * 4 + (e & 1) * 2) * side_words + i];
         }
         __syncthreads();
-        // kk generations in shared memory: generation g computes the shared
-        // rows [K - kk + g, K + B + kk - g) (what the halo still determines).
-        for (int g = 1; g <= kk; ++g) {
-            const int lo = K - kk + g, hi = K + B + kk - g;
-            const int per = (hi - lo + a.groups - 1) / a.groups;
-            const int r0 = lo + group * per, r1 = min(hi, r0 + per);
-            if (r0 < r1)   // the same for every lane of a warp (a warp is in one group)
-                resident_rows<WPL>(cur ? buf1 : buf0, cur ? buf0 : buf1, r0, r1, pitch, lane, col, a.W,
-                                   a.Y, y0 - K);
+        // Generations 1..ni near the edges: rows within g of the band's
+        // edges, and the halo rows the later generations still need.
+        for (int g = 1; g <= ni; ++g) {
+            const int sb = (cur + g - 1) & 1;
+            const uint32_t* S = lane0 + (sb ? (size_t)rows * stride : 0);
+            uint32_t* D = const_cast<uint32_t*>(lane0) + (sb ? 0 : (size_t)rows * stride);
+            const int tlo = top ? K : K - kk + g, thi = K + g;
+            const int blo = max(K + g, K + B - g), bhi = bottom ? K + B : K + B + kk - g;
+            resident_pass<WPL>(S, D, tlo, thi, group, 0, ng_top, stride, cm, rag);
+            resident_pass<WPL>(S, D, blo, bhi, group, g_bot, ng_bot, stride, cm, rag);
             __syncthreads();
-            cur ^= 1;
         }
+        // Generations ni+1..kk whole: the band and what the halo still
+        // determines.
+        for (int g = ni + 1; g <= kk; ++g) {
+            const int sb = (cur + g - 1) & 1;
+            const uint32_t* S = lane0 + (sb ? (size_t)rows * stride : 0);
+            uint32_t* D = const_cast<uint32_t*>(lane0) + (sb ? 0 : (size_t)rows * stride);
+            const int lo = top ? K : K - kk + g, hi = bottom ? K + B : K + B + kk - g;
+            resident_pass<WPL>(S, D, lo, hi, group, 0, a.groups, stride, cm, rag);
+            __syncthreads();
+        }
+        cur = (cur + kk) & 1;
         left -= kk;
     }
     // The band after the last generation.
     const uint32_t* A = cur ? buf1 : buf0;
     for (int i = threadIdx.x; i < B * a.W; i += blockDim.x) {
         const int r = i / a.W, c = i - r * a.W;
-        a.dst[(size_t)(y0 + r) * a.W + c] = A[(size_t)(K + r) * pitch + c];
+        a.dst[(size_t)(y0 + r) * a.W + c] = A[(size_t)(K + r) * stride + kResidentPad + c];
     }
 }
 
