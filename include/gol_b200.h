@@ -241,7 +241,8 @@ int gol_poisson_arrivals(uint64_t seed, uint32_t n, double rate, double* times);
 void* gol_device_grid(gol_engine* e);
 /* The engine's cudaStream_t. */
 void* gol_stream(gol_engine* e);
-/* Temporal depth and band height gol_run uses (after gol_init). */
+/* Temporal depth and band height gol_run uses (after gol_init). For
+ * GOL_ALG_RESIDENT: generations per epoch and the largest CTA band. */
 int gol_plan(const gol_engine* e, uint32_t* temporal_steps, uint32_t* band_rows,
              uint32_t* words_per_lane);
 

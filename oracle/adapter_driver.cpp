@@ -8,7 +8,7 @@
 //
 // Built by `make -C oracle adapter` from the reference sources in place, into
 // oracle/_ref/adapter_driver. Usage:
-//   adapter_driver X Y ITERATIONS SEED [temporal_steps] [local|k1]
+//   adapter_driver X Y ITERATIONS SEED [temporal_steps] [local|k1|resident]
 // `k1` registers the adapter with its depth forced to one generation per
 // pass (GolB200Algorithm<char, GOL_ALG_AUTO, 1>) and checks that the engine
 // ran at that depth.
@@ -47,7 +47,7 @@ static infrastructure::Grid<2, char> perform(Alg& alg, const infrastructure::Exp
 
 int main(int argc, char** argv) {
     if (argc < 5) {
-        std::fprintf(stderr, "usage: %s X Y ITERATIONS SEED [temporal_steps] [local]\n", argv[0]);
+        std::fprintf(stderr, "usage: %s X Y ITERATIONS SEED [temporal_steps] [local|k1|resident]\n", argv[0]);
         return 2;
     }
     infrastructure::ExperimentParams p;
@@ -84,6 +84,9 @@ int main(int argc, char** argv) {
                 alg.finalize_data_structures();
                 std::printf("engine depth: %u generation per pass\n", depth);
             }
+        } else if (argc > 6 && std::strcmp(argv[6], "resident") == 0) {
+            golb200::GolB200Algorithm<char, GOL_ALG_RESIDENT> alg;
+            for (int round = 0; round < 2; ++round) got = perform(alg, p, input, round == 1);
         } else {
             golb200::GolB200Algorithm<char> alg;
             for (int round = 0; round < 2; ++round) got = perform(alg, p, input, round == 1);

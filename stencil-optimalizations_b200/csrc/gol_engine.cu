@@ -632,6 +632,12 @@ int gol_plan(const gol_engine* e, uint32_t* temporal_steps, uint32_t* band_rows,
              uint32_t* words_per_lane) {
     if (!e) return GOL_E_INVALID;
     if (!e->initialized) return GOL_E_STATE;
+    if (e->resident) {   // generations per epoch, the largest CTA band
+        if (temporal_steps) *temporal_steps = (uint32_t)e->rplan.K;
+        if (band_rows) *band_rows = (uint32_t)e->rplan.band;
+        if (words_per_lane) *words_per_lane = (uint32_t)e->rplan.wpl;
+        return GOL_OK;
+    }
     if (temporal_steps) *temporal_steps = (uint32_t)e->k;
     if (band_rows) *band_rows = (uint32_t)e->plan.band;
     if (words_per_lane) *words_per_lane = (uint32_t)e->plan.wpl;

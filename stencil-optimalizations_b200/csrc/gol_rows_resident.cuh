@@ -289,15 +289,17 @@ __global__ void __launch_bounds__(kResidentMaxThreads, 1) rows_resident_kernel(R
         __syncthreads();
         if (stop) return;   // the same for every thread of the CTA
         // Halo rows: the upper neighbour's bottom rows, the lower one's top
-        // rows. At the grid's edges they stay zero (never written).
+        // rows, loaded from L2 (a slot is rewritten every other epoch, so no
+        // copy of it may linger in L1). At the grid's edges they stay zero
+        // (never written).
         for (int i = threadIdx.x; i < K * a.W; i += blockDim.x) {
             const int r = i / a.W, c = i - r * a.W;
             if (!top)
                 A[(size_t)r * stride + kResidentPad + c] =
-                    a.pub[((size_t)(cta - 1) * 4 + (e & 1) * 2 + 1) * side_words + i];
+                    __ldcg(a.pub + ((size_t)(cta - 1) * 4 + (e & 1) * 2 + 1) * side_words + i);
             if (!bottom)
                 A[(size_t)(K + B + r) * stride + kResidentPad + c] =
-                    a.pub[((size_t)(cta + 1) * 4 + (e & 1) * 2) * side_words + i];
+                    __ldcg(a.pub + ((size_t)(cta + 1) * 4 + (e & 1) * 2) * side_words + i);
         }
         __syncthreads();
         // Generations 1..ni near the edges: rows within g of the band's

@@ -20,7 +20,8 @@ DRIVER = os.path.join(ROOT, "oracle", "_ref", "adapter_driver")
                                   ["1024", "96", "64", "3", "8", "local"],
                                   ["128", "64", "0", "5"],
                                   ["512", "200", "33", "9", "1", "k1"],
-                                  ["2048", "64", "20", "4", "6", "k1"]])
+                                  ["2048", "64", "20", "4", "6", "k1"],
+                                  ["1024", "500", "100", "11", "6", "resident"]])
 def test_engine_behind_reference_algorithm_interface(args):
     r = subprocess.run([DRIVER, *args], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
