@@ -157,7 +157,7 @@ bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPla
 }
 
 #ifndef GOL_RESIDENT_K
-#define GOL_RESIDENT_K 6   // generations per epoch of the resident run
+#define GOL_RESIDENT_K 8   // generations per epoch of the resident run
 #endif
 #ifndef GOL_RESIDENT_WPL
 #define GOL_RESIDENT_WPL 2
@@ -197,16 +197,30 @@ bool plan_resident(int W, int Y, int k_epoch, int device, ResidentPlan* p) {
     return true;
 }
 
-template <int WPL>
-static cudaError_t launch_resident_wpl(const ResidentLaunch& a, const ResidentPlan& p,
-                                       cudaStream_t stream) {
-    cudaError_t e = cudaFuncSetAttribute(rows_resident_kernel<WPL>,
+template <int WPL, int LANES>
+static cudaError_t launch_resident_lanes(const ResidentLaunch& a, const ResidentPlan& p,
+                                         cudaStream_t stream) {
+    cudaError_t e = cudaFuncSetAttribute(rows_resident_kernel<WPL, LANES>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
     if (e != cudaSuccess) return e;
     ResidentLaunch arg = a;
     void* args[] = {&arg};
-    return cudaLaunchCooperativeKernel((const void*)rows_resident_kernel<WPL>, dim3(p.nbands),
-                                       dim3(p.lanes * p.groups), args, p.smem, stream);
+    return cudaLaunchCooperativeKernel((const void*)rows_resident_kernel<WPL, LANES>,
+                                       dim3(p.nbands), dim3(p.lanes * p.groups), args, p.smem,
+                                       stream);
+}
+
+// Row widths of 64, 128 and 256 lanes (4096-, 8192- and 16384-cell rows at
+// two words per lane) get a compile-time row stride; others a runtime one.
+template <int WPL>
+static cudaError_t launch_resident_wpl(const ResidentLaunch& a, const ResidentPlan& p,
+                                       cudaStream_t stream) {
+    switch (p.lanes) {
+        case 64: return launch_resident_lanes<WPL, 64>(a, p, stream);
+        case 128: return launch_resident_lanes<WPL, 128>(a, p, stream);
+        case 256: return launch_resident_lanes<WPL, 256>(a, p, stream);
+        default: return launch_resident_lanes<WPL, 0>(a, p, stream);
+    }
 }
 
 cudaError_t launch_resident(const uint32_t* src, uint32_t* dst, int W, int Y, long long gens,

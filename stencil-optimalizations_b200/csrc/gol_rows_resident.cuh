@@ -116,6 +116,21 @@ __device__ __forceinline__ void sts_words_gen(uint32_t* p, const uint32_t (&v)[W
     }
 }
 
+// A lane's WPL words from global memory through L2 only (the exchange
+// slots, which other CTAs rewrite).
+template <int WPL>
+__device__ __forceinline__ void ldcg_words(const uint32_t* p, uint32_t (&v)[WPL]) {
+    if constexpr (WPL == 4) {
+        const uint4 t = __ldcg(reinterpret_cast<const uint4*>(p));
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    } else if constexpr (WPL == 2) {
+        const uint2 t = __ldcg(reinterpret_cast<const uint2*>(p));
+        v[0] = t.x; v[1] = t.y;
+    } else {
+        v[0] = __ldcg(p);
+    }
+}
+
 // Horizontal sums of the shared-memory row at p (this lane's words). The
 // words just outside the lane's span are plain loads from the row (its
 // neighbours' words, or the zero padding at the row's ends): no shuffles,
@@ -206,15 +221,16 @@ __device__ __forceinline__ void resident_pass(const uint32_t* S, uint32_t* D, in
         resident_range<WPL, false>(S, D, lo, hi, g, g0, ng, stride, cm);
 }
 
-template <int WPL>
+// LANES: the lanes across a row when known at compile time (0: a.lanes), so
+// that the shared-memory row stride is a constant and row addresses are
+// immediate offsets (common widths are instantiated so; 1-2 % at 8192^2).
+template <int WPL, int LANES>
 __global__ void __launch_bounds__(kResidentMaxThreads, 1) rows_resident_kernel(ResidentLaunch a) {
     extern __shared__ __align__(16) uint32_t smem[];
     __shared__ int stop;
     const int K = a.K;
-    const int stride = resident_stride(a.lanes, WPL);
+    const int stride = LANES ? resident_stride(LANES, WPL) : resident_stride(a.lanes, WPL);
     const int rows = a.band + 2 * K;            // shared-memory rows: K halo each side
-    uint32_t* const buf0 = smem;
-    uint32_t* const buf1 = smem + (size_t)rows * stride;
     const int lane_in_row = threadIdx.x % a.lanes;
     const int group = threadIdx.x / a.lanes;
     const int col = lane_in_row * WPL;
@@ -235,13 +251,21 @@ __global__ void __launch_bounds__(kResidentMaxThreads, 1) rows_resident_kernel(R
     const int g_bot = a.groups > 1 ? ng_top : 0;
     const int ng_bot = a.groups > 1 ? a.groups - ng_top : 1;
 
-    // Band rows into buffer 0 (shared row K + i = grid row y0 + i);
-    // everything else zero.
-    for (int i = threadIdx.x; i < rows * stride; i += blockDim.x) {
-        const int r = i / stride, c = i - r * stride - kResidentPad;
-        buf0[i] = (r >= K && r < K + B && c >= 0 && c < a.W)
-                      ? a.src[(size_t)(y0 - K + r) * a.W + c] : 0u;
-        buf1[i] = 0u;
+    // Buffers zero (halo rows, padding, columns past W), then the band rows
+    // into buffer 0 (shared row K + i = grid row y0 + i). Copies between
+    // global and shared rows below go by row group and lane: each thread
+    // moves its lane's WPL words (W is a multiple of WPL) of every
+    // groups-th row.
+    for (int i = threadIdx.x; i < 2 * rows * stride; i += blockDim.x) smem[i] = 0u;
+    __syncthreads();
+    const bool in_w = col < a.W;
+    uint32_t* const lane0w = smem + kResidentPad + col;   // this lane's words of shared row 0
+    if (in_w) {
+        for (int r = group; r < B; r += a.groups) {
+            uint32_t v[WPL];
+            load_words<WPL>(a.src + (size_t)(y0 + r) * a.W + col, v);
+            sts_words_gen<WPL>(lane0w + (size_t)(K + r) * stride, v);
+        }
     }
     if (threadIdx.x == 0) stop = 0;
     __syncthreads();
@@ -251,13 +275,21 @@ __global__ void __launch_bounds__(kResidentMaxThreads, 1) rows_resident_kernel(R
     long long left = a.gens;
     for (int e = 0; left > 0; ++e) {
         const int kk = (int)min((long long)K, left);
-        uint32_t* A = cur ? buf1 : buf0;
         // Publish the band's top and bottom K rows (the state at epoch start).
-        uint32_t* mine = a.pub + ((size_t)cta * 4 + (e & 1) * 2) * side_words;
-        for (int i = threadIdx.x; i < K * a.W; i += blockDim.x) {
-            const int r = i / a.W, c = i - r * a.W;
-            if (!top) mine[i] = A[(size_t)(K + r) * stride + kResidentPad + c];
-            if (!bottom) mine[side_words + i] = A[(size_t)(B + r) * stride + kResidentPad + c];
+        uint32_t* mine = a.pub + ((size_t)cta * 4 + (e & 1) * 2) * side_words + col;
+        const uint32_t* Aw = lane0w + (cur ? (size_t)rows * stride : 0);
+        if (in_w) {
+            for (int r = group; r < K; r += a.groups) {
+                uint32_t v[WPL];
+                if (!top) {
+                    lds_words_gen<WPL>(Aw + (size_t)(K + r) * stride, v);
+                    store_words<WPL>(mine + (size_t)r * a.W, v);
+                }
+                if (!bottom) {
+                    lds_words_gen<WPL>(Aw + (size_t)(B + r) * stride, v);
+                    store_words<WPL>(mine + side_words + (size_t)r * a.W, v);
+                }
+            }
         }
         __syncthreads();
         if (threadIdx.x == 0) st_release_gpu(a.epoch_done + cta, e + 1);
@@ -292,14 +324,21 @@ __global__ void __launch_bounds__(kResidentMaxThreads, 1) rows_resident_kernel(R
         // rows, loaded from L2 (a slot is rewritten every other epoch, so no
         // copy of it may linger in L1). At the grid's edges they stay zero
         // (never written).
-        for (int i = threadIdx.x; i < K * a.W; i += blockDim.x) {
-            const int r = i / a.W, c = i - r * a.W;
-            if (!top)
-                A[(size_t)r * stride + kResidentPad + c] =
-                    __ldcg(a.pub + ((size_t)(cta - 1) * 4 + (e & 1) * 2 + 1) * side_words + i);
-            if (!bottom)
-                A[(size_t)(K + B + r) * stride + kResidentPad + c] =
-                    __ldcg(a.pub + ((size_t)(cta + 1) * 4 + (e & 1) * 2) * side_words + i);
+        if (in_w) {
+            const uint32_t* up = a.pub + ((size_t)(cta - 1) * 4 + (e & 1) * 2 + 1) * side_words + col;
+            const uint32_t* dn = a.pub + ((size_t)(cta + 1) * 4 + (e & 1) * 2) * side_words + col;
+            uint32_t* Aw = lane0w + (cur ? (size_t)rows * stride : 0);
+            for (int r = group; r < K; r += a.groups) {
+                uint32_t v[WPL];
+                if (!top) {
+                    ldcg_words<WPL>(up + (size_t)r * a.W, v);
+                    sts_words_gen<WPL>(Aw + (size_t)r * stride, v);
+                }
+                if (!bottom) {
+                    ldcg_words<WPL>(dn + (size_t)r * a.W, v);
+                    sts_words_gen<WPL>(Aw + (size_t)(K + B + r) * stride, v);
+                }
+            }
         }
         __syncthreads();
         // Generations 1..ni near the edges: rows within g of the band's
@@ -328,10 +367,13 @@ __global__ void __launch_bounds__(kResidentMaxThreads, 1) rows_resident_kernel(R
         left -= kk;
     }
     // The band after the last generation.
-    const uint32_t* A = cur ? buf1 : buf0;
-    for (int i = threadIdx.x; i < B * a.W; i += blockDim.x) {
-        const int r = i / a.W, c = i - r * a.W;
-        a.dst[(size_t)(y0 + r) * a.W + c] = A[(size_t)(K + r) * stride + kResidentPad + c];
+    if (in_w) {
+        const uint32_t* Aw = lane0w + (cur ? (size_t)rows * stride : 0);
+        for (int r = group; r < B; r += a.groups) {
+            uint32_t v[WPL];
+            lds_words_gen<WPL>(Aw + (size_t)(K + r) * stride, v);
+            store_words<WPL>(a.dst + (size_t)(y0 + r) * a.W + col, v);
+        }
     }
 }
 

@@ -4,6 +4,7 @@ profiling (ncu) and quick timing.
     python stencil-optimalizations_b200/profile_pass.py --size 16384 --k 5 --passes 8
     python stencil-optimalizations_b200/profile_pass.py --mode local --size 4096 --gens 400
     python stencil-optimalizations_b200/profile_pass.py --mode batch --grids 32
+    python stencil-optimalizations_b200/profile_pass.py --mode resident --size 8192 --gens 240 --k 0
 
 dense (default): k-generation passes of the row-band kernel on the dense
 benchmark input (Bernoulli(0.5), seed 42, from the reference's
@@ -16,6 +17,10 @@ input (--input random); prints the run time and the fraction of tiles
 computed. --dense-pct sets the active-tile share from which passes run dense.
 batch: the first --grids grids of the uneven batched workload (seed 42), one
 persistent launch after a warm-up launch; prints the launch time.
+resident: the shared-memory-resident run (GOL_ALG_RESIDENT) on the dense
+benchmark input, --gens generations in one cooperative launch after a
+warm-up run, --k generations per epoch (0 = the engine's default); prints
+the launch time.
 """
 from __future__ import annotations
 
@@ -37,7 +42,7 @@ def main() -> None:
     ap.add_argument("--passes", type=int, default=8)
     ap.add_argument("--band", type=int, default=0)
     ap.add_argument("--wpl", type=int, default=0)
-    ap.add_argument("--mode", choices=["dense", "local", "batch"], default="dense")
+    ap.add_argument("--mode", choices=["dense", "local", "batch", "resident"], default="dense")
     ap.add_argument("--gens", type=int, default=400)
     ap.add_argument("--grids", type=int, default=32)
     ap.add_argument("--tile-rows", type=int, default=0, help="change-tracking tile height (0 = auto)")
@@ -48,6 +53,8 @@ def main() -> None:
         return run_local(a)
     if a.mode == "batch":
         return run_batch(a)
+    if a.mode == "resident":
+        return run_resident(a)
 
     import torch
     x, y = a.size, a.height or a.size
@@ -96,6 +103,29 @@ def run_local(a) -> None:
     frac = st["computed_tiles"] / max(1, st["passes"] * st["tiles_per_pass"])
     print(f"local {x}x{y}, {a.gens} generations, k={a.k}: {dt * 1e3:.2f} ms (wall), "
           f"{frac:.3f} of tile-passes computed")
+
+
+def run_resident(a) -> None:
+    import torch
+    x, y = a.size, a.height or a.size
+    g = golb200.load_random_ones_zeros(x, y, 42)
+    s = torch.cuda.Stream()
+    with golb200.GolB200(grid_dimensions=(x, y), state_bits_count=32, temporal_steps=a.k,
+                         algorithm="resident", stream=s.cuda_stream) as alg:
+        alg.set_and_format_input_data(g)
+        alg.initialize_data_structures()
+        alg.run(min(a.gens, 16))   # warm-up (module load, attributes)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        alg.run(a.gens)
+        e1.record(s)
+        plan = alg.plan()
+        alg.finalize_data_structures()
+        ms = e0.elapsed_time(e1)
+    print(f"resident {x}x{y}, {a.gens} generations, epochs of {plan['temporal_steps']}, "
+          f"bands of {plan['band_rows']} rows, {plan['words_per_lane']} words per lane: {ms:.3f} ms, "
+          f"{x * y * a.gens / (ms * 1e-3) / 1e12:.2f} Tcell-updates/s")
 
 
 def run_batch(a) -> None:
