@@ -370,10 +370,6 @@ static bool plan_request(gol_server* s, Request& r, uint64_t generations) {
 static uint32_t* slot_gstat(gol_server* s, const Request& r) { return s->arena + r.offset + 2 * r.stride; }
 static uint32_t* slot_trk(gol_server* s, const Request& r) { return slot_gstat(s, r) + 2; }
 
-// Generations a request advances in one round: the quantum, or under the
-// shortest-work-first policy the quantum scaled up for grids smaller than
-// kServeRefCells cells (so small requests finish in few rounds while a
-// round's work stays bounded by the large ones' quantum).
 // Generations a request advances in one round: the quantum. Every round
 // but a request's last advances a multiple of its depth k, so its change
 // flags (which speak of k-generation passes) stay valid from round to
