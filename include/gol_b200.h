@@ -66,8 +66,13 @@ enum gol_algorithm {
     GOL_ALG_LOCAL = 2,       /* change-tracking tiles (skips stable tiles)      */
     GOL_ALG_RESIDENT = 3     /* the whole run in one cooperative launch, bands
                                 kept in shared memory (grids that fit in the
-                                SMs' shared memory, e.g. 8192 x 8192); the run
-                                budget is checked only before the launch      */
+                                SMs' shared memory, e.g. 8192 x 8192, else
+                                gol_init returns GOL_E_UNSUPPORTED);
+                                temporal_steps = generations between halo
+                                exchanges (0 = 8); the run budget is checked
+                                only before the launch; a band that waits too
+                                long for a neighbour stops the run with
+                                GOL_E_TIMEOUT (from gol_sync / gol_finalize) */
 };
 
 /* Mirrors the ExperimentParams fields the hot path reads
