@@ -396,7 +396,7 @@ void gol_batch_destroy(gol_batch* b);
  * half the free HBM at creation) in which admitted requests keep their two
  * grid buffers until fetched. gol_serve_step admits queued requests that fit
  * (arrival order, first fit) and queues one persistent batch launch that
- * advances every admitted request by up to `quantum` generations (0 = 128);
+ * advances every admitted request by up to `quantum` generations (0 = 64);
  * up to three rounds are queued at once, so requests arriving meanwhile join
  * the next round while the GPU keeps working. */
 typedef struct gol_server gol_server;

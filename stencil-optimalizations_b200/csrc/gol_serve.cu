@@ -101,7 +101,7 @@ struct gol_server {
     uint32_t* arena = nullptr;
     size_t arena_words = 0;
     std::map<size_t, size_t> free_blocks;   // offset -> length (words)
-    uint64_t quantum = 128;
+    uint64_t quantum = 64;
     int policy = GOL_SERVE_FIFO;
     int track_mode = GOL_TRACK_AUTO;
     unsigned long long* d_census = nullptr;   // wait / work cycles, items computed / skipped
@@ -303,7 +303,7 @@ int gol_serve_create(gol_server** out, int32_t device, uint64_t arena_bytes, uin
     gol_server* s = new (std::nothrow) gol_server();
     if (!s) return GOL_E_NOMEM;
     s->device = device;
-    s->quantum = quantum ? quantum : 128;
+    s->quantum = quantum ? quantum : 64;
     cudaError_t ce = cudaSetDevice(device);
     if (ce == cudaSuccess) {
         if (stream) {

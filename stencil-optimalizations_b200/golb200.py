@@ -731,7 +731,7 @@ class GolServer:
     """Continuous-batching server (gol_serve_*): requests stay resident on the
     device and advance together, one persistent launch per round."""
 
-    def __init__(self, device: int = 0, arena_bytes: int = 0, quantum: int = 128,
+    def __init__(self, device: int = 0, arena_bytes: int = 0, quantum: int = 0,
                  stream: int | None = None):
         self._s = _vp()
         rc = lib().gol_serve_create(ctypes.byref(self._s), device, arena_bytes, quantum, stream)

@@ -41,7 +41,7 @@ def usable_cpus() -> int:
 
 
 def run_stream(rate: float = 2000.0, seconds: float = 2.0, seed: int = 42, min_side: int = 128,
-               max_side: int = 8192, density=(0.1, 0.5), gens=(16, 8192), quantum: int = 128,
+               max_side: int = 8192, density=(0.1, 0.5), gens=(16, 8192), quantum: int = 0,
                arena_bytes: int = 0, device: int = 0, fetch: str = "words",
                max_requests: int | None = None, server: golb200.GolServer | None = None,
                policy: str = "fifo", tracking: str = "auto", host_io: bool = False,
@@ -135,7 +135,7 @@ def run_stream(rate: float = 2000.0, seconds: float = 2.0, seed: int = 42, min_s
         "latency_p99_ms": float(np.percentile(lat, 99) * 1e3),
         "latency_max_ms": float(lat.max() * 1e3),
         "rounds": stats["rounds"],
-        "quantum_generations": quantum,
+        "quantum_generations": quantum or 64,
     }
 
 
@@ -144,7 +144,7 @@ def main() -> None:
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--seconds", type=float, default=2.0)
     ap.add_argument("--seed", type=int, default=42)
-    ap.add_argument("--quantum", type=int, default=128)
+    ap.add_argument("--quantum", type=int, default=0, help="generations per round (0 = the server default, 64)")
     ap.add_argument("--policy", choices=["fifo", "srpt"], default="fifo")
     ap.add_argument("--tracking", choices=["auto", "on", "off"], default="auto")
     ap.add_argument("--host-io", action="store_true")
