@@ -468,13 +468,19 @@ int gol_run(gol_engine* e, uint64_t n) {
         return (uint64_t)s.count() >= budget;
     };
     if (e->resident) {   // every generation in one cooperative launch
-        if (time_is_up()) return GOL_OK;
-        cudaError_t ce = golb200::launch_resident(e->d[e->cur], e->d[e->cur ^ 1], e->W, e->Y,
-                                                  (long long)n, e->rplan, e->r_pub, e->r_ints,
-                                                  e->r_ints + e->rplan.nbands, e->stream);
-        if (ce != cudaSuccess) return e->cuda_fail(ce, "resident run launch");
-        e->cur ^= 1;
-        e->performed = n;
+        // (runs longer than 2^30 generations in several, so the kernel's
+        // epoch counters stay within int)
+        for (uint64_t done = 0; done < n;) {
+            if (time_is_up()) return GOL_OK;
+            const uint64_t chunk = std::min<uint64_t>(n - done, 1ull << 30);
+            cudaError_t ce = golb200::launch_resident(e->d[e->cur], e->d[e->cur ^ 1], e->W, e->Y,
+                                                      (long long)chunk, e->rplan, e->r_pub, e->r_ints,
+                                                      e->r_ints + e->rplan.nbands, e->stream);
+            if (ce != cudaSuccess) return e->cuda_fail(ce, "resident run launch");
+            e->cur ^= 1;
+            done += chunk;
+            e->performed = done;
+        }
         return GOL_OK;
     }
     const int k = e->k;

@@ -181,8 +181,8 @@ bool plan_resident(int W, int Y, int k_epoch, int device, ResidentPlan* p) {
         return false;
     // Every band at least K rows (a band's halo comes from its neighbours
     // only), at most one CTA per SM; the largest band's two buffers must fit.
-    const int nbands = std::min(sms, Y / K);
-    if (nbands < 1) return false;
+    // A grid of fewer than K rows is one band with no neighbours.
+    const int nbands = std::max(1, std::min(sms, Y / K));
     const int band = (Y + nbands - 1) / nbands;
     const size_t smem = resident_smem_bytes(band, K, lanes, wpl);
     if (smem + 1024 > (size_t)smem_max) return false;

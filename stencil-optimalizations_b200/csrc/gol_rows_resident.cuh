@@ -64,7 +64,8 @@ struct ResidentLaunch {
     int* epoch_done;       // [nbands], zero at launch: epochs published
     int* status;           // GOL_E_TIMEOUT if a wait gave up
     int W, Y;
-    int band;              // rows of the largest band (bands split Y evenly, each >= K)
+    int band;              // rows of the largest band (bands split Y evenly, each >= K
+                           // when there are several)
     int K;                 // generations per epoch
     int lanes;             // lanes across a row (ceil(W / WPL), a multiple of 32)
     int groups;            // row groups (blockDim.x = lanes * groups)
@@ -347,8 +348,9 @@ __global__ void __launch_bounds__(kResidentMaxThreads, 1) rows_resident_kernel(R
             const int sb = (cur + g - 1) & 1;
             const uint32_t* S = lane0 + (sb ? (size_t)rows * stride : 0);
             uint32_t* D = const_cast<uint32_t*>(lane0) + (sb ? 0 : (size_t)rows * stride);
-            const int tlo = top ? K : K - kk + g, thi = K + g;
-            const int blo = max(K + g, K + B - g), bhi = bottom ? K + B : K + B + kk - g;
+            const int bhi = bottom ? K + B : K + B + kk - g;
+            const int tlo = top ? K : K - kk + g, thi = min(K + g, bhi);   // (a band under g rows)
+            const int blo = max(K + g, K + B - g);
             resident_pass<WPL>(S, D, tlo, thi, group, 0, ng_top, stride, cm, rag);
             resident_pass<WPL>(S, D, blo, bhi, group, g_bot, ng_bot, stride, cm, rag);
             __syncthreads();
