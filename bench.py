@@ -553,10 +553,12 @@ def _plain_graphs_multistream(work, inputs, device, nstreams: int = 8) -> tuple:
 
 def bench_batched(stream, device, n: int = 512, seed: int = SEED) -> dict:
     """512 grids, sides log-uniform [256, 4096] (multiples of 64), density
-    U[0.2, 0.5], generations log-uniform [64, 4096]: one persistent launch,
-    against (1) one launch per pass per grid on one stream and (2) every grid
-    through the one-grid engine's graph-chunked gol_run over 8 streams; every
-    grid's batched result checked against the oracle."""
+    U[0.2, 0.5], generations log-uniform [64, 4096]: one persistent launch
+    (both batched modes: dependent pass items, and bands resident in shared
+    memory; value_batched is the faster), against (1) one launch per pass per
+    grid on one stream and (2) every grid through the one-grid engine's
+    graph-chunked gol_run over 8 streams; every grid's result of both batched
+    modes checked against the oracle."""
     import concurrent.futures as cf
 
     import golb200
@@ -584,6 +586,13 @@ def bench_batched(stream, device, n: int = 512, seed: int = SEED) -> dict:
     tiles = b.tiles()
     tracked = sum(1 for i in range(n) if b.grid_stats(i)["tracked"])
     results = [oracle.pack_rows(b.fetch(i), 64) for i in range(n)]
+    # the resident batch: every grid's bands in shared memory for all their
+    # generations (first run plans the bands)
+    b.run_resident()
+    b.sync()
+    resident = [_events_ms(stream, b.run_resident, b.sync) for _ in range(3)]
+    rinfo = b.resident_info()
+    results_res = [oracle.pack_rows(b.fetch(i), 64) for i in range(n)]
     b.run_plain(4)
     b.sync()
     plain = [_events_ms(stream, lambda: b.run_plain(4), b.sync) for _ in range(2)]
@@ -596,17 +605,28 @@ def bench_batched(stream, device, n: int = 512, seed: int = SEED) -> dict:
         d = work[i]
         want = oracle.life_rows(inputs[i], d["x"], d["gens"], 64,
                                 threads=1 if inputs[i].size < (1 << 16) else 4)
-        return bool(np.array_equal(results[i], want))
+        return bool(np.array_equal(results[i], want)), bool(np.array_equal(results_res[i], want))
     with cf.ThreadPoolExecutor(max_workers=max(1, (usable_cpus() or 2) // 2)) as pool:
         ok = list(pool.map(check, range(n)))
     cu = info["cell_updates"]
-    vb = cu / (min(batched) * 1e-3) / 1e9
+    v_passes = cu / (min(batched) * 1e-3) / 1e9
+    v_res = cu / (min(resident) * 1e-3) / 1e9
+    vb = max(v_passes, v_res)
     vp = cu / (min(plain) * 1e-3) / 1e9
     vg = cu / (ms_graphs * 1e-3) / 1e9
     return {"workload": f"{n} grids, sides log-uniform [256, 4096] x64, density U[0.2, 0.5], "
                         f"generations log-uniform [64, 4096], seed {seed}",
             "cell_updates": cu, "work_items": info["items"], "unit": UNIT,
-            "value_batched": vb, "ms_batched": min(batched),
+            "value_batched": vb, "ms_batched": min(min(batched), min(resident)),
+            "batched_mode": "resident" if v_res >= v_passes else "passes",
+            "value_batched_passes": v_passes, "ms_batched_passes": min(batched),
+            "value_batched_resident": v_res, "ms_batched_resident": min(resident),
+            "resident_plan": rinfo,
+            "modes": {"passes": "gol_batch_run: one persistent launch of dependent k-generation "
+                                "work items (bands of passes), change tracking autotuned",
+                      "resident": "gol_batch_run_resident: every grid cut into bands, each band "
+                                  "in one CTA's shared memory for all its generations, halo "
+                                  "rows exchanged every 8 generations"},
             "autotuner": {"first_run_items": first_tiles, "grids_tracked_after_retune": tracked,
                           "timed_run_items": tiles},
             "value_plain_per_grid": vp, "ms_plain": min(plain), "speedup": vb / vp,
@@ -616,7 +636,10 @@ def bench_batched(stream, device, n: int = 512, seed: int = SEED) -> dict:
                                         "of 16 passes), 8 streams, one engine per grid",
             "batched_equals_plain_on_sample": same,
             "batched_equals_graphs_multistream_all": graphs_same,
-            "batched_all_equal_oracle": all(ok), "grids_checked_vs_oracle": len(ok)}
+            "batched_all_equal_oracle": all(o[0] and o[1] for o in ok),
+            "batched_passes_all_equal_oracle": all(o[0] for o in ok),
+            "batched_resident_all_equal_oracle": all(o[1] for o in ok),
+            "grids_checked_vs_oracle": len(ok)}
 
 
 def _check_serving_samples(samples) -> dict:
@@ -644,7 +667,8 @@ def bench_batched_settling(stream, device, n: int = 512, seed: int = SEED) -> di
     settling inputs: dead grids with patches of Bernoulli(0.35) soup in 5 %
     of their 64 x 64 slots (at least one). Batched with change tracking
     (autotuned: a first run, gol_batch_retune, then timed runs) against the
-    same batch with every grid tracked and with none; every grid of every
+    same batch with every grid tracked and with none, and the resident batch
+    (every generation computed, bands in shared memory); every grid of every
     run checked against the oracle."""
     import concurrent.futures as cf
 
@@ -663,13 +687,22 @@ def bench_batched_settling(stream, device, n: int = 512, seed: int = SEED) -> di
     results = {}
     # on: every grid tracked; off: none; auto: the autotuner (a first run,
     # gol_batch_retune, then the timed runs)
-    for mode in ("on", "off", "auto"):
+    for mode in ("on", "off", "auto", "resident"):
         b = golb200.GolBatch(device=device, stream=stream.cuda_stream)
         for d, w in zip(work, inputs):
             gid = b.add(oracle.unpack_rows(w, d["x"], 64), d["gens"])
-            b.set_tracking(gid, mode)
+            b.set_tracking(gid, "off" if mode == "resident" else mode)
         b.upload()
         info = b.info()
+        if mode == "resident":   # bands in shared memory, every generation computed
+            b.run_resident()
+            b.sync()
+            ms = min(_events_ms(stream, b.run_resident, b.sync) for _ in range(3))
+            out["value_resident"] = info["cell_updates"] / (ms * 1e-3) / 1e9
+            out["ms_resident"] = ms
+            results[mode] = [oracle.pack_rows(b.fetch(i), 64) for i in range(n)]
+            b.close()
+            continue
         b.run()
         b.sync()
         if mode == "auto":

@@ -352,6 +352,18 @@ int gol_batch_run(gol_batch* b);
 /* Baseline: the same grids one after another through the single-grid pass
  * kernel, one launch per k-generation pass per grid. */
 int gol_batch_run_plain(gol_batch* b, uint32_t temporal_steps);
+/* Every grid in shared memory: each grid is cut into bands, and one
+ * persistent cooperative launch runs every band to its grid's last generation
+ * in one CTA's shared memory (the GOL_ALG_RESIDENT algorithm; neighbouring
+ * bands exchange halo rows every 8 generations). CTAs take bands in order of
+ * their work, a grid's bands consecutively. Asynchronous; restarts from the
+ * inputs; gol_batch_sync reports GOL_E_TIMEOUT if a band waited too long for
+ * a neighbour. GOL_E_UNSUPPORTED if a grid is wider than 32768 cells or
+ * needs more bands than the GPU runs CTAs. No change tracking. */
+int gol_batch_run_resident(gol_batch* b);
+/* The last resident plan: bands, CTAs, shared memory per CTA. */
+int gol_batch_resident_info(const gol_batch* b, uint64_t* bands, uint32_t* ctas,
+                            uint64_t* smem_bytes);
 /* Waits; GOL_E_TIMEOUT if the persistent kernel gave up a dependency wait. */
 int gol_batch_sync(gol_batch* b);
 int gol_batch_fetch(gol_batch* b, int32_t grid_id, uint8_t* cells);

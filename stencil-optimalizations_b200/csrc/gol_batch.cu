@@ -44,6 +44,7 @@
 
 #include "gol_b200.h"
 #include "gol_internal.h"
+#include "gol_rows_resident.cuh"
 #include "gol_rows_temporal.cuh"
 
 #ifndef GOL_BATCH_REPLAN
@@ -615,6 +616,14 @@ struct gol_batch {
     int wpl_only = 0;                     // lane width shared by every grid (0: mixed)
     bool uploaded = false, ran = false;
     cudaGraphExec_t graph = nullptr;
+    // Resident runs (gol_batch_run_resident): bands of every grid, their
+    // exchange slots and epoch counters; built on the first such run after
+    // an upload.
+    golb200::ResidentBand* d_rjobs = nullptr;
+    uint32_t* d_rpub = nullptr;
+    int* d_rdone = nullptr;
+    int rjobs = 0, rdone = 0, rctas = 0;
+    size_t rsmem = 0;
     double last_ms = 0;
     std::string err;
 
@@ -646,6 +655,13 @@ int forced_band(const gol_batch::Entry& e) { return e.force_band ? e.force_band 
 void batch_free_device(gol_batch* b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
+    for (void* p : {(void*)b->d_rjobs, (void*)b->d_rpub, (void*)b->d_rdone})
+        if (p) cudaFree(p);
+    b->d_rjobs = nullptr;
+    b->d_rpub = nullptr;
+    b->d_rdone = nullptr;
+    b->rjobs = b->rdone = b->rctas = 0;
+    b->rsmem = 0;
     for (void* p : {(void*)b->arena, (void*)b->d_grids, (void*)b->d_items, (void*)b->d_done,
                     (void*)b->d_ticket, (void*)b->d_status, (void*)b->d_census, (void*)b->d_trk,
                     (void*)b->d_pstat, (void*)b->d_gstat})
@@ -1003,6 +1019,178 @@ int gol_batch_run_plain(gol_batch* b, uint32_t temporal_steps) {
         e.result_buf = cur;
     }
     b->ran = true;
+    return GOL_OK;
+}
+
+namespace {
+
+constexpr int kResidentBatchWpl = 2;        // words per lane of the resident batch kernel
+constexpr int kResidentBatchThreads = 512;  // threads per CTA
+constexpr int kResidentBatchK = 8;          // generations per epoch
+constexpr int kResidentBatchRowsPerGroup = 8;   // fewer rows per group and pass cost warm-up
+constexpr int kResidentBatchBandsPerCta = 3;    // about this many bands per CTA (balance)
+
+cudaError_t resident_batch_launch(gol_batch* b, int njobs, cudaStream_t s) {
+    using golb200::batch_resident_kernel;
+    cudaError_t ce = cudaFuncSetAttribute(batch_resident_kernel<kResidentBatchWpl>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->rsmem);
+    if (ce != cudaSuccess) return ce;
+    golb200::ResidentBand* jobs = b->d_rjobs;
+    int* ticket = b->d_ticket;
+    int* status = b->d_status;
+    long long spin = 1ll << 24;
+    void* args[] = {&jobs, &njobs, &ticket, &status, &spin};
+    return cudaLaunchCooperativeKernel((const void*)batch_resident_kernel<kResidentBatchWpl>,
+                                       dim3(b->rctas), dim3(kResidentBatchThreads), args, b->rsmem, s);
+}
+
+// Bands of every grid for the resident batch kernel: per grid, lanes of two
+// words across its row and row groups over the CTA's threads; as many bands
+// as the shared memory needs, more for grids whose work would otherwise make
+// one band a long job (about kResidentBatchBandsPerCta bands per CTA over the
+// batch), fewer where a band would give a row group under
+// kResidentBatchRowsPerGroup rows; every band of a grid at least K rows, at
+// most as many bands as CTAs. Bands are ordered by their work, longest
+// first, a grid's bands consecutive.
+int resident_batch_plan(gol_batch* b) {
+    int smem_optin = 0;
+    cudaError_t ce = cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
+    if (ce != cudaSuccess) return b->cuda_fail(ce, "device attribute");
+    const size_t avail = (size_t)smem_optin - 1024;
+    double total = 0;
+    for (const auto& e : b->grids) total += (double)e.W * e.Y * e.gens;
+    struct GridBands { int gi, nb, K, lanes, groups; double band_work; size_t smem; };
+    std::vector<GridBands> gb;
+    size_t smem = 0;
+    for (size_t gi = 0; gi < b->grids.size(); ++gi) {
+        const auto& e = b->grids[gi];
+        if (e.gens == 0 || e.W == 0 || e.Y == 0) continue;
+        const int lanes = (e.W + kResidentBatchWpl - 1) / kResidentBatchWpl;
+        if (lanes > kResidentBatchThreads)
+            return b->fail(GOL_E_UNSUPPORTED, "a grid is too wide for the resident batch");
+        const int groups = kResidentBatchThreads / lanes;
+        const int K = (int)std::min<uint64_t>(e.gens, kResidentBatchK);
+        const size_t row_bytes = 2ull * golb200::resident_stride(lanes, kResidentBatchWpl) * 4;
+        const long long fit = (long long)(avail / row_bytes) - 2 * K;   // band rows that fit
+        if (fit < 1) return b->fail(GOL_E_UNSUPPORTED, "a grid's rows do not fit in shared memory");
+        const int nb_min = (int)((e.Y + fit - 1) / fit);
+        const double work = (double)e.W * e.Y * e.gens;
+        const int nb_work = (int)std::ceil(work / std::max(1.0, total / ((double)b->num_sms *
+                                                                          kResidentBatchBandsPerCta)));
+        const int nb_rows = std::max(1, e.Y / std::max(K, kResidentBatchRowsPerGroup * groups));
+        int nb = std::max(nb_min, std::min(nb_work, nb_rows));
+        const int nb_cap = std::max(1, e.Y / K);
+        if (nb > nb_cap) {
+            if (nb_min > nb_cap) return b->fail(GOL_E_UNSUPPORTED, "a grid needs bands under K rows");
+            nb = nb_cap;
+        }
+        const int B = (e.Y + nb - 1) / nb;
+        const size_t need = (size_t)(B + 2 * K) * row_bytes;
+        smem = std::max(smem, need);
+        gb.push_back({(int)gi, nb, K, lanes, groups, (double)e.W * B * e.gens, need});
+    }
+    int per_sm = 0;
+    ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, golb200::batch_resident_kernel<kResidentBatchWpl>, kResidentBatchThreads,
+        std::max<size_t>(smem, 1));
+    if (ce == cudaSuccess && smem > 48 * 1024) {
+        ce = cudaFuncSetAttribute(golb200::batch_resident_kernel<kResidentBatchWpl>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (ce == cudaSuccess)
+            ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, golb200::batch_resident_kernel<kResidentBatchWpl>, kResidentBatchThreads, smem);
+    }
+    if (ce != cudaSuccess) return b->cuda_fail(ce, "resident batch occupancy");
+    if (per_sm < 1) return b->fail(GOL_E_UNSUPPORTED, "resident batch kernel does not fit on an SM");
+    const int ctas = per_sm * b->num_sms;
+    for (const auto& g : gb)
+        if (g.nb > ctas) return b->fail(GOL_E_UNSUPPORTED, "a grid needs more bands than CTAs");
+    std::stable_sort(gb.begin(), gb.end(),
+                     [](const GridBands& a, const GridBands& c) { return a.band_work > c.band_work; });
+    // exchange slots and counters
+    size_t pub_words = 0;
+    int ndone = 0;
+    std::vector<size_t> pub_off(gb.size());
+    std::vector<int> done_off(gb.size());
+    for (size_t i = 0; i < gb.size(); ++i) {
+        const auto& e = b->grids[gb[i].gi];
+        const int ppitch = (e.W + 3) / 4 * 4;
+        pub_off[i] = pub_words;
+        pub_words += (size_t)gb[i].nb * 4 * gb[i].K * ppitch;
+        done_off[i] = ndone;
+        ndone += gb[i].nb;
+    }
+    ce = cudaMalloc(&b->d_rpub, std::max<size_t>(pub_words, 1) * sizeof(uint32_t));
+    if (ce == cudaSuccess) ce = cudaMalloc(&b->d_rdone, std::max(ndone, 1) * sizeof(int));
+    if (ce == cudaSuccess)
+        ce = cudaMalloc(&b->d_rjobs, std::max(ndone, 1) * sizeof(golb200::ResidentBand));
+    if (ce != cudaSuccess) return b->cuda_fail(ce, "resident batch scratch");
+    std::vector<golb200::ResidentBand> jobs;
+    jobs.reserve(ndone);
+    for (size_t i = 0; i < gb.size(); ++i) {
+        const auto& e = b->grids[gb[i].gi];
+        for (int band = 0; band < gb[i].nb; ++band) {
+            golb200::ResidentBand j{};
+            j.src = b->arena + e.offset;
+            j.dst = b->arena + e.offset + e.stride;
+            j.pub = b->d_rpub + pub_off[i];
+            j.done = b->d_rdone + done_off[i];
+            j.pitch = e.pitch;
+            j.ppitch = (e.W + 3) / 4 * 4;
+            j.W = e.W;
+            j.Y = e.Y;
+            j.K = gb[i].K;
+            j.lanes = gb[i].lanes;
+            j.groups = gb[i].groups;
+            j.b = band;
+            j.nb = gb[i].nb;
+            j.gens = (long long)e.gens;
+            jobs.push_back(j);
+        }
+    }
+    ce = cudaMemcpyAsync(b->d_rjobs, jobs.data(), jobs.size() * sizeof(golb200::ResidentBand),
+                         cudaMemcpyHostToDevice, b->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(b->stream);
+    if (ce != cudaSuccess) return b->cuda_fail(ce, "resident batch jobs");
+    b->rjobs = (int)jobs.size();
+    b->rdone = ndone;
+    b->rctas = ctas;
+    b->rsmem = smem;
+    return GOL_OK;
+}
+
+} // namespace
+
+// Every grid's bands kept in shared memory for all their generations (the
+// single-grid resident run's algorithm), persistent CTAs taking bands in
+// ticket order. Asynchronous like gol_batch_run; results in buf[1].
+int gol_batch_run_resident(gol_batch* b) {
+    if (!b) return GOL_E_INVALID;
+    int rc;
+    if (!b->uploaded && (rc = gol_batch_upload(b))) return rc;
+    if (!b->d_rjobs && (rc = resident_batch_plan(b))) return rc;
+    cudaError_t ce = batch_restore_inputs(b, b->stream);
+    // grids with no generations: the result is the input
+    for (auto& e : b->grids)
+        if (ce == cudaSuccess && e.gens == 0 && e.W && e.Y)
+            ce = cudaMemcpyAsync(b->arena + e.offset + e.stride, b->arena + e.offset,
+                                 (size_t)e.pitch * e.Y * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                                 b->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_rdone, 0, std::max(b->rdone, 1) * sizeof(int), b->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_ticket, 0, sizeof(int), b->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_status, 0, sizeof(int), b->stream);
+    if (ce == cudaSuccess && b->rjobs) ce = resident_batch_launch(b, b->rjobs, b->stream);
+    if (ce != cudaSuccess) return b->cuda_fail(ce, "resident batch launch");
+    for (auto& e : b->grids) e.result_buf = 1;
+    b->ran = true;
+    return GOL_OK;
+}
+
+int gol_batch_resident_info(const gol_batch* b, uint64_t* bands, uint32_t* ctas, uint64_t* smem_bytes) {
+    if (!b) return GOL_E_INVALID;
+    if (bands) *bands = (uint64_t)b->rjobs;
+    if (ctas) *ctas = (uint32_t)b->rctas;
+    if (smem_bytes) *smem_bytes = (uint64_t)b->rsmem;
     return GOL_OK;
 }
 

@@ -57,7 +57,7 @@ constexpr int kResidentPad = 4;   // zero words each side of a shared-memory row
 // for the neighbours' rows.
 constexpr int kResidentInterior = GOL_RESIDENT_INTERIOR;
 
-struct ResidentLaunch {
+struct ResidentLaunch {   // one grid (rows_resident_kernel)
     const uint32_t* src;   // the grid at generation 0 (W words per row, Y rows)
     uint32_t* dst;         // the grid after `gens` generations (not src)
     uint32_t* pub;         // [nbands][2 parities][2 sides][K rows][W words]
@@ -222,78 +222,119 @@ __device__ __forceinline__ void resident_pass(const uint32_t* S, uint32_t* D, in
         resident_range<WPL, false>(S, D, lo, hi, g, g0, ng, stride, cm);
 }
 
-// LANES: the lanes across a row when known at compile time (0: a.lanes), so
-// that the shared-memory row stride is a constant and row addresses are
-// immediate offsets (common widths are instantiated so; 1-2 % at 8192^2).
+// One band of one grid, all generations, in this CTA's shared memory.
+struct ResidentBand {
+    const uint32_t* src;   // the grid at generation 0 (row r at src + r * pitch)
+    uint32_t* dst;         // the grid after `gens` generations (not src)
+    uint32_t* pub;         // the grid's exchange slots: band b's at (b * 4 + parity * 2 + side)
+                           // * K * ppitch words (side 0: its top K rows, 1: its bottom K rows)
+    int* done;             // the grid's epoch counters, one per band, zero at start
+    int pitch;             // words from one grid row to the next (>= W)
+    int ppitch;            // words per row in the exchange slots (>= W, a multiple of WPL)
+    int W, Y;              // words per row, rows
+    int K;                 // generations per epoch
+    int lanes, groups;     // threads: lanes across a row x row groups
+    int b, nb;             // this band, bands of the grid (rows split evenly)
+    long long gens;
+};
+
+// Global <-> register copies of a lane's words: vector accesses where the
+// lane's words are whole and aligned, else word by word up to W.
+template <int WPL>
+__device__ __forceinline__ void band_load(const uint32_t* p, bool vec, int n, uint32_t (&v)[WPL]) {
+    if (vec) {
+        load_words<WPL>(p, v);
+    } else {
+#pragma unroll
+        for (int w = 0; w < WPL; ++w) v[w] = w < n ? __ldg(p + w) : 0u;
+    }
+}
+
+template <int WPL>
+__device__ __forceinline__ void band_store(uint32_t* p, bool vec, int n, const uint32_t (&v)[WPL]) {
+    if (vec) {
+        store_words<WPL>(p, v);
+    } else {
+#pragma unroll
+        for (int w = 0; w < WPL; ++w)
+            if (w < n) p[w] = v[w];
+    }
+}
+
+// Runs band j.b of its grid: returns false if a wait gave up (GOL_E_TIMEOUT
+// in *status; the caller ends the CTA). Every thread of the CTA calls it;
+// smem holds 2 * (B + 2K) rows of the stride. LANES: the lanes across a row
+// when known at compile time (0: j.lanes), so the shared-memory row stride
+// is a constant and row addresses are immediate offsets.
 template <int WPL, int LANES>
-__global__ void __launch_bounds__(kResidentMaxThreads, 1) rows_resident_kernel(ResidentLaunch a) {
-    extern __shared__ __align__(16) uint32_t smem[];
-    __shared__ int stop;
-    const int K = a.K;
-    const int stride = LANES ? resident_stride(LANES, WPL) : resident_stride(a.lanes, WPL);
-    const int rows = a.band + 2 * K;            // shared-memory rows: K halo each side
-    const int lane_in_row = threadIdx.x % a.lanes;
-    const int group = threadIdx.x / a.lanes;
+__device__ __forceinline__ bool resident_band(const ResidentBand& j, uint32_t* smem, int* stop,
+                                              int* status, long long spin_limit) {
+    const int K = j.K;
+    const int stride = LANES ? resident_stride(LANES, WPL) : resident_stride(j.lanes, WPL);
+    const int lane_in_row = threadIdx.x % j.lanes;
+    const int group = threadIdx.x / j.lanes;   // >= j.groups: idle in the passes
     const int col = lane_in_row * WPL;
-    // Warps whose span reaches column W mask their results past it.
-    const bool rag = (lane_in_row | 31) * WPL + WPL > a.W;
+    const int W = j.W;
+    // Warps whose span reaches column W mask their results past it (when
+    // lanes is a multiple of 32 a warp lies within one row).
+    const bool rag = (j.lanes & 31) ? col + WPL > W : (lane_in_row | 31) * WPL + WPL > W;
     uint32_t cm[WPL];
 #pragma unroll
-    for (int w = 0; w < WPL; ++w) cm[w] = col + w < a.W ? 0xffffffffu : 0u;
-    const int cta = blockIdx.x;
-    const int nbands = gridDim.x;
-    const bool top = cta == 0, bottom = cta == nbands - 1;
-    // Bands split the rows evenly (sizes differ by at most one row, and the
-    // planner makes every band at least K rows).
-    const int y0 = (int)((long long)cta * a.Y / nbands);
-    const int B = (int)((long long)(cta + 1) * a.Y / nbands) - y0;
-    const size_t side_words = (size_t)K * a.W;
-    const int ng_top = a.groups > 1 ? a.groups / 2 : 1;
-    const int g_bot = a.groups > 1 ? ng_top : 0;
-    const int ng_bot = a.groups > 1 ? a.groups - ng_top : 1;
+    for (int w = 0; w < WPL; ++w) cm[w] = col + w < W ? 0xffffffffu : 0u;
+    const bool top = j.b == 0, bottom = j.b == j.nb - 1;
+    // Bands split the rows evenly (sizes differ by at most one row; with
+    // several bands every band is at least K rows).
+    const int y0 = (int)((long long)j.b * j.Y / j.nb);
+    const int B = (int)((long long)(j.b + 1) * j.Y / j.nb) - y0;
+    const int rows = B + 2 * K;                 // shared-memory rows: K halo each side
+    const size_t side_words = (size_t)K * j.ppitch;
+    const int ng_top = j.groups > 1 ? j.groups / 2 : 1;
+    const int g_bot = j.groups > 1 ? ng_top : 0;
+    const int ng_bot = j.groups > 1 ? j.groups - ng_top : 1;
+    const bool mine_lane = col < W && group < j.groups;   // moves words between global and shared
+    const int nw = W - col;                             // words of this lane inside the row
+    const bool gvec = col + WPL <= W && (j.pitch % WPL) == 0;
 
     // Buffers zero (halo rows, padding, columns past W), then the band rows
     // into buffer 0 (shared row K + i = grid row y0 + i). Copies between
-    // global and shared rows below go by row group and lane: each thread
-    // moves its lane's WPL words (W is a multiple of WPL) of every
-    // groups-th row.
+    // global and shared rows go by row group and lane: each thread moves its
+    // lane's WPL words of every groups-th row.
     for (int i = threadIdx.x; i < 2 * rows * stride; i += blockDim.x) smem[i] = 0u;
     __syncthreads();
-    const bool in_w = col < a.W;
     uint32_t* const lane0w = smem + kResidentPad + col;   // this lane's words of shared row 0
-    if (in_w) {
-        for (int r = group; r < B; r += a.groups) {
+    if (mine_lane) {
+        for (int r = group; r < B; r += j.groups) {
             uint32_t v[WPL];
-            load_words<WPL>(a.src + (size_t)(y0 + r) * a.W + col, v);
+            band_load<WPL>(j.src + (size_t)(y0 + r) * j.pitch + col, gvec, nw, v);
             sts_words_gen<WPL>(lane0w + (size_t)(K + r) * stride, v);
         }
     }
-    if (threadIdx.x == 0) stop = 0;
+    if (threadIdx.x == 0) *stop = 0;
     __syncthreads();
 
-    const uint32_t* const lane0 = reinterpret_cast<const uint32_t*>(smem) + kResidentPad + col;
+    const uint32_t* const lane0 = lane0w;
     int cur = 0;
-    long long left = a.gens;
+    long long left = j.gens;
     for (int e = 0; left > 0; ++e) {
         const int kk = (int)min((long long)K, left);
         // Publish the band's top and bottom K rows (the state at epoch start).
-        uint32_t* mine = a.pub + ((size_t)cta * 4 + (e & 1) * 2) * side_words + col;
+        uint32_t* mine = j.pub + ((size_t)j.b * 4 + (e & 1) * 2) * side_words + col;
         const uint32_t* Aw = lane0w + (cur ? (size_t)rows * stride : 0);
-        if (in_w) {
-            for (int r = group; r < K; r += a.groups) {
+        if (mine_lane) {
+            for (int r = group; r < K; r += j.groups) {
                 uint32_t v[WPL];
                 if (!top) {
                     lds_words_gen<WPL>(Aw + (size_t)(K + r) * stride, v);
-                    store_words<WPL>(mine + (size_t)r * a.W, v);
+                    store_words<WPL>(mine + (size_t)r * j.ppitch, v);
                 }
                 if (!bottom) {
                     lds_words_gen<WPL>(Aw + (size_t)(B + r) * stride, v);
-                    store_words<WPL>(mine + side_words + (size_t)r * a.W, v);
+                    store_words<WPL>(mine + side_words + (size_t)r * j.ppitch, v);
                 }
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0) st_release_gpu(a.epoch_done + cta, e + 1);
+        if (threadIdx.x == 0) st_release_gpu(j.done + j.b, e + 1);
         // The interior: generation g's rows at least g from the band's edges,
         // for the first ni generations (enough to cover the exchange).
         const int ni = min(kk, kResidentInterior);
@@ -301,18 +342,18 @@ __global__ void __launch_bounds__(kResidentMaxThreads, 1) rows_resident_kernel(R
             const int sb = (cur + g - 1) & 1;
             const uint32_t* S = lane0 + (sb ? (size_t)rows * stride : 0);
             uint32_t* D = const_cast<uint32_t*>(lane0) + (sb ? 0 : (size_t)rows * stride);
-            resident_pass<WPL>(S, D, K + g, K + B - g, group, 0, a.groups, stride, cm, rag);
+            resident_pass<WPL>(S, D, K + g, K + B - g, group, 0, j.groups, stride, cm, rag);
             __syncthreads();
         }
         // Wait for the neighbours' rows of this epoch (bounded).
         if (threadIdx.x < 2) {
-            const int nb = threadIdx.x == 0 ? cta - 1 : cta + 1;
-            if (nb >= 0 && nb < nbands) {
+            const int nb = threadIdx.x == 0 ? j.b - 1 : j.b + 1;
+            if (nb >= 0 && nb < j.nb) {
                 long long spins = 0;
-                while (ld_acquire_gpu(a.epoch_done + nb) < e + 1) {
-                    if (++spins > a.spin_limit || *(volatile int*)a.status != 0) {
-                        atomicCAS(a.status, 0, GOL_E_TIMEOUT);
-                        atomicExch(&stop, 1);
+                while (ld_acquire_gpu(j.done + nb) < e + 1) {
+                    if (++spins > spin_limit || *(volatile int*)status != 0) {
+                        atomicCAS(status, 0, GOL_E_TIMEOUT);
+                        atomicExch(stop, 1);
                         break;
                     }
                     __nanosleep(64);
@@ -320,24 +361,24 @@ __global__ void __launch_bounds__(kResidentMaxThreads, 1) rows_resident_kernel(R
             }
         }
         __syncthreads();
-        if (stop) return;   // the same for every thread of the CTA
+        if (*(volatile int*)stop) return false;   // the same for every thread of the CTA
         // Halo rows: the upper neighbour's bottom rows, the lower one's top
         // rows, loaded from L2 (a slot is rewritten every other epoch, so no
         // copy of it may linger in L1). At the grid's edges they stay zero
         // (never written).
-        if (in_w) {
-            const uint32_t* up = a.pub + ((size_t)(cta - 1) * 4 + (e & 1) * 2 + 1) * side_words + col;
-            const uint32_t* dn = a.pub + ((size_t)(cta + 1) * 4 + (e & 1) * 2) * side_words + col;
-            uint32_t* Aw = lane0w + (cur ? (size_t)rows * stride : 0);
-            for (int r = group; r < K; r += a.groups) {
+        if (mine_lane) {
+            const uint32_t* up = j.pub + ((size_t)(j.b - 1) * 4 + (e & 1) * 2 + 1) * side_words + col;
+            const uint32_t* dn = j.pub + ((size_t)(j.b + 1) * 4 + (e & 1) * 2) * side_words + col;
+            uint32_t* Aw2 = lane0w + (cur ? (size_t)rows * stride : 0);
+            for (int r = group; r < K; r += j.groups) {
                 uint32_t v[WPL];
                 if (!top) {
-                    ldcg_words<WPL>(up + (size_t)r * a.W, v);
-                    sts_words_gen<WPL>(Aw + (size_t)r * stride, v);
+                    ldcg_words<WPL>(up + (size_t)r * j.ppitch, v);
+                    sts_words_gen<WPL>(Aw2 + (size_t)r * stride, v);
                 }
                 if (!bottom) {
-                    ldcg_words<WPL>(dn + (size_t)r * a.W, v);
-                    sts_words_gen<WPL>(Aw + (size_t)(K + B + r) * stride, v);
+                    ldcg_words<WPL>(dn + (size_t)r * j.ppitch, v);
+                    sts_words_gen<WPL>(Aw2 + (size_t)(K + B + r) * stride, v);
                 }
             }
         }
@@ -362,20 +403,68 @@ __global__ void __launch_bounds__(kResidentMaxThreads, 1) rows_resident_kernel(R
             const uint32_t* S = lane0 + (sb ? (size_t)rows * stride : 0);
             uint32_t* D = const_cast<uint32_t*>(lane0) + (sb ? 0 : (size_t)rows * stride);
             const int lo = top ? K : K - kk + g, hi = bottom ? K + B : K + B + kk - g;
-            resident_pass<WPL>(S, D, lo, hi, group, 0, a.groups, stride, cm, rag);
+            resident_pass<WPL>(S, D, lo, hi, group, 0, j.groups, stride, cm, rag);
             __syncthreads();
         }
         cur = (cur + kk) & 1;
         left -= kk;
     }
     // The band after the last generation.
-    if (in_w) {
+    if (mine_lane) {
         const uint32_t* Aw = lane0w + (cur ? (size_t)rows * stride : 0);
-        for (int r = group; r < B; r += a.groups) {
+        for (int r = group; r < B; r += j.groups) {
             uint32_t v[WPL];
             lds_words_gen<WPL>(Aw + (size_t)(K + r) * stride, v);
-            store_words<WPL>(a.dst + (size_t)(y0 + r) * a.W + col, v);
+            band_store<WPL>(j.dst + (size_t)(y0 + r) * j.pitch + col, gvec, nw, v);
         }
+    }
+    return true;
+}
+
+// One grid: CTA c runs band c.
+template <int WPL, int LANES>
+__global__ void __launch_bounds__(kResidentMaxThreads, 1) rows_resident_kernel(ResidentLaunch a) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    __shared__ int stop;
+    ResidentBand j;
+    j.src = a.src;
+    j.dst = a.dst;
+    j.pub = a.pub;
+    j.done = a.epoch_done;
+    j.pitch = a.W;
+    j.ppitch = a.W;
+    j.W = a.W;
+    j.Y = a.Y;
+    j.K = a.K;
+    j.lanes = a.lanes;
+    j.groups = a.groups;
+    j.b = blockIdx.x;
+    j.nb = gridDim.x;
+    j.gens = a.gens;
+    resident_band<WPL, LANES>(j, smem, &stop, a.status, a.spin_limit);
+}
+
+// Many grids: persistent CTAs (all resident: a cooperative launch) take
+// bands in ticket order and run each to its last generation. The bands of a
+// grid have consecutive tickets, so a band's neighbours are always taken by
+// CTAs that are running or will be as soon as one frees up: a grid has at
+// most as many bands as there are CTAs, and bands of earlier grids never
+// wait on later tickets.
+template <int WPL>
+__global__ void __launch_bounds__(kResidentMaxThreads, 1)
+batch_resident_kernel(const ResidentBand* __restrict__ jobs, int njobs, int* ticket, int* status,
+                      long long spin_limit) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    __shared__ int stop;
+    __shared__ int job;
+    for (;;) {
+        if (threadIdx.x == 0) job = atomicAdd(ticket, 1);
+        __syncthreads();
+        const int t = job;
+        if (t >= njobs) return;
+        const ResidentBand j = jobs[t];
+        if (!resident_band<WPL, 0>(j, smem, &stop, status, spin_limit)) return;
+        __syncthreads();   // shared memory and `job` are reused by the next band
     }
 }
 

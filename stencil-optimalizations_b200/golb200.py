@@ -151,6 +151,9 @@ def lib():
     L.gol_batch_upload.argtypes = [_vp]
     L.gol_batch_run.argtypes = [_vp]
     L.gol_batch_run_plain.argtypes = [_vp, _u32]
+    L.gol_batch_run_resident.argtypes = [_vp]
+    L.gol_batch_resident_info.argtypes = [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u32),
+                                          ctypes.POINTER(_u64)]
     L.gol_batch_sync.argtypes = [_vp]
     L.gol_batch_fetch.argtypes = [_vp, ctypes.c_int32, _vp]
     L.gol_batch_info.argtypes = [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u64)]
@@ -650,6 +653,17 @@ class GolBatch:
 
     def run_plain(self, temporal_steps: int = 4) -> None:
         self._check(lib().gol_batch_run_plain(self._b, temporal_steps), "batch_run_plain")
+
+    def run_resident(self) -> None:
+        """Every grid's bands in shared memory for all their generations, one
+        persistent cooperative launch (gol_batch_run_resident)."""
+        self._check(lib().gol_batch_run_resident(self._b), "batch_run_resident")
+
+    def resident_info(self) -> dict:
+        n, c, m = ctypes.c_uint64(), ctypes.c_uint32(), ctypes.c_uint64()
+        self._check(lib().gol_batch_resident_info(self._b, ctypes.byref(n), ctypes.byref(c),
+                                                  ctypes.byref(m)), "batch_resident_info")
+        return {"bands": n.value, "ctas": c.value, "smem_bytes": m.value}
 
     def sync(self) -> None:
         self._check(lib().gol_batch_sync(self._b), "batch_sync")

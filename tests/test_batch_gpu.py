@@ -43,6 +43,33 @@ def test_batch_forced_plans(wpl, k, band):
             assert np.array_equal(b.fetch(gid), oracle.life_cells(c, n)), (gid, c.shape, n)
 
 
+def test_batch_resident_vs_oracle():
+    """gol_batch_run_resident: every grid cut into bands held in shared memory
+    for all its generations; uneven sizes (odd word counts, one row, fewer
+    rows than an epoch), zero, one and few generations, twice in a row and
+    after a pass-by-pass run of the same batch."""
+    work = small_workload(11, 40, lo=32, hi=2048, gens=(1, 300))
+    work += [(oracle.random_ones_zeros(32 * 37, 90, 3), 41),     # odd word count
+             (oracle.random_ones_zeros(32, 1, 5), 9),            # one word, one row
+             (oracle.random_ones_zeros(64, 3, 6), 0),            # zero generations
+             (oracle.random_ones_zeros(128, 5, 7), 20),          # fewer rows than an epoch
+             (oracle.random_ones_zeros(4096, 700, 8), 3),        # fewer generations than an epoch
+             (oracle.random_ones_zeros(8192, 1000, 9), 64)]      # many bands
+    with golb200.GolBatch() as b:
+        ids = [b.add(c, n) for c, n in work]
+        want = [oracle.life_cells(c, n) for c, n in work]
+        for run in ("resident", "passes", "resident"):
+            if run == "resident":
+                b.run_resident()
+            else:
+                b.run()
+            b.sync()
+            for gid, w in zip(ids, want):
+                assert np.array_equal(b.fetch(gid), w), (run, gid, work[gid][0].shape, work[gid][1])
+        info = b.resident_info()
+        assert info["bands"] > len(work) and info["ctas"] >= 148
+
+
 def test_batch_wide_sliced_and_tiny_grids():
     work = [(oracle.random_ones_zeros(5120, 40, 3), 37),        # 160 words: x-sliced
             (oracle.random_ones_zeros(8192, 24, 4), 21),

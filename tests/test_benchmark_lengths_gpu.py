@@ -66,7 +66,8 @@ def oracle_grid(words: np.ndarray, x: int, gens: int) -> np.ndarray:
     return oracle.life_rows(words, x, gens, 64, threads=threads)
 
 
-def test_batched_workload_every_grid():
+@pytest.mark.parametrize("mode", ["passes", "resident"])
+def test_batched_workload_every_grid(mode):
     work = golb200.workload_uneven(42, 512, 256, 4096, 64, (0.2, 0.5), (64, 4096))
     inputs = []
     with golb200.GolBatch() as b:
@@ -75,7 +76,10 @@ def test_batched_workload_every_grid():
             inputs.append(oracle.pack_rows(cells, 64))
             b.add(cells, d["gens"])
         b.upload()
-        b.run()
+        if mode == "resident":
+            b.run_resident()
+        else:
+            b.run()
         b.sync()
         got = [oracle.pack_rows(b.fetch(i), 64) for i in range(len(work))]
     workers = max(1, (usable_cpus() or 1) // 2)
