@@ -16,7 +16,8 @@ reference's always-changing loader (--input blinkers) or the dense benchmark
 input (--input random); prints the run time and the fraction of tiles
 computed. --dense-pct sets the active-tile share from which passes run dense.
 batch: the first --grids grids of the uneven batched workload (seed 42), one
-persistent launch after a warm-up launch; prints the launch time.
+persistent launch after a warm-up launch (--batch-mode passes: gol_batch_run;
+resident: gol_batch_run_resident); prints the launch time.
 resident: the shared-memory-resident run (GOL_ALG_RESIDENT) on the dense
 benchmark input, --gens generations in one cooperative launch after a
 warm-up run, --k generations per epoch (0 = the engine's default); prints
@@ -48,6 +49,7 @@ def main() -> None:
     ap.add_argument("--tile-rows", type=int, default=0, help="change-tracking tile height (0 = auto)")
     ap.add_argument("--input", choices=["sparse", "blinkers", "random"], default="sparse")
     ap.add_argument("--dense-pct", type=int, default=0)
+    ap.add_argument("--batch-mode", choices=["passes", "resident"], default="passes")
     a = ap.parse_args()
     if a.mode == "local":
         return run_local(a)
@@ -138,16 +140,19 @@ def run_batch(a) -> None:
         b.add(golb200.load_bernoulli(d["x"], d["y"], d["cell_seed"], d["density"]), d["gens"])
         cu += d["x"] * d["y"] * d["gens"]
     b.upload()
-    b.run()
+    run = b.run_resident if a.batch_mode == "resident" else b.run
+    run()
     b.sync()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(s)
-    b.run()
+    run()
     e1.record(s)
     b.sync()
     ms = e0.elapsed_time(e1)
-    print(f"batch of {len(work)} grids, {b.info()['items']} items: {ms:.2f} ms, "
+    units = (f"{b.resident_info()['bands']} bands" if a.batch_mode == "resident"
+             else f"{b.info()['items']} items")
+    print(f"batch of {len(work)} grids ({a.batch_mode}), {units}: {ms:.2f} ms, "
           f"{cu / (ms * 1e-3) / 1e12:.2f} Tcell-updates/s")
     b.close()
 
