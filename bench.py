@@ -742,27 +742,33 @@ def bench_serving(device) -> dict:
     copied back, then both with host I/O (host cells, made before the stream
     starts, in through gol_serve_submit; cells out through gol_serve_fetch)
     on the stream's first 0.5 s. Change tracking is on for long requests
-    (auto). Every 64th request of the FIFO runs is checked against the
-    oracle."""
+    (auto). The FIFO runs again with resident rounds (every request's bands
+    in shared memory, no change tracking). Every 64th request of the FIFO
+    runs is checked against the oracle."""
     import serve
     out = {"workload": "Poisson arrivals, mean 2000 req/s for 2 s, sides log-uniform [128, 8192] "
                        "x64, density U[0.1, 0.5], generations log-uniform [16, 8192], seed 42",
            "unit_throughput": "cell-updates/s"}
-    for policy in ("fifo", "srpt"):
-        for host_io in (False, True):
-            r = serve.run_stream(rate=2000.0, seconds=0.5 if host_io else 2.0, seed=SEED,
-                                 device=device, policy=policy, host_io=host_io,
-                                 check_every=64 if policy == "fifo" else 0)
-            samples = r.pop("samples")
-            if samples:
-                r["check"] = _check_serving_samples(samples)
-            r["p99_over_p50"] = r["latency_p99_ms"] / max(r["latency_p50_ms"], 1e-9)
-            out[f"{policy}{'_host_io' if host_io else ''}"] = r
-    # the headline figures: the FIFO run with device-side inputs
+    runs = [("fifo", False, "passes"), ("fifo", True, "passes"), ("srpt", False, "passes"),
+            ("srpt", True, "passes"), ("fifo", False, "resident"), ("fifo", True, "resident")]
+    for policy, host_io, mode in runs:
+        r = serve.run_stream(rate=2000.0, seconds=0.5 if host_io else 2.0, seed=SEED,
+                             device=device, policy=policy, host_io=host_io, mode=mode,
+                             check_every=64 if policy == "fifo" else 0)
+        samples = r.pop("samples")
+        if samples:
+            r["check"] = _check_serving_samples(samples)
+        r["p99_over_p50"] = r["latency_p99_ms"] / max(r["latency_p50_ms"], 1e-9)
+        out[f"{policy}{'_host_io' if host_io else ''}{'_resident' if mode == 'resident' else ''}"] = r
+    # the headline figures: the FIFO run with device-side inputs, in the
+    # round mode with the lower p50
+    best = min(("fifo", "fifo_resident"), key=lambda k: out[k]["latency_p50_ms"])
+    out["headline_run"] = best
     for k in ("requests", "cell_updates_per_s", "latency_p50_ms", "latency_p99_ms"):
-        out[k] = out["fifo"][k]
-    out["serving_sample_equal_oracle"] = all(out[k].get("check", {}).get("all_equal_oracle", True)
-                                             for k in ("fifo", "fifo_host_io"))
+        out[k] = out[best][k]
+    out["serving_sample_equal_oracle"] = all(
+        out[k].get("check", {}).get("all_equal_oracle", True)
+        for k in ("fifo", "fifo_host_io", "fifo_resident", "fifo_host_io_resident"))
     return out
 
 

@@ -359,7 +359,7 @@ int gol_batch_run_plain(gol_batch* b, uint32_t temporal_steps);
  * their work, a grid's bands consecutively. Asynchronous; restarts from the
  * inputs; gol_batch_sync reports GOL_E_TIMEOUT if a band waited too long for
  * a neighbour. GOL_E_UNSUPPORTED if a grid is wider than 32768 cells or
- * needs more bands than the GPU runs CTAs. No change tracking. */
+ * needs more bands than the GPU has SMs. No change tracking. */
 int gol_batch_run_resident(gol_batch* b);
 /* The last resident plan: bands, CTAs, shared memory per CTA. */
 int gol_batch_resident_info(const gol_batch* b, uint64_t* bands, uint32_t* ctas,
@@ -450,6 +450,17 @@ int gol_serve_set_policy(gol_server* s, int32_t policy);
  * changes nothing the request is finished at the end of that round, before
  * its remaining generations (they could not change it). */
 int gol_serve_set_tracking(gol_server* s, int32_t mode);
+/* How a round runs: GOL_SERVE_PASSES (default) as one persistent launch of
+ * dependent k-generation work items (change tracking as set above);
+ * GOL_SERVE_RESIDENT with every running request's grid cut into bands held
+ * in shared memory for the round's generations (gol_batch_run_resident's
+ * kernel; no change tracking, requests finish when their generations are
+ * done; in this mode gol_serve_submit rejects, GOL_E_UNSUPPORTED, a request
+ * whose bands cannot all be resident at once: rows wider than 32768 cells, or
+ * taller than the SMs' shared memory holds). Changes only while no request is
+ * queued or running (GOL_E_STATE). */
+enum gol_serve_mode { GOL_SERVE_PASSES = 0, GOL_SERVE_RESIDENT = 1 };
+int gol_serve_set_mode(gol_server* s, int32_t mode);
 /* Work items computed and skipped over all rounds so far, and the number of
  * requests finished early because they became still. */
 int gol_serve_tiles(gol_server* s, uint64_t* computed, uint64_t* skipped, uint64_t* early_finished);

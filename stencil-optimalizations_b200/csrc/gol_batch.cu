@@ -569,6 +569,140 @@ cudaError_t launch_batch_kernel(const BatchGrid* d_grids, const BatchItem* d_ite
 using golb200::BatchGrid;
 using golb200::BatchItem;
 
+namespace golb200 {
+
+namespace {
+constexpr int kResidentBatchWpl = 2;        // words per lane of the resident batch kernel
+constexpr int kResidentBatchThreads = 512;  // threads per CTA
+constexpr int kResidentBatchK = 8;          // generations per epoch
+constexpr int kResidentBatchRowsPerGroup = 8;   // fewer rows per group and pass cost warm-up
+constexpr int kResidentBatchBandsPerCta = 3;    // about this many bands per CTA (balance)
+} // namespace
+
+// Per grid: lanes of two words across its row and row groups over the CTA's
+// threads; as many bands as the shared memory needs, more for grids whose
+// work would otherwise make one band a long job (about
+// kResidentBatchBandsPerCta bands per CTA over the batch), fewer where a
+// band would give a row group under kResidentBatchRowsPerGroup rows; every
+// band of a grid at least K rows, at most one band per SM.
+const char* plan_resident_batch(const ResidentGrid* g, size_t n, int num_sms, int device,
+                                ResidentBatchPlan* p) {
+    int smem_optin = 0;
+    if (cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess)
+        return "device attribute";
+    const size_t avail = (size_t)smem_optin - 1024;
+    double total = 0;
+    for (size_t i = 0; i < n; ++i) total += (double)g[i].W * g[i].Y * g[i].gens;
+    std::vector<std::pair<double, ResidentBatchPlan::Grid>> order;
+    size_t smem = 0;
+    for (size_t i = 0; i < n; ++i) {
+        const ResidentGrid& e = g[i];
+        const int lanes = (e.W + kResidentBatchWpl - 1) / kResidentBatchWpl;
+        if (lanes > kResidentBatchThreads) return "a grid is too wide for the resident batch";
+        const int groups = kResidentBatchThreads / lanes;
+        const int K = (int)std::min<long long>(e.gens, kResidentBatchK);
+        const size_t row_bytes = 2ull * resident_stride(lanes, kResidentBatchWpl) * 4;
+        const long long fit = (long long)(avail / row_bytes) - 2 * K;   // band rows that fit
+        if (fit < 1) return "a grid's rows do not fit in shared memory";
+        const int nb_min = (int)((e.Y + fit - 1) / fit);
+        const double work = (double)e.W * e.Y * e.gens;
+        const int nb_work = (int)std::ceil(work / std::max(1.0, total / ((double)num_sms *
+                                                                          kResidentBatchBandsPerCta)));
+        const int nb_rows = std::max(1, e.Y / std::max(K, kResidentBatchRowsPerGroup * groups));
+        int nb = std::max(nb_min, std::min(nb_work, nb_rows));
+        // at most one band per SM (every CTA may hold the largest shared
+        // memory), every band at least K rows
+        const int nb_cap = std::min(num_sms, std::max(1, e.Y / K));
+        if (nb > nb_cap) {
+            if (nb_min > nb_cap) return "a grid needs more bands than the GPU runs at once, or bands under K rows";
+            nb = nb_cap;
+        }
+        const int B = (e.Y + nb - 1) / nb;
+        smem = std::max(smem, (size_t)(B + 2 * K) * row_bytes);
+        ResidentBatchPlan::Grid pg{(int)i, nb, K, lanes, groups, (e.W + 3) / 4 * 4, 0, 0};
+        order.push_back({(double)e.W * B * e.gens, pg});
+    }
+    int per_sm = 0;
+    if (cudaFuncSetAttribute(batch_resident_kernel<kResidentBatchWpl>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)std::max<size_t>(smem, 1)) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_resident_kernel<kResidentBatchWpl>,
+                                                      kResidentBatchThreads,
+                                                      std::max<size_t>(smem, 1)) != cudaSuccess)
+        return "resident batch occupancy";
+    if (per_sm < 1) return "resident batch kernel does not fit on an SM";
+    const int ctas = per_sm * num_sms;
+    std::stable_sort(order.begin(), order.end(),
+                     [](const auto& a, const auto& c) { return a.first > c.first; });
+    p->grids.clear();
+    p->pub_words = 0;
+    p->ndone = 0;
+    for (auto& o : order) {
+        if (o.second.nb > ctas) return "a grid needs more bands than CTAs";
+        o.second.pub_off = p->pub_words;
+        o.second.done_off = p->ndone;
+        p->pub_words += (size_t)o.second.nb * 4 * o.second.K * o.second.ppitch;
+        p->ndone += o.second.nb;
+        p->grids.push_back(o.second);
+    }
+    p->smem = smem;
+    p->ctas = ctas;
+    return nullptr;
+}
+
+bool resident_batch_fits(int W, int Y, int num_sms, int device) {
+    int smem_optin = 0;
+    if (W <= 0 || Y <= 0 ||
+        cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess)
+        return false;
+    const int lanes = (W + kResidentBatchWpl - 1) / kResidentBatchWpl;
+    if (lanes > kResidentBatchThreads) return false;
+    const size_t row_bytes = 2ull * resident_stride(lanes, kResidentBatchWpl) * 4;
+    const long long fit = (long long)(((size_t)smem_optin - 1024) / row_bytes) - 2 * kResidentBatchK;
+    if (fit < 1) return false;
+    const long long nb_min = (Y + fit - 1) / fit;
+    return nb_min <= std::min(num_sms, std::max(1, Y / kResidentBatchK));
+}
+
+void fill_resident_jobs(const ResidentBatchPlan& p, const ResidentGrid* g, uint32_t* pub, int* done,
+                        ResidentBand* jobs) {
+    int t = 0;
+    for (const auto& pg : p.grids) {
+        const ResidentGrid& e = g[pg.index];
+        for (int band = 0; band < pg.nb; ++band) {
+            ResidentBand& j = jobs[t++];
+            j.src = e.src;
+            j.dst = e.dst;
+            j.pub = pub + pg.pub_off;
+            j.done = done + pg.done_off;
+            j.pitch = e.pitch;
+            j.ppitch = pg.ppitch;
+            j.W = e.W;
+            j.Y = e.Y;
+            j.K = pg.K;
+            j.lanes = pg.lanes;
+            j.groups = pg.groups;
+            j.b = band;
+            j.nb = pg.nb;
+            j.gens = e.gens;
+        }
+    }
+}
+
+cudaError_t launch_batch_resident(const ResidentBand* jobs, int njobs, int* ticket, int* status,
+                                  const ResidentBatchPlan& p, cudaStream_t stream) {
+    cudaError_t ce = cudaFuncSetAttribute(batch_resident_kernel<kResidentBatchWpl>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)std::max<size_t>(p.smem, 1));
+    if (ce != cudaSuccess) return ce;
+    long long spin = 1ll << 24;
+    void* args[] = {&jobs, &njobs, &ticket, &status, &spin};
+    return cudaLaunchCooperativeKernel((const void*)batch_resident_kernel<kResidentBatchWpl>,
+                                       dim3(p.ctas), dim3(kResidentBatchThreads), args, p.smem, stream);
+}
+
+} // namespace golb200
+
 struct gol_batch {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -624,6 +758,7 @@ struct gol_batch {
     int* d_rdone = nullptr;
     int rjobs = 0, rdone = 0, rctas = 0;
     size_t rsmem = 0;
+    golb200::ResidentBatchPlan rplan;
     double last_ms = 0;
     std::string err;
 
@@ -1022,145 +1157,6 @@ int gol_batch_run_plain(gol_batch* b, uint32_t temporal_steps) {
     return GOL_OK;
 }
 
-namespace {
-
-constexpr int kResidentBatchWpl = 2;        // words per lane of the resident batch kernel
-constexpr int kResidentBatchThreads = 512;  // threads per CTA
-constexpr int kResidentBatchK = 8;          // generations per epoch
-constexpr int kResidentBatchRowsPerGroup = 8;   // fewer rows per group and pass cost warm-up
-constexpr int kResidentBatchBandsPerCta = 3;    // about this many bands per CTA (balance)
-
-cudaError_t resident_batch_launch(gol_batch* b, int njobs, cudaStream_t s) {
-    using golb200::batch_resident_kernel;
-    cudaError_t ce = cudaFuncSetAttribute(batch_resident_kernel<kResidentBatchWpl>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->rsmem);
-    if (ce != cudaSuccess) return ce;
-    golb200::ResidentBand* jobs = b->d_rjobs;
-    int* ticket = b->d_ticket;
-    int* status = b->d_status;
-    long long spin = 1ll << 24;
-    void* args[] = {&jobs, &njobs, &ticket, &status, &spin};
-    return cudaLaunchCooperativeKernel((const void*)batch_resident_kernel<kResidentBatchWpl>,
-                                       dim3(b->rctas), dim3(kResidentBatchThreads), args, b->rsmem, s);
-}
-
-// Bands of every grid for the resident batch kernel: per grid, lanes of two
-// words across its row and row groups over the CTA's threads; as many bands
-// as the shared memory needs, more for grids whose work would otherwise make
-// one band a long job (about kResidentBatchBandsPerCta bands per CTA over the
-// batch), fewer where a band would give a row group under
-// kResidentBatchRowsPerGroup rows; every band of a grid at least K rows, at
-// most as many bands as CTAs. Bands are ordered by their work, longest
-// first, a grid's bands consecutive.
-int resident_batch_plan(gol_batch* b) {
-    int smem_optin = 0;
-    cudaError_t ce = cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
-    if (ce != cudaSuccess) return b->cuda_fail(ce, "device attribute");
-    const size_t avail = (size_t)smem_optin - 1024;
-    double total = 0;
-    for (const auto& e : b->grids) total += (double)e.W * e.Y * e.gens;
-    struct GridBands { int gi, nb, K, lanes, groups; double band_work; size_t smem; };
-    std::vector<GridBands> gb;
-    size_t smem = 0;
-    for (size_t gi = 0; gi < b->grids.size(); ++gi) {
-        const auto& e = b->grids[gi];
-        if (e.gens == 0 || e.W == 0 || e.Y == 0) continue;
-        const int lanes = (e.W + kResidentBatchWpl - 1) / kResidentBatchWpl;
-        if (lanes > kResidentBatchThreads)
-            return b->fail(GOL_E_UNSUPPORTED, "a grid is too wide for the resident batch");
-        const int groups = kResidentBatchThreads / lanes;
-        const int K = (int)std::min<uint64_t>(e.gens, kResidentBatchK);
-        const size_t row_bytes = 2ull * golb200::resident_stride(lanes, kResidentBatchWpl) * 4;
-        const long long fit = (long long)(avail / row_bytes) - 2 * K;   // band rows that fit
-        if (fit < 1) return b->fail(GOL_E_UNSUPPORTED, "a grid's rows do not fit in shared memory");
-        const int nb_min = (int)((e.Y + fit - 1) / fit);
-        const double work = (double)e.W * e.Y * e.gens;
-        const int nb_work = (int)std::ceil(work / std::max(1.0, total / ((double)b->num_sms *
-                                                                          kResidentBatchBandsPerCta)));
-        const int nb_rows = std::max(1, e.Y / std::max(K, kResidentBatchRowsPerGroup * groups));
-        int nb = std::max(nb_min, std::min(nb_work, nb_rows));
-        const int nb_cap = std::max(1, e.Y / K);
-        if (nb > nb_cap) {
-            if (nb_min > nb_cap) return b->fail(GOL_E_UNSUPPORTED, "a grid needs bands under K rows");
-            nb = nb_cap;
-        }
-        const int B = (e.Y + nb - 1) / nb;
-        const size_t need = (size_t)(B + 2 * K) * row_bytes;
-        smem = std::max(smem, need);
-        gb.push_back({(int)gi, nb, K, lanes, groups, (double)e.W * B * e.gens, need});
-    }
-    int per_sm = 0;
-    ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, golb200::batch_resident_kernel<kResidentBatchWpl>, kResidentBatchThreads,
-        std::max<size_t>(smem, 1));
-    if (ce == cudaSuccess && smem > 48 * 1024) {
-        ce = cudaFuncSetAttribute(golb200::batch_resident_kernel<kResidentBatchWpl>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (ce == cudaSuccess)
-            ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &per_sm, golb200::batch_resident_kernel<kResidentBatchWpl>, kResidentBatchThreads, smem);
-    }
-    if (ce != cudaSuccess) return b->cuda_fail(ce, "resident batch occupancy");
-    if (per_sm < 1) return b->fail(GOL_E_UNSUPPORTED, "resident batch kernel does not fit on an SM");
-    const int ctas = per_sm * b->num_sms;
-    for (const auto& g : gb)
-        if (g.nb > ctas) return b->fail(GOL_E_UNSUPPORTED, "a grid needs more bands than CTAs");
-    std::stable_sort(gb.begin(), gb.end(),
-                     [](const GridBands& a, const GridBands& c) { return a.band_work > c.band_work; });
-    // exchange slots and counters
-    size_t pub_words = 0;
-    int ndone = 0;
-    std::vector<size_t> pub_off(gb.size());
-    std::vector<int> done_off(gb.size());
-    for (size_t i = 0; i < gb.size(); ++i) {
-        const auto& e = b->grids[gb[i].gi];
-        const int ppitch = (e.W + 3) / 4 * 4;
-        pub_off[i] = pub_words;
-        pub_words += (size_t)gb[i].nb * 4 * gb[i].K * ppitch;
-        done_off[i] = ndone;
-        ndone += gb[i].nb;
-    }
-    ce = cudaMalloc(&b->d_rpub, std::max<size_t>(pub_words, 1) * sizeof(uint32_t));
-    if (ce == cudaSuccess) ce = cudaMalloc(&b->d_rdone, std::max(ndone, 1) * sizeof(int));
-    if (ce == cudaSuccess)
-        ce = cudaMalloc(&b->d_rjobs, std::max(ndone, 1) * sizeof(golb200::ResidentBand));
-    if (ce != cudaSuccess) return b->cuda_fail(ce, "resident batch scratch");
-    std::vector<golb200::ResidentBand> jobs;
-    jobs.reserve(ndone);
-    for (size_t i = 0; i < gb.size(); ++i) {
-        const auto& e = b->grids[gb[i].gi];
-        for (int band = 0; band < gb[i].nb; ++band) {
-            golb200::ResidentBand j{};
-            j.src = b->arena + e.offset;
-            j.dst = b->arena + e.offset + e.stride;
-            j.pub = b->d_rpub + pub_off[i];
-            j.done = b->d_rdone + done_off[i];
-            j.pitch = e.pitch;
-            j.ppitch = (e.W + 3) / 4 * 4;
-            j.W = e.W;
-            j.Y = e.Y;
-            j.K = gb[i].K;
-            j.lanes = gb[i].lanes;
-            j.groups = gb[i].groups;
-            j.b = band;
-            j.nb = gb[i].nb;
-            j.gens = (long long)e.gens;
-            jobs.push_back(j);
-        }
-    }
-    ce = cudaMemcpyAsync(b->d_rjobs, jobs.data(), jobs.size() * sizeof(golb200::ResidentBand),
-                         cudaMemcpyHostToDevice, b->stream);
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(b->stream);
-    if (ce != cudaSuccess) return b->cuda_fail(ce, "resident batch jobs");
-    b->rjobs = (int)jobs.size();
-    b->rdone = ndone;
-    b->rctas = ctas;
-    b->rsmem = smem;
-    return GOL_OK;
-}
-
-} // namespace
-
 // Every grid's bands kept in shared memory for all their generations (the
 // single-grid resident run's algorithm), persistent CTAs taking bands in
 // ticket order. Asynchronous like gol_batch_run; results in buf[1].
@@ -1168,7 +1164,33 @@ int gol_batch_run_resident(gol_batch* b) {
     if (!b) return GOL_E_INVALID;
     int rc;
     if (!b->uploaded && (rc = gol_batch_upload(b))) return rc;
-    if (!b->d_rjobs && (rc = resident_batch_plan(b))) return rc;
+    if (!b->d_rjobs) {   // plan the bands once per upload
+        std::vector<golb200::ResidentGrid> rg;
+        for (const auto& e : b->grids)
+            if (e.gens && e.W && e.Y)
+                rg.push_back({b->arena + e.offset, b->arena + e.offset + e.stride, e.pitch, e.W, e.Y,
+                              (long long)e.gens});
+        golb200::ResidentBatchPlan plan;
+        if (const char* why = golb200::plan_resident_batch(rg.data(), rg.size(), b->num_sms,
+                                                           b->device, &plan))
+            return b->fail(GOL_E_UNSUPPORTED, why);
+        cudaError_t ce = cudaMalloc(&b->d_rpub, std::max<size_t>(plan.pub_words, 1) * sizeof(uint32_t));
+        if (ce == cudaSuccess) ce = cudaMalloc(&b->d_rdone, std::max(plan.ndone, 1) * sizeof(int));
+        if (ce == cudaSuccess)
+            ce = cudaMalloc(&b->d_rjobs, std::max(plan.ndone, 1) * sizeof(golb200::ResidentBand));
+        if (ce != cudaSuccess) return b->cuda_fail(ce, "resident batch scratch");
+        std::vector<golb200::ResidentBand> jobs(plan.ndone);
+        golb200::fill_resident_jobs(plan, rg.data(), b->d_rpub, b->d_rdone, jobs.data());
+        ce = cudaMemcpyAsync(b->d_rjobs, jobs.data(), jobs.size() * sizeof(golb200::ResidentBand),
+                             cudaMemcpyHostToDevice, b->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(b->stream);
+        if (ce != cudaSuccess) return b->cuda_fail(ce, "resident batch bands");
+        b->rplan = plan;
+        b->rjobs = plan.ndone;
+        b->rdone = plan.ndone;
+        b->rctas = plan.ctas;
+        b->rsmem = plan.smem;
+    }
     cudaError_t ce = batch_restore_inputs(b, b->stream);
     // grids with no generations: the result is the input
     for (auto& e : b->grids)
@@ -1179,7 +1201,9 @@ int gol_batch_run_resident(gol_batch* b) {
     if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_rdone, 0, std::max(b->rdone, 1) * sizeof(int), b->stream);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_ticket, 0, sizeof(int), b->stream);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_status, 0, sizeof(int), b->stream);
-    if (ce == cudaSuccess && b->rjobs) ce = resident_batch_launch(b, b->rjobs, b->stream);
+    if (ce == cudaSuccess && b->rjobs)
+        ce = golb200::launch_batch_resident(b->d_rjobs, b->rjobs, b->d_ticket, b->d_status, b->rplan,
+                                            b->stream);
     if (ce != cudaSuccess) return b->cuda_fail(ce, "resident batch launch");
     for (auto& e : b->grids) e.result_buf = 1;
     b->ran = true;

@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 namespace golb200 {
 
@@ -37,6 +38,60 @@ bool plan_rows(int W, int Y, int k, int band_rows, int wpl, int num_sms, RowsPla
 // Shared-memory-resident run (gol_rows_resident.cuh): every generation of
 // a grid whose bands fit in the SMs' shared memory, in one cooperative
 // launch of one CTA per band.
+// One band of one grid, all generations, in one CTA's shared memory
+// (resident_band in gol_rows_resident.cuh).
+struct ResidentBand {
+    const uint32_t* src;   // the grid at generation 0 (row r at src + r * pitch)
+    uint32_t* dst;         // the grid after `gens` generations (not src)
+    uint32_t* pub;         // the grid's exchange slots: band b's at (b * 4 + parity * 2 + side)
+                           // * K * ppitch words (side 0: its top K rows, 1: its bottom K rows)
+    int* done;             // the grid's epoch counters, one per band, zero at start
+    int pitch;             // words from one grid row to the next (>= W)
+    int ppitch;            // words per row in the exchange slots (>= W, a multiple of 4)
+    int W, Y;              // words per row, rows
+    int K;                 // generations per epoch
+    int lanes, groups;     // threads: lanes across a row x row groups
+    int b, nb;             // this band, bands of the grid (rows split evenly)
+    long long gens;
+};
+
+// A grid of a resident batch launch (batch_resident_kernel).
+struct ResidentGrid {
+    const uint32_t* src;
+    uint32_t* dst;
+    int pitch, W, Y;
+    long long gens;        // > 0
+};
+
+// The bands of a resident batch: per grid its band count, epoch length,
+// lanes and row groups, in launch order (longest band first, a grid's bands
+// consecutive); the exchange slots, counters and shared memory they need and
+// the CTAs the launch runs.
+struct ResidentBatchPlan {
+    struct Grid {
+        int index;             // into the ResidentGrid list
+        int nb, K, lanes, groups, ppitch;
+        size_t pub_off;        // words into the exchange slots
+        int done_off;          // ints into the counters
+    };
+    std::vector<Grid> grids;
+    size_t smem = 0, pub_words = 0;
+    int ndone = 0;             // bands in all
+    int ctas = 0;
+};
+// Plans grids g[0..n) (every gens > 0); nullptr or why they cannot run.
+const char* plan_resident_batch(const ResidentGrid* g, size_t n, int num_sms, int device,
+                                ResidentBatchPlan* p);
+// Whether a W x Y grid can run in a resident batch (whatever its generations).
+bool resident_batch_fits(int W, int Y, int num_sms, int device);
+// The band list (p.ndone entries, launch order) given the slots and counters.
+void fill_resident_jobs(const ResidentBatchPlan& p, const ResidentGrid* g, uint32_t* pub, int* done,
+                        ResidentBand* jobs);
+// One persistent cooperative launch over the bands; ticket, status and the
+// counters must be zero.
+cudaError_t launch_batch_resident(const ResidentBand* jobs, int njobs, int* ticket, int* status,
+                                  const ResidentBatchPlan& p, cudaStream_t stream);
+
 struct ResidentPlan {
     int wpl = 0, lanes = 0, groups = 0;   // lanes of wpl words across a row, row groups
     int K = 0;                            // generations per epoch (halo rows)

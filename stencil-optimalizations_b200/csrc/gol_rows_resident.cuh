@@ -40,6 +40,7 @@
 
 #include <cstdint>
 
+#include "gol_internal.h"
 #include "gol_rows_temporal.cuh"
 #include "gol_word_ops.cuh"
 
@@ -221,22 +222,6 @@ __device__ __forceinline__ void resident_pass(const uint32_t* S, uint32_t* D, in
     else
         resident_range<WPL, false>(S, D, lo, hi, g, g0, ng, stride, cm);
 }
-
-// One band of one grid, all generations, in this CTA's shared memory.
-struct ResidentBand {
-    const uint32_t* src;   // the grid at generation 0 (row r at src + r * pitch)
-    uint32_t* dst;         // the grid after `gens` generations (not src)
-    uint32_t* pub;         // the grid's exchange slots: band b's at (b * 4 + parity * 2 + side)
-                           // * K * ppitch words (side 0: its top K rows, 1: its bottom K rows)
-    int* done;             // the grid's epoch counters, one per band, zero at start
-    int pitch;             // words from one grid row to the next (>= W)
-    int ppitch;            // words per row in the exchange slots (>= W, a multiple of WPL)
-    int W, Y;              // words per row, rows
-    int K;                 // generations per epoch
-    int lanes, groups;     // threads: lanes across a row x row groups
-    int b, nb;             // this band, bands of the grid (rows split evenly)
-    long long gens;
-};
 
 // Global <-> register copies of a lane's words: vector accesses where the
 // lane's words are whole and aligned, else word by word up to W.

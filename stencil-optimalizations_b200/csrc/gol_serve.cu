@@ -68,6 +68,12 @@ struct RoundBuffers {
     int* d_still = nullptr;                  // per request of the round: it is still
     int* h_still = nullptr;                  // pinned copy
     size_t cap_grids = 0, cap_items = 0, cap_done = 0, cap_pstat = 0, cap_still = 0;
+    // resident rounds (GOL_SERVE_RESIDENT): bands, exchange slots, counters
+    golb200::ResidentBand* d_rjobs = nullptr;
+    golb200::ResidentBand* h_rjobs = nullptr;   // pinned staging
+    uint32_t* d_rpub = nullptr;
+    int* d_rdone = nullptr;
+    size_t cap_rjobs = 0, cap_rpub = 0, cap_rdone = 0;
     std::vector<uint64_t> ids;               // request of each grid of the round
     golb200::BatchGrid* h_grids = nullptr;   // pinned staging
     golb200::BatchItem* h_items = nullptr;
@@ -104,6 +110,7 @@ struct gol_server {
     uint64_t quantum = 64;
     int policy = GOL_SERVE_FIFO;
     int track_mode = GOL_TRACK_AUTO;
+    int mode = GOL_SERVE_PASSES;           // how a round runs (gol_serve_set_mode)
     unsigned long long* d_census = nullptr;   // wait / work cycles, items computed / skipped
     uint64_t early_finished = 0;
     uint64_t next_id = 1;
@@ -183,6 +190,25 @@ int ensure_round_capacity(gol_server* s, RoundBuffers& r, size_t grids, size_t i
     if (ce == cudaSuccess && !r.h_status) ce = cudaMallocHost(&r.h_status, sizeof(int));
     if (ce == cudaSuccess && !r.done_event) ce = cudaEventCreateWithFlags(&r.done_event, cudaEventDisableTiming);
     if (ce != cudaSuccess) return s->cuda_fail(ce, "round buffers");
+    return GOL_OK;
+}
+
+int ensure_resident_capacity(gol_server* s, RoundBuffers& r, size_t jobs, size_t pub, size_t done) {
+    cudaError_t ce = cudaSuccess;
+    auto grow = [&](size_t need, size_t& cap, auto** dptr, auto** hptr) {
+        if (need <= cap || ce != cudaSuccess) return;
+        size_t n = std::max<size_t>(need, cap * 2);
+        if (*dptr) cudaFree(*dptr);
+        if (hptr && *hptr) cudaFreeHost(*hptr);
+        *dptr = nullptr;
+        ce = cudaMalloc(reinterpret_cast<void**>(dptr), n * sizeof(**dptr));
+        if (ce == cudaSuccess && hptr) ce = cudaMallocHost(reinterpret_cast<void**>(hptr), n * sizeof(**hptr));
+        cap = ce == cudaSuccess ? n : 0;
+    };
+    grow(std::max<size_t>(jobs, 1), r.cap_rjobs, &r.d_rjobs, &r.h_rjobs);
+    grow(std::max<size_t>(pub, 1), r.cap_rpub, &r.d_rpub, static_cast<uint32_t**>(nullptr));
+    grow(std::max<size_t>(done, 1), r.cap_rdone, &r.d_rdone, static_cast<int**>(nullptr));
+    if (ce != cudaSuccess) return s->cuda_fail(ce, "resident round buffers");
     return GOL_OK;
 }
 
@@ -385,6 +411,67 @@ static uint64_t round_generations(const gol_server* s, const Request& r) {
     return left <= q ? left : q;
 }
 
+// A resident round: every running request advances up to the quantum of
+// generations with its grid cut into bands held in shared memory (one
+// persistent cooperative launch, gol_batch_run_resident's kernel), from its
+// current buffer into the other. No change flags: requests finish when their
+// generations are done.
+static int queue_resident_round(gol_server* s, RoundBuffers& rb) {
+    std::vector<golb200::ResidentGrid> grids;
+    std::vector<uint64_t> still;
+    rb.ids.clear();
+    for (uint64_t id : s->running) {
+        Request& r = s->reqs[id];
+        const uint64_t left = r.gens - r.planned;
+        const uint64_t g = std::min<uint64_t>(left, s->quantum);
+        uint32_t* cur = s->arena + r.offset + (size_t)r.parity * r.stride;
+        uint32_t* nxt = s->arena + r.offset + (size_t)(r.parity ^ 1) * r.stride;
+        grids.push_back({cur, nxt, r.W, r.W, r.Y, (long long)g});
+        rb.ids.push_back(id);
+        r.planned += g;
+        r.parity ^= 1;
+        s->cell_updates_done += r.x * r.y * g;
+        if (r.planned >= r.gens)
+            rb.finishing.push_back(id);
+        else
+            still.push_back(id);
+    }
+    s->running.swap(still);
+    golb200::ResidentBatchPlan plan;
+    if (const char* why = golb200::plan_resident_batch(grids.data(), grids.size(), s->num_sms,
+                                                       s->device, &plan))
+        return s->fail(GOL_E_UNSUPPORTED, why);
+    int rc = ensure_round_capacity(s, rb, grids.size(), 1, 1, 1);
+    if (rc) return rc;
+    if ((rc = ensure_resident_capacity(s, rb, (size_t)plan.ndone, plan.pub_words, (size_t)plan.ndone)))
+        return rc;
+    golb200::fill_resident_jobs(plan, grids.data(), rb.d_rpub, rb.d_rdone, rb.h_rjobs);
+    cudaError_t ce = cudaMemcpyAsync(rb.d_rjobs, rb.h_rjobs, (size_t)plan.ndone * sizeof(golb200::ResidentBand),
+                                     cudaMemcpyHostToDevice, s->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(rb.d_rdone, 0, (size_t)std::max(plan.ndone, 1) * sizeof(int), s->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(rb.d_ticket, 0, sizeof(int), s->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(rb.d_status, 0, sizeof(int), s->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(rb.d_still, 0, grids.size() * sizeof(int), s->stream);
+    if (ce == cudaSuccess && plan.ndone)
+        ce = golb200::launch_batch_resident(rb.d_rjobs, plan.ndone, rb.d_ticket, rb.d_status, plan, s->stream);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(rb.h_status, rb.d_status, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(rb.h_still, rb.d_still, grids.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                             s->stream);
+    if (ce == cudaSuccess) ce = cudaEventRecord(rb.done_event, s->stream);
+    if (ce != cudaSuccess) return s->cuda_fail(ce, "resident round launch");
+    rb.in_flight = true;
+    rb.seq = ++s->round_seq;
+    for (uint64_t id : rb.finishing) {
+        s->reqs[id].last_round_slot = s->next_slot;
+        s->reqs[id].last_round_seq = rb.seq;
+    }
+    ++s->rounds_launched;
+    s->next_slot = (s->next_slot + 1) % kRoundsInFlight;
+    return GOL_OK;
+}
+
 int gol_serve_submit(gol_server* s, const uint8_t* cells, uint64_t x, uint64_t y,
                      uint64_t generations, uint64_t* id) {
     if (!s) return GOL_E_INVALID;
@@ -398,6 +485,8 @@ int gol_serve_submit(gol_server* s, const uint8_t* cells, uint64_t x, uint64_t y
     r.Y = (int)y;
     r.gens = generations;
     if (!plan_request(s, r, generations)) return s->fail(GOL_E_UNSUPPORTED, "no plan for this request");
+    if (s->mode == GOL_SERVE_RESIDENT && !golb200::resident_batch_fits(r.W, r.Y, s->num_sms, s->device))
+        return s->fail(GOL_E_UNSUPPORTED, "request does not fit a resident round");
     if (r.slot_words > s->arena_words) return s->fail(GOL_E_NOMEM, "request larger than the device arena");
     r.words.resize((size_t)r.W * r.Y);
     golb200::host_pack_u8(cells, x, y, r.words.data());
@@ -426,6 +515,8 @@ int gol_serve_submit_random(gol_server* s, uint64_t x, uint64_t y, uint64_t gene
     r.input_seed = seed;
     r.input_density = density;
     if (!plan_request(s, r, generations)) return s->fail(GOL_E_UNSUPPORTED, "no plan for this request");
+    if (s->mode == GOL_SERVE_RESIDENT && !golb200::resident_batch_fits(r.W, r.Y, s->num_sms, s->device))
+        return s->fail(GOL_E_UNSUPPORTED, "request does not fit a resident round");
     if (r.slot_words > s->arena_words) return s->fail(GOL_E_NOMEM, "request larger than the device arena");
     if (id) *id = r.id;
     s->queue.push_back(r.id);
@@ -493,6 +584,7 @@ int gol_serve_step(gol_server* s) {
         rc = harvest(s, true);
         if (rc) return rc;
     }
+    if (s->mode == GOL_SERVE_RESIDENT) return queue_resident_round(s, rb);
     // Plan this round: every running request advances its round's
     // generations (round_generations).
     std::vector<golb200::BatchGrid> grids;
@@ -685,6 +777,16 @@ int gol_serve_set_tracking(gol_server* s, int32_t mode) {
     return GOL_OK;
 }
 
+int gol_serve_set_mode(gol_server* s, int32_t mode) {
+    if (!s) return GOL_E_INVALID;
+    if (mode != GOL_SERVE_PASSES && mode != GOL_SERVE_RESIDENT)
+        return s->fail(GOL_E_INVALID, "mode must be GOL_SERVE_PASSES or GOL_SERVE_RESIDENT");
+    if (!s->running.empty() || !s->queue.empty())
+        return s->fail(GOL_E_STATE, "the round mode changes only while no request is queued or running");
+    s->mode = mode;
+    return GOL_OK;
+}
+
 int gol_serve_tiles(gol_server* s, uint64_t* computed, uint64_t* skipped, uint64_t* early_finished) {
     if (!s) return GOL_E_INVALID;
     unsigned long long c[4] = {0, 0, 0, 0};
@@ -715,6 +817,10 @@ void gol_serve_destroy(gol_server* s) {
         if (r.d_pstat) cudaFree(r.d_pstat);
         if (r.d_still) cudaFree(r.d_still);
         if (r.h_still) cudaFreeHost(r.h_still);
+        if (r.d_rjobs) cudaFree(r.d_rjobs);
+        if (r.h_rjobs) cudaFreeHost(r.h_rjobs);
+        if (r.d_rpub) cudaFree(r.d_rpub);
+        if (r.d_rdone) cudaFree(r.d_rdone);
         if (r.done_event) cudaEventDestroy(r.done_event);
     }
     if (s->arena) cudaFree(s->arena);

@@ -182,6 +182,7 @@ def lib():
     L.gol_serve_stats.argtypes = [_vp] + [ctypes.POINTER(_u64)] * 5
     L.gol_serve_drain.argtypes = [_vp]
     L.gol_serve_set_policy.argtypes = [_vp, ctypes.c_int32]
+    L.gol_serve_set_mode.argtypes = [_vp, ctypes.c_int32]
     L.gol_serve_set_tracking.argtypes = [_vp, ctypes.c_int32]
     L.gol_serve_tiles.argtypes = [_vp] + [ctypes.POINTER(_u64)] * 3
     L.gol_serve_last_error.argtypes = [_vp]
@@ -812,12 +813,20 @@ class GolServer:
     POLICIES = {"fifo": 0, "srpt": 1}
 
     def set_policy(self, policy: str) -> None:
-        """"fifo" (arrival order, fixed quantum) or "srpt" (least work first,
-        small grids get more generations per round)."""
+        """"fifo" (arrival order) or "srpt" (least work first) admission; every
+        running request advances the quantum per round either way."""
         self._check(lib().gol_serve_set_policy(self._s, self.POLICIES[policy]), "serve_set_policy")
 
     def set_tracking(self, mode: str) -> None:
         self._check(lib().gol_serve_set_tracking(self._s, GolBatch.TRACK[mode]), "serve_set_tracking")
+
+    MODES = {"passes": 0, "resident": 1}
+
+    def set_mode(self, mode: str) -> None:
+        """"passes" (dependent pass items, change tracking) or "resident"
+        (bands in shared memory for the round's generations); only while no
+        request is queued or running."""
+        self._check(lib().gol_serve_set_mode(self._s, self.MODES[mode]), "serve_set_mode")
 
     def tiles(self) -> dict:
         c, k, e = _u64(), _u64(), _u64()

@@ -45,7 +45,7 @@ def run_stream(rate: float = 2000.0, seconds: float = 2.0, seed: int = 42, min_s
                arena_bytes: int = 0, device: int = 0, fetch: str = "words",
                max_requests: int | None = None, server: golb200.GolServer | None = None,
                policy: str = "fifo", tracking: str = "auto", host_io: bool = False,
-               check_every: int = 0) -> dict:
+               check_every: int = 0, mode: str = "passes") -> dict:
     """Serves the seeded Poisson stream that arrives within `seconds`.
 
     host_io: every request's cells are made on the host before the stream
@@ -55,7 +55,9 @@ def run_stream(rate: float = 2000.0, seconds: float = 2.0, seed: int = 42, min_s
     cells (copy back, host unpack). Otherwise inputs are generated on the
     device and results fetched as packed words.
     check_every > 0 keeps the fetched result of every check_every-th request
-    (submission order) in r["samples"] as (request, result)."""
+    (submission order) in r["samples"] as (request, result).
+    mode: "passes" (rounds of dependent pass items, change tracking as set)
+    or "resident" (rounds with every request's bands in shared memory)."""
     from concurrent.futures import ThreadPoolExecutor
     n = int(rate * seconds * 1.2) + 16
     if max_requests:
@@ -67,6 +69,7 @@ def run_stream(rate: float = 2000.0, seconds: float = 2.0, seed: int = 42, min_s
     srv = server or golb200.GolServer(device=device, arena_bytes=arena_bytes, quantum=quantum)
     srv.set_policy(policy)
     srv.set_tracking(tracking)
+    srv.set_mode(mode)
     host_cells = []
     if host_io:
         with ThreadPoolExecutor(max_workers=usable_cpus() or 1) as pool:
@@ -122,7 +125,7 @@ def run_stream(rate: float = 2000.0, seconds: float = 2.0, seed: int = 42, min_s
             srv.close()
     lat = np.array(latencies) if latencies else np.zeros(1)
     return {
-        "policy": policy, "tracking": tracking, "host_io": host_io,
+        "policy": policy, "tracking": tracking, "host_io": host_io, "mode": mode,
         "tiles_computed": tiles["computed"],
         "tiles_skipped": tiles["skipped"], "finished_early_still": tiles["early_finished"],
         "samples": samples,
@@ -148,9 +151,10 @@ def main() -> None:
     ap.add_argument("--policy", choices=["fifo", "srpt"], default="fifo")
     ap.add_argument("--tracking", choices=["auto", "on", "off"], default="auto")
     ap.add_argument("--host-io", action="store_true")
+    ap.add_argument("--mode", choices=["passes", "resident"], default="passes")
     a = ap.parse_args()
     r = run_stream(a.rate, a.seconds, a.seed, quantum=a.quantum, policy=a.policy,
-                   tracking=a.tracking, host_io=a.host_io)
+                   tracking=a.tracking, host_io=a.host_io, mode=a.mode)
     r.pop("samples")
     print(json.dumps(r))
 

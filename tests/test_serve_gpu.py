@@ -42,6 +42,38 @@ def test_results_same_alone_and_in_the_mix():
             assert np.array_equal(alone, oracle.life_cells(c, d["gens"])), i
 
 
+def test_resident_rounds_vs_oracle():
+    """GOL_SERVE_RESIDENT: rounds with every running request's bands in
+    shared memory; staggered arrivals, quanta that split a request's
+    generations unevenly, odd word counts, one row; every result equals the
+    oracle. The mode cannot change while requests are queued."""
+    work = golb200.workload_uneven(9, 20, 64, 1536, 64, (0.1, 0.5), (1, 500))
+    cells = [golb200.load_bernoulli(d["x"], d["y"], d["cell_seed"], d["density"]) for d in work]
+    gens = [d["gens"] for d in work]
+    cells += [oracle.random_ones_zeros(32 * 37, 200, 1), oracle.random_ones_zeros(64, 1, 2),
+              oracle.random_ones_zeros(2048, 3, 3)]
+    gens += [77, 33, 0]
+    with golb200.GolServer(arena_bytes=256 << 20, quantum=48) as s:
+        s.set_mode("resident")
+        with pytest.raises(RuntimeError, match="resident round"):   # rows wider than 32768 cells
+            s.submit(np.zeros((2, 32768 + 64), np.uint8), 5)
+        ids = {}
+        got = {}
+        for i, (c, n) in enumerate(zip(cells, gens)):
+            ids[s.submit(c, n)] = i
+            if i == 0:
+                with pytest.raises(RuntimeError, match="mode"):
+                    s.set_mode("passes")
+            if i % 3 == 2:
+                s.step()
+        while len(got) < len(ids):
+            s.step()
+            for rid in s.finished():
+                got[ids[rid]] = s.fetch(rid)
+    for i, (c, n) in enumerate(zip(cells, gens)):
+        assert np.array_equal(got[i], oracle.life_cells(c, n)), (i, c.shape, n)
+
+
 def test_admission_waits_for_memory():
     # room for about two 1024 x 1024 requests at a time (2 x 2 x 128 KiB)
     cells = [oracle.random_ones_zeros(1024, 1024, seed) for seed in range(6)]
