@@ -229,7 +229,7 @@ cudaError_t launch_resident(const uint32_t* src, uint32_t* dst, int W, int Y, lo
     cudaError_t e = cudaMemsetAsync(epoch_done, 0, (size_t)p.nbands * sizeof(int), stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, sizeof(int), stream);
     if (e != cudaSuccess) return e;
-    ResidentLaunch a{src, dst, pub, epoch_done, status, W, Y, p.band, p.K, p.lanes, p.groups, gens,
+    ResidentLaunch a{src, dst, pub, epoch_done, status, W, Y, p.K, p.lanes, p.groups, gens,
                      spin_limit > 0 ? spin_limit : (1ll << 24)};
     switch (p.wpl) {
         case 4: return launch_resident_wpl<4>(a, p, stream);

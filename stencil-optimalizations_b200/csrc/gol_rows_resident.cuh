@@ -32,10 +32,13 @@
 // four zero words of padding each side, so the words just outside a lane's
 // span are plain loads from the row (cheaper on the integer pipe, the
 // bound here, than shuffles and selects). Columns at or past W exist only
-// in the last warps of a row, which alone run the masked variant.
+// in the last lanes of a row, which alone run the masked variant.
 //
-// All CTAs must be resident at once (they wait on each other): the launch
-// is cooperative, one CTA per SM at most.
+// The band algorithm (resident_band) serves two kernels: one grid, CTA c
+// running band c (rows_resident_kernel), and many grids, persistent CTAs
+// taking bands of a batch in ticket order (batch_resident_kernel). All
+// CTAs of a launch must be resident at once (they wait on each other): the
+// launches are cooperative.
 #pragma once
 
 #include <cstdint>
@@ -65,8 +68,6 @@ struct ResidentLaunch {   // one grid (rows_resident_kernel)
     int* epoch_done;       // [nbands], zero at launch: epochs published
     int* status;           // GOL_E_TIMEOUT if a wait gave up
     int W, Y;
-    int band;              // rows of the largest band (bands split Y evenly, each >= K
-                           // when there are several)
     int K;                 // generations per epoch
     int lanes;             // lanes across a row (ceil(W / WPL), a multiple of 32)
     int groups;            // row groups (blockDim.x = lanes * groups)
