@@ -571,12 +571,23 @@ using golb200::BatchItem;
 
 namespace golb200 {
 
+#ifndef GOL_RBATCH_K
+#define GOL_RBATCH_K 8
+#endif
+#ifndef GOL_RBATCH_ROWS_PER_GROUP
+#define GOL_RBATCH_ROWS_PER_GROUP 8
+#endif
+#ifndef GOL_RBATCH_BANDS_PER_CTA
+#define GOL_RBATCH_BANDS_PER_CTA 3
+#endif
 namespace {
 constexpr int kResidentBatchWpl = 2;        // words per lane of the resident batch kernel
 constexpr int kResidentBatchThreads = 512;  // threads per CTA
-constexpr int kResidentBatchK = 8;          // generations per epoch
-constexpr int kResidentBatchRowsPerGroup = 8;   // fewer rows per group and pass cost warm-up
-constexpr int kResidentBatchBandsPerCta = 3;    // about this many bands per CTA (balance)
+constexpr int kResidentBatchK = GOL_RBATCH_K;   // generations per epoch
+constexpr int kResidentBatchRowsPerGroup = GOL_RBATCH_ROWS_PER_GROUP;   // fewer rows per group and
+                                                                        // pass cost warm-up
+constexpr int kResidentBatchBandsPerCta = GOL_RBATCH_BANDS_PER_CTA;     // about this many bands per
+                                                                        // CTA (balance)
 } // namespace
 
 // Per grid: lanes of two words across its row and row groups over the CTA's
