@@ -417,16 +417,25 @@ static uint64_t round_generations(const gol_server* s, const Request& r) {
 // current buffer into the other. No change flags: requests finish when their
 // generations are done.
 static int queue_resident_round(gol_server* s, RoundBuffers& rb) {
+    // the round's grids first (requests change state only once it is planned)
     std::vector<golb200::ResidentGrid> grids;
-    std::vector<uint64_t> still;
-    rb.ids.clear();
     for (uint64_t id : s->running) {
-        Request& r = s->reqs[id];
-        const uint64_t left = r.gens - r.planned;
-        const uint64_t g = std::min<uint64_t>(left, s->quantum);
+        const Request& r = s->reqs[id];
+        const uint64_t g = std::min<uint64_t>(r.gens - r.planned, s->quantum);
         uint32_t* cur = s->arena + r.offset + (size_t)r.parity * r.stride;
         uint32_t* nxt = s->arena + r.offset + (size_t)(r.parity ^ 1) * r.stride;
         grids.push_back({cur, nxt, r.W, r.W, r.Y, (long long)g});
+    }
+    golb200::ResidentBatchPlan plan;
+    if (const char* why = golb200::plan_resident_batch(grids.data(), grids.size(), s->num_sms,
+                                                       s->device, &plan))
+        return s->fail(GOL_E_UNSUPPORTED, why);
+    std::vector<uint64_t> still;
+    rb.ids.clear();
+    for (size_t i = 0; i < s->running.size(); ++i) {
+        const uint64_t id = s->running[i];
+        Request& r = s->reqs[id];
+        const uint64_t g = (uint64_t)grids[i].gens;
         rb.ids.push_back(id);
         r.planned += g;
         r.parity ^= 1;
@@ -437,10 +446,6 @@ static int queue_resident_round(gol_server* s, RoundBuffers& rb) {
             still.push_back(id);
     }
     s->running.swap(still);
-    golb200::ResidentBatchPlan plan;
-    if (const char* why = golb200::plan_resident_batch(grids.data(), grids.size(), s->num_sms,
-                                                       s->device, &plan))
-        return s->fail(GOL_E_UNSUPPORTED, why);
     int rc = ensure_round_capacity(s, rb, grids.size(), 1, 1, 1);
     if (rc) return rc;
     if ((rc = ensure_resident_capacity(s, rb, (size_t)plan.ndone, plan.pub_words, (size_t)plan.ndone)))
