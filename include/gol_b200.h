@@ -69,8 +69,9 @@ enum gol_algorithm {
                                 SMs' shared memory, e.g. 8192 x 8192, else
                                 gol_init returns GOL_E_UNSUPPORTED);
                                 temporal_steps = generations between halo
-                                exchanges (0 = 8); the run budget is checked
-                                only before the launch; a band that waits too
+                                exchanges (0 = 8); with a run budget the run
+                                goes in launches of 64, 128, ... generations,
+                                the budget checked before each; a band that waits too
                                 long for a neighbour stops the run with
                                 GOL_E_TIMEOUT (from gol_sync / gol_finalize) */
 };

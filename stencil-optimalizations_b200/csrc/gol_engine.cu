@@ -452,6 +452,8 @@ int gol_init(gol_engine* e) {
     return GOL_OK;
 }
 
+static int resident_status(gol_engine* e);
+
 int gol_run(gol_engine* e, uint64_t n) {
     if (!e) return GOL_E_INVALID;
     if (!e->initialized) return e->fail(GOL_E_STATE, "run before initialize");
@@ -468,18 +470,27 @@ int gol_run(gol_engine* e, uint64_t n) {
         return (uint64_t)s.count() >= budget;
     };
     if (e->resident) {   // every generation in one cooperative launch
-        // (runs longer than 2^30 generations in several, so the kernel's
-        // epoch counters stay within int)
+        // Runs longer than 2^30 generations take several launches (the
+        // kernel's epoch counters stay within int). With a time budget the
+        // run goes in launches of 64, 128, 256, ... generations, each waited
+        // for, and stops before the first launch past the budget (so it ends
+        // within about twice the budget).
+        uint64_t step = 64;
         for (uint64_t done = 0; done < n;) {
             if (time_is_up()) return GOL_OK;
-            const uint64_t chunk = std::min<uint64_t>(n - done, 1ull << 30);
+            const uint64_t chunk = std::min<uint64_t>(n - done, budget ? step : (1ull << 30));
             cudaError_t ce = golb200::launch_resident(e->d[e->cur], e->d[e->cur ^ 1], e->W, e->Y,
                                                       (long long)chunk, e->rplan, e->r_pub, e->r_ints,
                                                       e->r_ints + e->rplan.nbands, e->stream);
+            if (ce == cudaSuccess && budget) ce = cudaStreamSynchronize(e->stream);
             if (ce != cudaSuccess) return e->cuda_fail(ce, "resident run launch");
             e->cur ^= 1;
             done += chunk;
             e->performed = done;
+            if (budget) {
+                if (int st = resident_status(e)) return st;
+                step = std::min<uint64_t>(step * 2, 1ull << 30);
+            }
         }
         return GOL_OK;
     }

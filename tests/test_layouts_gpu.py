@@ -37,11 +37,14 @@ def test_device_conversions_match_oracle(layout, word_bits, x, y):
     assert torch.equal(back, rows)
 
 
-@pytest.mark.parametrize("layout,word_bits", [("tiles", 64), ("columns", 32), ("tiles", 16)])
-def test_engine_run_through_layout_io(layout, word_bits):
+@pytest.mark.parametrize("layout,word_bits,algorithm", [("tiles", 64, "auto"), ("columns", 32, "auto"),
+                                                        ("tiles", 16, "auto"), ("tiles", 64, "resident"),
+                                                        ("columns", 64, "resident")])
+def test_engine_run_through_layout_io(layout, word_bits, algorithm):
     x, y, n = 512, 256, 77
     g = oracle.random_ones_zeros(x, y, 21)
-    with golb200.GolB200(grid_dimensions=(x, y), state_bits_count=64, temporal_steps=4) as alg:
+    with golb200.GolB200(grid_dimensions=(x, y), state_bits_count=64, temporal_steps=4,
+                         algorithm=algorithm) as alg:
         alg.set_input_layout(golb200.pack_layout(g, layout, word_bits), layout, word_bits)
         alg.initialize_data_structures()
         alg.run(n)

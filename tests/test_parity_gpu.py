@@ -153,9 +153,10 @@ def test_zero_generations_is_identity():
     assert np.array_equal(run_engine(g, 0), g)
 
 
-def test_int32_encoding():
+@pytest.mark.parametrize("alg", ["auto", "resident"])
+def test_int32_encoding(alg):
     g = oracle.random_ones_zeros(192, 50, 8).astype(np.int32)
-    out = run_engine(g, 19)
+    out = run_engine(g, 19, algorithm=alg)
     assert out.dtype == np.int32
     assert np.array_equal(out, oracle.life_cells(g.astype(np.uint8), 19).astype(np.int32))
 
@@ -182,10 +183,11 @@ def test_graph_chunked_long_run():
         assert np.array_equal(run_engine(g, n, k=k), oracle.life_cells(g, n)), (k, n)
 
 
-def test_runtime_budget_stops_early_and_reports_generations():
+@pytest.mark.parametrize("alg", ["auto", "resident"])
+def test_runtime_budget_stops_early_and_reports_generations(alg):
     g = oracle.random_ones_zeros(64, 64, 1)
-    with golb200.GolB200(grid_dimensions=(64, 64), temporal_steps=1,
-                         max_runtime_seconds=1) as alg:
+    with golb200.GolB200(grid_dimensions=(64, 64), temporal_steps=1 if alg == "auto" else 0,
+                         max_runtime_seconds=1, algorithm=alg) as alg:
         alg.set_and_format_input_data(g)
         alg.initialize_data_structures()
         alg.run(10**12)
