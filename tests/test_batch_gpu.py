@@ -54,7 +54,8 @@ def test_batch_resident_vs_oracle():
              (oracle.random_ones_zeros(64, 3, 6), 0),            # zero generations
              (oracle.random_ones_zeros(128, 5, 7), 20),          # fewer rows than an epoch
              (oracle.random_ones_zeros(4096, 700, 8), 3),        # fewer generations than an epoch
-             (oracle.random_ones_zeros(8192, 1000, 9), 64)]      # many bands
+             (oracle.random_ones_zeros(8192, 1000, 9), 64),      # many bands
+             (oracle.random_ones_zeros(32768, 300, 10), 20)]     # 512 lanes, one row group
     with golb200.GolBatch() as b:
         ids = [b.add(c, n) for c, n in work]
         want = [oracle.life_cells(c, n) for c, n in work]

@@ -111,13 +111,15 @@ def test_streaming_kernel_stateless_pass():
 @pytest.mark.parametrize("x,y,gens,k", [(8192, 8192, 300, 0), (4096, 1000, 77, 8), (96, 40, 33, 4),
                                          (32 * 37, 300, 100, 5), (2048, 64, 0, 8), (1024, 500, 1, 8),
                                          (64, 148 * 9 + 5, 50, 3), (32 * 255, 700, 64, 16),
-                                         (64, 5, 40, 8), (96, 1, 9, 4), (128, 12, 30, 8)])
+                                         (64, 5, 40, 8), (96, 1, 9, 4), (128, 12, 30, 8),
+                                         (32768, 1000, 30, 8)])
 def test_resident_run(x, y, gens, k):
     """GOL_ALG_RESIDENT: the whole run in one cooperative launch, each CTA's
     band in shared memory, halos exchanged every k generations; odd widths
     (one word per lane), bands of unequal height, generation counts that k
     does not divide, zero and one generation, grids of fewer rows than k
-    (one band) and of one row."""
+    (one band) and of one row, and 32768-cell rows (512 lanes, one row group
+    doing both edges)."""
     g = oracle.random_ones_zeros(x, y, x + y + gens)
     out = run_engine(g, gens, k=k, word_bits=32, algorithm="resident")
     assert np.array_equal(out, oracle.life_cells(g, gens)), (x, y, gens, k)
