@@ -38,6 +38,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -596,11 +598,51 @@ constexpr int kResidentBatchBandsPerCta = GOL_RBATCH_BANDS_PER_CTA;     // about
 // kResidentBatchBandsPerCta bands per CTA over the batch), fewer where a
 // band would give a row group under kResidentBatchRowsPerGroup rows; every
 // band of a grid at least K rows, at most one band per SM.
+namespace {
+// Per device: the opt-in shared memory per CTA, with the kernel's dynamic
+// shared memory limit raised to it (once), and the resident CTAs per SM by
+// shared memory size in 4 KB steps. Serving plans a launch per round, so
+// these are looked up once.
+struct ResidentDeviceInfo {
+    int smem_optin = 0;
+    std::map<size_t, int> per_sm;
+};
+std::mutex g_resident_info_mu;
+std::map<int, ResidentDeviceInfo> g_resident_info;
+
+const char* resident_device(int device, size_t smem, int* smem_optin, int* per_sm) {
+    std::lock_guard<std::mutex> lock(g_resident_info_mu);
+    ResidentDeviceInfo& d = g_resident_info[device];
+    if (!d.smem_optin) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess ||
+            cudaFuncSetAttribute(batch_resident_kernel<kResidentBatchWpl>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, v - 1024) != cudaSuccess)
+            return "device attribute";
+        d.smem_optin = v;
+    }
+    *smem_optin = d.smem_optin;
+    if (per_sm) {
+        const size_t key = (std::max<size_t>(smem, 1) + 4095) / 4096 * 4096;
+        auto it = d.per_sm.find(key);
+        if (it == d.per_sm.end()) {
+            int n = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &n, batch_resident_kernel<kResidentBatchWpl>, kResidentBatchThreads,
+                    std::min<size_t>(key, (size_t)d.smem_optin - 1024)) != cudaSuccess)
+                return "resident batch occupancy";
+            it = d.per_sm.emplace(key, n).first;
+        }
+        *per_sm = it->second;
+    }
+    return nullptr;
+}
+} // namespace
+
 const char* plan_resident_batch(const ResidentGrid* g, size_t n, int num_sms, int device,
                                 ResidentBatchPlan* p) {
     int smem_optin = 0;
-    if (cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess)
-        return "device attribute";
+    if (const char* why = resident_device(device, 0, &smem_optin, nullptr)) return why;
     const size_t avail = (size_t)smem_optin - 1024;
     double total = 0;
     for (size_t i = 0; i < n; ++i) total += (double)g[i].W * g[i].Y * g[i].gens;
@@ -634,13 +676,7 @@ const char* plan_resident_batch(const ResidentGrid* g, size_t n, int num_sms, in
         order.push_back({(double)e.W * B * e.gens, pg});
     }
     int per_sm = 0;
-    if (cudaFuncSetAttribute(batch_resident_kernel<kResidentBatchWpl>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)std::max<size_t>(smem, 1)) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_resident_kernel<kResidentBatchWpl>,
-                                                      kResidentBatchThreads,
-                                                      std::max<size_t>(smem, 1)) != cudaSuccess)
-        return "resident batch occupancy";
+    if (const char* why = resident_device(device, smem, &smem_optin, &per_sm)) return why;
     if (per_sm < 1) return "resident batch kernel does not fit on an SM";
     const int ctas = per_sm * num_sms;
     std::stable_sort(order.begin(), order.end(),
@@ -663,9 +699,7 @@ const char* plan_resident_batch(const ResidentGrid* g, size_t n, int num_sms, in
 
 bool resident_batch_fits(int W, int Y, int num_sms, int device) {
     int smem_optin = 0;
-    if (W <= 0 || Y <= 0 ||
-        cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess)
-        return false;
+    if (W <= 0 || Y <= 0 || resident_device(device, 0, &smem_optin, nullptr)) return false;
     const int lanes = (W + kResidentBatchWpl - 1) / kResidentBatchWpl;
     if (lanes > kResidentBatchThreads) return false;
     const size_t row_bytes = 2ull * resident_stride(lanes, kResidentBatchWpl) * 4;
@@ -702,10 +736,7 @@ void fill_resident_jobs(const ResidentBatchPlan& p, const ResidentGrid* g, uint3
 
 cudaError_t launch_batch_resident(const ResidentBand* jobs, int njobs, int* ticket, int* status,
                                   const ResidentBatchPlan& p, cudaStream_t stream) {
-    cudaError_t ce = cudaFuncSetAttribute(batch_resident_kernel<kResidentBatchWpl>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)std::max<size_t>(p.smem, 1));
-    if (ce != cudaSuccess) return ce;
+    // (the kernel's dynamic shared memory limit was raised when p was planned)
     long long spin = 1ll << 24;
     void* args[] = {&jobs, &njobs, &ticket, &status, &spin};
     return cudaLaunchCooperativeKernel((const void*)batch_resident_kernel<kResidentBatchWpl>,
